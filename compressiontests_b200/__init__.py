@@ -1,0 +1,25 @@
+"""B200 (sm_100a) implementation of the sparse solver path of nickreserved/CompressionTests.
+
+CSR and DuVi sparse matrix-vector products, weighted Jacobi and Gauss-Seidel
+smoothing, geometric-multigrid transfers and the PCG reductions, behind the C
+ABI of include/duvi_gpu.h (libduvigpu.so, built in-tree).  This package is a
+thin Python view of that ABI, shaped like the reference's C# solver classes.
+"""
+from . import _native
+from ._native import DuviError, NotImplementedFeatureError, NotInitializedError, NoDeviceError
+from .sparse import CudaContext, SparseMatrix
+from .solvers import (CudaCsrGeometricMultigridSolver, CudaCsrPcgSolver, CudaDuViGeometricMultigridSolver,
+                      IterativeStatistics, MultigridPcgSolver, make_path)
+from .cantilever import FemCantilever3D, hex_hierarchy, hex_stiffness, hex_trilinear, traction_rhs, cartesian_transfer
+
+__all__ = [
+    "CudaContext", "SparseMatrix", "CudaCsrGeometricMultigridSolver", "CudaDuViGeometricMultigridSolver",
+    "CudaCsrPcgSolver", "MultigridPcgSolver", "IterativeStatistics", "FemCantilever3D", "hex_hierarchy",
+    "hex_stiffness", "hex_trilinear", "traction_rhs", "cartesian_transfer", "make_path", "DuviError",
+    "NotImplementedFeatureError", "NotInitializedError", "NoDeviceError",
+]
+
+
+def load():
+    """Load the native library now (raises ImportError if it was not built)."""
+    return _native.lib()

@@ -1,0 +1,584 @@
+// Host-side setup of libduvigpu.so: DuVi encoding, row bundles, Jacobi and
+// coarse-solve preparation, Gauss-Seidel orderings, structured hex workload
+// generator.  None of this runs inside a solve.
+#include "dv_internal.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+// ---------------------------------------------------------------------------
+// .NET Dictionary<double,int> semantics used by the DuVi value dedup
+// ---------------------------------------------------------------------------
+// double.GetHashCode (.NET 8): zeros and NaNs normalised, then the two 32-bit
+// halves xor-ed.
+static inline int32_t net_double_hash(double x) {
+    uint64_t bits;
+    std::memcpy(&bits, &x, 8);
+    const uint64_t sign = 0x8000000000000000ull, pinf = 0x7FF0000000000000ull;
+    if (((bits - 1) & ~sign) >= pinf) bits &= pinf;
+    return (int32_t)(uint32_t)bits ^ (int32_t)(uint32_t)(bits >> 32);
+}
+
+namespace {
+// Chained hash table with the bucket-chain discipline of System.Collections.
+// Generic.Dictionary: new entries go to the head of their chain, lookups walk
+// newest-first and accept the first entry whose 32-bit hash code matches and
+// whose comparer says Equals (DuViCompressedSparseMatrix.cs:168-174).
+struct NetDoubleDict {
+    double tol;
+    std::vector<double> keys;
+    std::vector<int32_t> codes, next;
+    std::vector<int32_t> buckets;   // head entry + 1, 0 = empty
+    uint32_t mask = 0;
+    explicit NetDoubleDict(double t) : tol(t) { rehash(1024); }
+    int32_t code(double x) const {
+        return tol > 0 ? net_double_hash(std::nearbyint(x / (2 * tol))) : net_double_hash(x);
+    }
+    bool eq(double s, double k) const {
+        return tol > 0 ? std::fabs(s - k) < tol : (s == k || (std::isnan(s) && std::isnan(k)));
+    }
+    void rehash(size_t nb) {
+        buckets.assign(nb, 0);
+        mask = (uint32_t)nb - 1;
+        for (size_t i = 0; i < keys.size(); ++i) {
+            uint32_t b = (uint32_t)codes[i] & mask;
+            next[i] = buckets[b] - 1;
+            buckets[b] = (int32_t)i + 1;
+        }
+    }
+    int32_t find_or_insert(double v) {
+        int32_t c = code(v);
+        uint32_t b = (uint32_t)c & mask;
+        for (int32_t i = buckets[b] - 1; i >= 0; i = next[i])
+            if (codes[i] == c && eq(keys[i], v)) return i;
+        int32_t id = (int32_t)keys.size();
+        keys.push_back(v);
+        codes.push_back(c);
+        next.push_back(buckets[b] - 1);
+        buckets[b] = id + 1;
+        if (keys.size() > buckets.size()) rehash(buckets.size() * 2);
+        return id;
+    }
+};
+}  // namespace
+
+// FromDokRowMajor (OpenCLDuViGeometricMultigridSolver.cs:753-851).  The block
+// ("DU") part is independent per row and built in parallel; the value ("VI")
+// part is sequential in CSR order because first occurrence defines the index.
+void dv_encode_duvi(const dv_csr_host &a, double tol, int force_bits, DuviHost &h) {
+    const int32_t n = a.n_rows;
+    const int64_t nnz = a.rowptr[n];
+    DV_REQUIRE(nnz <= 0xFFFFFFFFll, DV_ERR_FORMAT, "DuVi offsets are 32-bit");
+    std::vector<int64_t> row_blocks(n + 1, 0);
+#pragma omp parallel for schedule(static)
+    for (int32_t i = 0; i < n; ++i) {
+        int32_t from = a.rowptr[i], to = a.rowptr[i + 1];
+        int64_t nb = 0;
+        for (int32_t j = from; j < to; ++j) {
+            ++nb;
+            int cnt = 0;
+            for (; j + 1 < to && cnt < 255; ++j) {
+                if (a.col[j + 1] - a.col[j] - 1 < 256) ++cnt;
+                else break;
+            }
+        }
+        row_blocks[i + 1] = nb;
+    }
+    for (int32_t i = 0; i < n; ++i) row_blocks[i + 1] += row_blocks[i];
+    h.row_to_col.resize(n + 1);
+    h.row_to_dist.resize(n + 1);
+    h.col_idx.resize(row_blocks[n]);
+    h.dist.assign(nnz, 0);
+#pragma omp parallel for schedule(static)
+    for (int32_t i = 0; i <= n; ++i) {
+        h.row_to_col[i] = (uint32_t)row_blocks[i];
+        h.row_to_dist[i] = (uint32_t)(i < n ? a.rowptr[i] : nnz);
+        if (i == n) continue;
+        int32_t from = a.rowptr[i], to = a.rowptr[i + 1];
+        int64_t b = row_blocks[i];
+        for (int32_t j = from; j < to; ++j) {
+            int64_t begin = j;
+            int cnt = 0;
+            h.col_idx[b++] = (uint32_t)a.col[j];
+            for (; j + 1 < to && cnt < 255; ++j) {
+                int32_t diff = a.col[j + 1] - a.col[j] - 1;
+                if (diff < 256) { ++cnt; h.dist[j + 1] = (uint8_t)diff; }
+                else break;
+            }
+            h.dist[begin] = (uint8_t)cnt;
+        }
+    }
+    NetDoubleDict map(tol);
+    h.vidx.resize(nnz);
+    for (int64_t i = 0; i < nnz; ++i) h.vidx[i] = (uint32_t)map.find_or_insert(a.val[i]);
+    h.values = map.keys;
+    int64_t nu = (int64_t)h.values.size();
+    int bits = nu <= 256 ? 8 : (nu <= 65536 ? 16 : 32);
+    if (force_bits != 0) {
+        DV_REQUIRE(force_bits == 8 || force_bits == 16 || force_bits == 32, DV_ERR_ARG,
+                   "value_index_bits must be 0, 8, 16 or 32");
+        DV_REQUIRE(force_bits >= bits, DV_ERR_FORMAT, "too many distinct values for the requested index width");
+        bits = force_bits;
+    }
+    h.vi_bits = bits;
+}
+
+void dv_make_bundles(const DuviHost &h, int32_t n_rows, int vi_bits, std::vector<int32_t> &bundles) {
+    (void)vi_bits;
+    bundles.clear();
+    int32_t r = 0;
+    while (r < n_rows) {
+        bundles.push_back(r);
+        int32_t r1 = r + 1;
+        while (r1 < n_rows && r1 - r < kBundleRows) {
+            uint32_t bytes = h.row_to_dist[r1 + 1] - h.row_to_dist[r];
+            uint32_t blocks = h.row_to_col[r1 + 1] - h.row_to_col[r];
+            if (bytes > (uint32_t)kBundleBytes || blocks > (uint32_t)kBundleBlocks) break;
+            ++r1;
+        }
+        r = r1;
+    }
+    bundles.push_back(n_rows);
+}
+
+void dv_extract_diag(const dv_csr_host &a, std::vector<double> &d) {
+    d.assign(a.n_rows, 0.0);
+#pragma omp parallel for schedule(static)
+    for (int32_t i = 0; i < a.n_rows; ++i)
+        for (int32_t k = a.rowptr[i]; k < a.rowptr[i + 1]; ++k)
+            if (a.col[k] == i) d[i] = a.val[k];
+}
+
+double dv_row_ratio_bound(const dv_csr_host &a) {
+    double l = 0;
+    for (int32_t i = 0; i < a.n_rows; ++i) {
+        double s = 0.0, mx = 0.0;
+        for (int32_t k = a.rowptr[i]; k < a.rowptr[i + 1]; ++k) {
+            double v = std::fabs(a.val[k]);
+            s += v;
+            mx = std::max(mx, v);
+        }
+        if (mx > 0) l = std::max(l, s / mx);
+    }
+    return l;
+}
+
+// In-place inverse of a dense SPD matrix through A = L D L^T: factor, then
+// solve for the unit vectors (columns in parallel).
+bool dv_dense_inverse(int32_t n, std::vector<double> &a, double pivot_tol) {
+    std::vector<double> f = a;   // factor in place: strict lower L, diagonal D
+    std::vector<double> v(n);
+    for (int32_t j = 0; j < n; ++j) {
+        double d = f[(size_t)j * n + j];
+        for (int32_t k = 0; k < j; ++k) {
+            v[k] = f[(size_t)j * n + k] * f[(size_t)k * n + k];
+            d -= f[(size_t)j * n + k] * v[k];
+        }
+        if (!(std::fabs(d) >= pivot_tol)) return false;
+        f[(size_t)j * n + j] = d;
+#pragma omp parallel for schedule(static)
+        for (int32_t i = j + 1; i < n; ++i) {
+            double s = f[(size_t)i * n + j];
+            const double *fi = &f[(size_t)i * n];
+            for (int32_t k = 0; k < j; ++k) s -= fi[k] * v[k];
+            f[(size_t)i * n + j] = s / d;
+        }
+    }
+#pragma omp parallel for schedule(dynamic, 8)
+    for (int32_t c = 0; c < n; ++c) {
+        std::vector<double> x(n, 0.0);
+        x[c] = 1.0;
+        for (int32_t i = c + 1; i < n; ++i) {
+            double s = 0.0;
+            const double *fi = &f[(size_t)i * n];
+            for (int32_t k = c; k < i; ++k) s += fi[k] * x[k];
+            x[i] = -s;
+        }
+        for (int32_t i = 0; i < n; ++i) x[i] /= f[(size_t)i * n + i];
+        for (int32_t i = n - 1; i >= 0; --i) {
+            double s = x[i];
+            for (int32_t k = i + 1; k < n; ++k) s -= f[(size_t)k * n + i] * x[k];
+            x[i] = s;
+        }
+        for (int32_t i = 0; i < n; ++i) a[(size_t)i * n + c] = x[i];
+    }
+    return true;
+}
+
+int dv_block_coloring(const dv_csr_host &a, int bs, std::vector<int32_t> &color) {
+    int32_t nb = (a.n_rows + bs - 1) / bs;
+    color.assign(nb, -1);
+    std::vector<int32_t> mark;
+    int ncolors = 0;
+    for (int32_t b = 0; b < nb; ++b) {
+        mark.assign(ncolors + 1, 0);
+        for (int32_t r = b * bs; r < std::min<int32_t>((b + 1) * bs, a.n_rows); ++r)
+            for (int32_t k = a.rowptr[r]; k < a.rowptr[r + 1]; ++k) {
+                int32_t nbk = a.col[k] / bs;
+                if (nbk != b && color[nbk] >= 0) mark[color[nbk]] = 1;
+            }
+        int c = 0;
+        while (c < ncolors && mark[c]) ++c;
+        color[b] = c;
+        if (c == ncolors) ++ncolors;
+    }
+    return ncolors;
+}
+
+int dv_gs_level_sets(const dv_csr_host &a, std::vector<int32_t> &perm, std::vector<int32_t> &offsets) {
+    int32_t n = a.n_rows;
+    std::vector<int32_t> lev(n, 0);
+    int32_t maxl = 0;
+    for (int32_t i = 0; i < n; ++i) {
+        int32_t l = 0;
+        for (int32_t k = a.rowptr[i]; k < a.rowptr[i + 1]; ++k) {
+            int32_t j = a.col[k];
+            if (j < i) l = std::max(l, lev[j] + 1);
+        }
+        lev[i] = l;
+        maxl = std::max(maxl, l);
+    }
+    offsets.assign(maxl + 2, 0);
+    for (int32_t i = 0; i < n; ++i) offsets[lev[i] + 1]++;
+    for (int32_t l = 0; l <= maxl; ++l) offsets[l + 1] += offsets[l];
+    perm.resize(n);
+    std::vector<int32_t> fill(offsets.begin(), offsets.end() - 1);
+    for (int32_t i = 0; i < n; ++i) perm[fill[lev[i]]++] = i;
+    return maxl + 1;
+}
+
+// ---------------------------------------------------------------------------
+// structured hex workload generator
+// ---------------------------------------------------------------------------
+// Element stiffness of FemCantilever3D.cs:225-313 (top3d), row-major 24x24.
+static void hex_ke(double E, double v, double *ke) {
+    static const double A[2][14] = {{32, 6, -8, 6, -6, 4, 3, -6, -10, 3, -3, -3, -4, -8},
+                                    {-48, 0, 0, -24, 24, 0, 0, 0, 12, -12, 0, 12, 12, 12}};
+    double k[15];
+    k[0] = 0;
+    for (int i = 0; i < 14; ++i) {
+        double t = 0.0;
+        t += A[0][i] * 1.0;
+        t += A[1][i] * v;
+        k[i + 1] = t * (1.0 / 72.0);
+    }
+    static const int K[6][6][6] = {
+        {{1, 2, 2, 3, 5, 5}, {2, 1, 2, 4, 6, 7}, {2, 2, 1, 4, 7, 6}, {3, 4, 4, 1, 8, 8}, {5, 6, 7, 8, 1, 2}, {5, 7, 6, 8, 2, 1}},
+        {{9, 8, 12, 6, 4, 7}, {8, 9, 12, 5, 3, 5}, {10, 10, 13, 7, 4, 6}, {6, 5, 11, 9, 2, 10}, {4, 3, 5, 2, 9, 12}, {11, 4, 6, 12, 10, 13}},
+        {{6, 7, 4, 9, 12, 8}, {7, 6, 4, 10, 13, 10}, {5, 5, 3, 8, 12, 9}, {9, 10, 2, 6, 11, 5}, {12, 13, 10, 11, 6, 4}, {2, 12, 9, 4, 5, 3}},
+        {{14, 11, 11, 13, 10, 10}, {11, 14, 11, 12, 9, 8}, {11, 11, 14, 12, 8, 9}, {13, 12, 12, 14, 7, 7}, {10, 9, 8, 7, 14, 11}, {10, 8, 9, 7, 11, 14}},
+        {{1, 2, 8, 3, 5, 4}, {2, 1, 8, 4, 6, 11}, {8, 8, 1, 5, 11, 6}, {3, 4, 5, 1, 8, 2}, {5, 6, 11, 8, 1, 8}, {4, 11, 6, 2, 8, 1}},
+        {{14, 11, 7, 13, 10, 12}, {11, 14, 7, 12, 9, 2}, {7, 7, 14, 10, 2, 9}, {13, 12, 10, 14, 7, 11}, {10, 9, 2, 7, 14, 7}, {12, 2, 9, 11, 7, 14}}};
+    // block (bi,bj) -> (matrix id, transposed): {K1,K2,K3,K4; K2',K5,K6,K3'; K3',K6,K5',K2'; K4,K3,K2,K1'}
+    static const int id[4][4] = {{0, 1, 2, 3}, {1, 4, 5, 2}, {2, 5, 4, 1}, {3, 2, 1, 0}};
+    static const bool tr[4][4] = {{0, 0, 0, 0}, {1, 0, 0, 1}, {1, 0, 1, 1}, {0, 0, 0, 1}};
+    double f = E / ((v + 1) * (1 - 2 * v));
+    for (int bi = 0; bi < 4; ++bi)
+        for (int bj = 0; bj < 4; ++bj)
+            for (int i = 0; i < 6; ++i)
+                for (int j = 0; j < 6; ++j) {
+                    int m = tr[bi][bj] ? K[id[bi][bj]][j][i] : K[id[bi][bj]][i][j];
+                    ke[(bi * 6 + i) * 24 + bj * 6 + j] = k[m] * f;
+                }
+}
+
+static inline int32_t hex_row_nodes(int32_t i, int32_t j, int32_t k, int32_t nx, int32_t ny, int32_t nz) {
+    int ci = (i > 1 ? 1 : 0) + 1 + (i + 1 < nx ? 1 : 0);   // x neighbours among free nodes (x index >= 1)
+    int cj = (j > 0 ? 1 : 0) + 1 + (j + 1 < ny ? 1 : 0);
+    int ck = (k > 0 ? 1 : 0) + 1 + (k + 1 < nz ? 1 : 0);
+    return ci * cj * ck;
+}
+
+extern "C" DV_API int dv_hex_csr_size(const int32_t *ne, int32_t *n_rows, int64_t *nnz) {
+    return dv_guard([&] {
+        DV_REQUIRE(ne && ne[0] > 0 && ne[1] > 0 && ne[2] > 0, DV_ERR_ARG, "element counts must be positive");
+        int64_t nx = ne[0] + 1, ny = ne[1] + 1, nz = ne[2] + 1;
+        int64_t rows = 3 * (nx - 1) * ny * nz;
+        DV_REQUIRE(rows < INT32_MAX, DV_ERR_ARG, "mesh too large for int32 rows");
+        // nnz = 9 * (sum over x of free neighbours) * (sum over y) * (sum over z), separable
+        auto s1 = [](int64_t n, bool clamp) {
+            int64_t s = 0;
+            for (int64_t i = clamp ? 1 : 0; i < n; ++i)
+                s += (clamp ? (i > 1) : (i > 0)) + 1 + (i + 1 < n);
+            return s;
+        };
+        int64_t z = 9 * s1(nx, true) * s1(ny, false) * s1(nz, false);
+        DV_REQUIRE(z < INT32_MAX, DV_ERR_ARG, "nnz exceeds int32 offsets");
+        *n_rows = (int32_t)rows;
+        *nnz = z;
+    });
+}
+
+// Row-wise assembly; each entry sums its element contributions in increasing
+// element id, starting from 0.0 + first term, exactly as DokRowMajor.AddSubmatrix
+// accumulates (DokRowMajor.cs:182-207) when FemCantileverBase.AssembleGlobalMatrix
+// visits the elements in order (FemCantileverBase.cs:95-101).
+extern "C" DV_API int dv_hex_assemble(const int32_t *ne, const double *elem_E, double scale, double E, double nu,
+                                      int32_t *rowptr, int32_t *col, double *val) {
+    return dv_guard([&] {
+        int32_t nrows;
+        int64_t nnz;
+        int st = dv_hex_csr_size(ne, &nrows, &nnz);
+        DV_REQUIRE(st == DV_OK, st, "bad mesh");
+        DV_REQUIRE(rowptr && col && val, DV_ERR_ARG, "null output array");
+        double ke[576];
+        hex_ke(E, nu, ke);
+        const int32_t nx = ne[0] + 1, ny = ne[1] + 1, nz = ne[2] + 1;
+        auto fidx = [&](int32_t i, int32_t j, int32_t k) { return 3 * ((i - 1) + (nx - 1) * (j + ny * k)); };
+        // row offsets (plane by plane prefix)
+        rowptr[0] = 0;
+        {
+            int64_t p = 0;
+            for (int32_t k = 0; k < nz; ++k)
+                for (int32_t j = 0; j < ny; ++j)
+                    for (int32_t i = 1; i < nx; ++i) {
+                        int32_t c = 3 * hex_row_nodes(i, j, k, nx, ny, nz);
+                        int32_t r = fidx(i, j, k);
+                        for (int d = 0; d < 3; ++d) { p += c; rowptr[r + d + 1] = (int32_t)p; }
+                    }
+        }
+        static const int vtk[8] = {0, 1, 3, 2, 4, 5, 7, 6};
+#pragma omp parallel for collapse(2) schedule(dynamic, 4)
+        for (int32_t k = 0; k < nz; ++k)
+            for (int32_t j = 0; j < ny; ++j)
+                for (int32_t i = 1; i < nx; ++i) {
+                    int32_t r0 = fidx(i, j, k);
+                    for (int d = 0; d < 3; ++d) {
+                        int64_t p = rowptr[r0 + d];
+                        for (int dk = -1; dk <= 1; ++dk)
+                            for (int dj = -1; dj <= 1; ++dj)
+                                for (int di = -1; di <= 1; ++di) {
+                                    int32_t ii = i + di, jj = j + dj, kk = k + dk;
+                                    if (ii < 1 || ii >= nx || jj < 0 || jj >= ny || kk < 0 || kk >= nz) continue;
+                                    int32_t c0 = std::max(std::max(k, kk) - 1, 0), c1 = std::min(std::min(k, kk), ne[2] - 1);
+                                    int32_t b0 = std::max(std::max(j, jj) - 1, 0), b1 = std::min(std::min(j, jj), ne[1] - 1);
+                                    int32_t a0 = std::max(std::max(i, ii) - 1, 0), a1 = std::min(std::min(i, ii), ne[0] - 1);
+                                    int32_t cbase = fidx(ii, jj, kk);
+                                    for (int d2 = 0; d2 < 3; ++d2) {
+                                        double s = 0.0;
+                                        bool first = true;
+                                        for (int32_t c = c0; c <= c1; ++c)
+                                            for (int32_t b = b0; b <= b1; ++b)
+                                                for (int32_t a = a0; a <= a1; ++a) {
+                                                    int64_t e = a + (int64_t)ne[0] * (b + (int64_t)ne[1] * c);
+                                                    int la = vtk[(i - a) + 2 * (j - b) + 4 * (k - c)];
+                                                    int lb = vtk[(ii - a) + 2 * (jj - b) + 4 * (kk - c)];
+                                                    double ce = elem_E ? scale * elem_E[e] : scale;
+                                                    double t = ce * ke[(3 * la + d) * 24 + 3 * lb + d2];
+                                                    if (first) { s = t + 0.0; first = false; }
+                                                    else s = t + s;
+                                                }
+                                        col[p] = cbase + d2;
+                                        val[p] = s;
+                                        ++p;
+                                    }
+                                }
+                    }
+                }
+    });
+}
+
+extern "C" DV_API int dv_hex_trilinear_size(const int32_t *nef, int32_t *n_rows, int32_t *n_cols, int64_t *nnz) {
+    return dv_guard([&] {
+        DV_REQUIRE(nef && nef[0] >= 2 && nef[1] >= 2 && nef[2] >= 2 && nef[0] % 2 == 0 && nef[1] % 2 == 0 &&
+                       nef[2] % 2 == 0, DV_ERR_ARG, "trilinear transfer needs even element counts");
+        int64_t nx = nef[0] + 1, ny = nef[1] + 1, nz = nef[2] + 1;
+        int64_t cx = nef[0] / 2 + 1, cy = nef[1] / 2 + 1, cz = nef[2] / 2 + 1;
+        int64_t sx = 0, sy = 0, sz = 0;
+        for (int64_t i = 1; i < nx; ++i) sx += (i & 1) ? ((i / 2 == 0) ? 1 : 2) : 1;   // coarse x=0 is clamped
+        for (int64_t j = 0; j < ny; ++j) sy += (j & 1) ? 2 : 1;
+        for (int64_t k = 0; k < nz; ++k) sz += (k & 1) ? 2 : 1;
+        *n_rows = (int32_t)(3 * (nx - 1) * ny * nz);
+        *n_cols = (int32_t)(3 * (cx - 1) * cy * cz);
+        *nnz = 3 * sx * sy * sz;
+    });
+}
+
+extern "C" DV_API int dv_hex_trilinear(const int32_t *nef, int32_t *rowptr, int32_t *col, double *val) {
+    return dv_guard([&] {
+        int32_t nr, nc;
+        int64_t nnz;
+        int st = dv_hex_trilinear_size(nef, &nr, &nc, &nnz);
+        DV_REQUIRE(st == DV_OK, st, "bad mesh");
+        int32_t nx = nef[0] + 1, ny = nef[1] + 1, nz = nef[2] + 1;
+        int32_t cx = nef[0] / 2 + 1, cy = nef[1] / 2 + 1;
+        int64_t p = 0;
+        int32_t r = 0;
+        rowptr[0] = 0;
+        for (int32_t k = 0; k < nz; ++k)
+            for (int32_t j = 0; j < ny; ++j)
+                for (int32_t i = 1; i < nx; ++i)
+                    for (int d = 0; d < 3; ++d) {
+                        int ni = (i & 1) ? 2 : 1, nj = (j & 1) ? 2 : 1, nk = (k & 1) ? 2 : 1;
+                        int32_t ci[2] = {i / 2, i / 2 + 1}, cj[2] = {j / 2, j / 2 + 1}, ck[2] = {k / 2, k / 2 + 1};
+                        double wi[2] = {ni == 2 ? 0.5 : 1.0, 0.5}, wj[2] = {nj == 2 ? 0.5 : 1.0, 0.5},
+                               wk[2] = {nk == 2 ? 0.5 : 1.0, 0.5};
+                        for (int c = 0; c < nk; ++c)
+                            for (int b = 0; b < nj; ++b)
+                                for (int a = 0; a < ni; ++a) {
+                                    if (ci[a] == 0) continue;
+                                    col[p] = 3 * ((ci[a] - 1) + (cx - 1) * (cj[b] + cy * ck[c])) + d;
+                                    val[p] = wi[a] * wj[b] * wk[c];
+                                    ++p;
+                                }
+                        rowptr[++r] = (int32_t)p;
+                    }
+        DV_REQUIRE(p == nnz && r == nr, DV_ERR_ARG, "internal size mismatch");
+    });
+}
+
+// Power-method bound of D^-1 A (GeometricMultigridSolver.cs:80-103): iterate
+// until the growth ratio is within 5 %, then extrapolate.
+double dv_power_bound_ref(const dv_csr_host &a, const std::vector<double> &inv_diag) {
+    const double percent = 0.05;
+    const int32_t n = a.n_rows;
+    std::vector<double> x(n, 1 / std::sqrt((double)n)), y(n);
+    double l = 1;
+    for (int it = 0; it < 100000; ++it) {
+#pragma omp parallel for schedule(static)
+        for (int32_t i = 0; i < n; ++i) {
+            double s = 0.0;
+            for (int32_t k = a.rowptr[i]; k < a.rowptr[i + 1]; ++k) s += a.val[k] * x[a.col[k]];
+            y[i] = s * inv_diag[i];
+        }
+        double l2 = 0.0;
+        for (int32_t i = 0; i < n; ++i) l2 += y[i] * y[i];
+        l2 = std::sqrt(l2);
+        const double sc = 1 / l2;
+        for (int32_t i = 0; i < n; ++i) x[i] = y[i] * sc;
+        const double ratio = l2 / l;
+        if (ratio > 1 - percent && ratio < 1 + percent) {
+            return ratio > 1 ? l2 * std::pow(ratio, 1 / std::sqrt(percent)) : (l2 * 9 + l) / 10;
+        }
+        l = l2;
+    }
+    return l;
+}
+
+// ---------------------------------------------------------------------------
+// Restriction / interpolation of structured Cartesian meshes
+// (IGeometricMultigridModel.cs:76-194): radial influence 1 - |(w - c)/h| of
+// the fine nodes in a window around each coarse node, restriction rows and
+// interpolation rows normalised to sum 1 before the fixed dofs are removed,
+// the same weight for every dof of a node, free-dof submatrices.
+// ---------------------------------------------------------------------------
+namespace {
+struct TransferBuild {
+    std::vector<std::vector<std::pair<int32_t, double>>> R, P;   // free rows: (free col, value)
+};
+void build_transfer(int dim, const int32_t *nef, const int32_t *nec, int dpn, int32_t nff, const int32_t *ff,
+                    int32_t ncf, const int32_t *cf, TransferBuild &out) {
+    DV_REQUIRE(dim == 2 || dim == 3, DV_ERR_ARG, "dim must be 2 or 3");
+    DV_REQUIRE(dpn >= 1, DV_ERR_ARG, "dofs per node must be positive");
+    int nfn[3] = {1, 1, 1}, ncn[3] = {1, 1, 1};
+    double dist[3] = {0, 0, 0};
+    for (int i = 0; i < dim; ++i) {
+        DV_REQUIRE(nef[i] >= 1 && nec[i] >= 1, DV_ERR_ARG, "element counts must be positive");
+        dist[i] = (double)nef[i] / nec[i];
+        nfn[i] = nef[i] + 1;
+        ncn[i] = nec[i] + 1;
+    }
+    const int64_t nf_nodes = (int64_t)nfn[0] * nfn[1] * nfn[2], nc_nodes = (int64_t)ncn[0] * ncn[1] * ncn[2];
+    std::vector<int32_t> fmap(nf_nodes * dpn, -1), cmap(nc_nodes * dpn, -1);
+    for (int32_t i = 0; i < nff; ++i) {
+        DV_REQUIRE(ff[i] >= 0 && ff[i] < nf_nodes * dpn, DV_ERR_ARG, "fine free dof out of range");
+        fmap[ff[i]] = i;
+    }
+    for (int32_t i = 0; i < ncf; ++i) {
+        DV_REQUIRE(cf[i] >= 0 && cf[i] < nc_nodes * dpn, DV_ERR_ARG, "coarse free dof out of range");
+        cmap[cf[i]] = i;
+    }
+    struct Tri { int32_t c, f; double v; };
+    std::vector<Tri> tris;
+    std::vector<double> sum_r(nc_nodes, 0.0), sum_i(nf_nodes, 0.0);
+    int a[3] = {0, 0, 0}, start[3] = {0, 0, 0}, end[3] = {0, 0, 0}, w[3] = {0, 0, 0};
+    double cursor[3] = {0, 0, 0};
+    if (dim < 3) end[2] = 1;
+    for (a[0] = 0; a[0] < ncn[0]; ++a[0])
+        for (a[2] = 0; a[2] < ncn[2]; ++a[2])
+            for (a[1] = 0; a[1] < ncn[1]; ++a[1]) {
+                for (int i = 0; i < dim; ++i) {
+                    cursor[i] = a[i] * dist[i];
+                    start[i] = (int)std::ceil(std::nextafter(cursor[i] - dist[i], INFINITY));
+                    if (start[i] < 0) start[i] = 0;
+                    end[i] = (int)std::floor(std::nextafter(cursor[i] + dist[i], -INFINITY)) + 1;
+                    if (end[i] > nfn[i]) end[i] = nfn[i];
+                }
+                int32_t cnode = a[0] + a[1] * ncn[0] + (dim == 3 ? a[2] * ncn[0] * ncn[1] : 0);
+                double s = 0;
+                for (w[0] = start[0]; w[0] < end[0]; ++w[0])
+                    for (w[2] = start[2]; w[2] < end[2]; ++w[2])
+                        for (w[1] = start[1]; w[1] < end[1]; ++w[1]) {
+                            int32_t fnode = w[0] + w[1] * nfn[0] + (dim == 3 ? w[2] * nfn[0] * nfn[1] : 0);
+                            double infl = 0;
+                            for (int i = 0; i < dim; ++i) {
+                                double d0 = (w[i] - cursor[i]) / dist[i];
+                                infl += d0 * d0;
+                            }
+                            infl = 1 - std::sqrt(infl);
+                            s += infl;
+                            sum_i[fnode] += infl;
+                            tris.push_back({cnode, fnode, infl});
+                        }
+                sum_r[cnode] = s;
+            }
+    out.R.assign(ncf, {});
+    out.P.assign(nff, {});
+    for (const Tri &t : tris) {
+        double rv = t.v / sum_r[t.c], pv = t.v / sum_i[t.f];
+        for (int d = 0; d < dpn; ++d) {
+            int32_t cr = cmap[(int64_t)t.c * dpn + d], fr = fmap[(int64_t)t.f * dpn + d];
+            if (cr >= 0 && fr >= 0) {
+                out.R[cr].push_back({fr, rv});
+                out.P[fr].push_back({cr, pv});
+            }
+        }
+    }
+    for (auto &row : out.R) std::sort(row.begin(), row.end(), [](auto &x, auto &y) { return x.first < y.first; });
+    for (auto &row : out.P) std::sort(row.begin(), row.end(), [](auto &x, auto &y) { return x.first < y.first; });
+}
+}  // namespace
+
+extern "C" DV_API int dv_cartesian_transfer_size(int32_t dim, const int32_t *ne_fine, const int32_t *ne_coarse,
+                                                 int32_t dofs_per_node, int32_t n_fine_free, const int32_t *fine_free,
+                                                 int32_t n_coarse_free, const int32_t *coarse_free, int64_t *nnz_r,
+                                                 int64_t *nnz_p) {
+    return dv_guard([&] {
+        DV_REQUIRE(ne_fine && ne_coarse && fine_free && coarse_free && nnz_r && nnz_p, DV_ERR_ARG, "null argument");
+        TransferBuild t;
+        build_transfer(dim, ne_fine, ne_coarse, dofs_per_node, n_fine_free, fine_free, n_coarse_free, coarse_free, t);
+        int64_t r = 0, p = 0;
+        for (auto &row : t.R) r += (int64_t)row.size();
+        for (auto &row : t.P) p += (int64_t)row.size();
+        *nnz_r = r;
+        *nnz_p = p;
+    });
+}
+
+extern "C" DV_API int dv_cartesian_transfer(int32_t dim, const int32_t *ne_fine, const int32_t *ne_coarse,
+                                            int32_t dofs_per_node, int32_t n_fine_free, const int32_t *fine_free,
+                                            int32_t n_coarse_free, const int32_t *coarse_free, int32_t *r_rowptr,
+                                            int32_t *r_col, double *r_val, int32_t *p_rowptr, int32_t *p_col,
+                                            double *p_val) {
+    return dv_guard([&] {
+        DV_REQUIRE(ne_fine && ne_coarse && fine_free && coarse_free && r_rowptr && r_col && r_val && p_rowptr &&
+                       p_col && p_val, DV_ERR_ARG, "null argument");
+        TransferBuild t;
+        build_transfer(dim, ne_fine, ne_coarse, dofs_per_node, n_fine_free, fine_free, n_coarse_free, coarse_free, t);
+        auto emit = [](const std::vector<std::vector<std::pair<int32_t, double>>> &rows, int32_t *rp, int32_t *ci, double *va) {
+            int64_t k = 0;
+            rp[0] = 0;
+            for (size_t i = 0; i < rows.size(); ++i) {
+                for (auto &cv : rows[i]) { ci[k] = cv.first; va[k] = cv.second; ++k; }
+                rp[i + 1] = (int32_t)k;
+            }
+        };
+        emit(t.R, r_rowptr, r_col, r_val);
+        emit(t.P, p_rowptr, p_col, p_val);
+    });
+}

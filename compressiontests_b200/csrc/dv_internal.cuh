@@ -1,0 +1,161 @@
+// Internal declarations of libduvigpu.so (B200 sparse solver path).
+#pragma once
+
+#include "../../include/duvi_gpu.h"
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+struct DvError : std::runtime_error {
+    int code;
+    DvError(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+
+#define DV_CUDA(call)                                                                          \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess)                                                                 \
+            throw DvError(e_ == cudaErrorMemoryAllocation ? DV_ERR_NOMEM : DV_ERR_CUDA,        \
+                          std::string(#call) + ": " + cudaGetErrorString(e_));                 \
+    } while (0)
+
+#define DV_REQUIRE(cond, code, msg)                   \
+    do {                                              \
+        if (!(cond)) throw DvError((code), (msg));    \
+    } while (0)
+
+void dv_set_last_error(const std::string &m);
+
+// Runs f, converting exceptions into status codes and the thread-local message.
+template <class F>
+int dv_guard(F &&f) {
+    try {
+        f();
+        return DV_OK;
+    } catch (const DvError &e) {
+        dv_set_last_error(e.what());
+        return e.code;
+    } catch (const std::bad_alloc &) {
+        dv_set_last_error("host allocation failed");
+        return DV_ERR_NOMEM;
+    } catch (const std::exception &e) {
+        dv_set_last_error(e.what());
+        return DV_ERR_ARG;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// device memory
+// ---------------------------------------------------------------------------
+struct DevMem {
+    void *p = nullptr;
+    size_t bytes = 0;
+    DevMem() = default;
+    explicit DevMem(size_t b) { alloc(b); }
+    DevMem(const DevMem &) = delete;
+    DevMem &operator=(const DevMem &) = delete;
+    DevMem(DevMem &&o) noexcept : p(o.p), bytes(o.bytes) { o.p = nullptr; o.bytes = 0; }
+    DevMem &operator=(DevMem &&o) noexcept {
+        if (this != &o) { release(); p = o.p; bytes = o.bytes; o.p = nullptr; o.bytes = 0; }
+        return *this;
+    }
+    ~DevMem() { release(); }
+    void alloc(size_t b) {
+        release();
+        // 64 bytes of tail padding: staged loads round ranges up to 16-byte units.
+        if (b) DV_CUDA(cudaMalloc(&p, b + 64));
+        if (b) DV_CUDA(cudaMemset(p, 0, b + 64));
+        bytes = b;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    template <class T> T *as() const { return static_cast<T *>(p); }
+};
+
+// Grid-wide deterministic reduction workspace: per-block partials and a ticket.
+struct ReduceWs {
+    double *partials = nullptr;   // [max_blocks * 8]
+    unsigned *ticket = nullptr;
+};
+
+// ---------------------------------------------------------------------------
+// context
+// ---------------------------------------------------------------------------
+struct dv_context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int num_sms = 0;
+    int max_smem_optin = 0;
+    int64_t launches = 0;
+    DevMem status;       // int[4]: device error word, bounded-wait sentinel
+    void count(int64_t n = 1) { launches += n; }
+};
+
+void dv_ctx_check(dv_context *ctx);   // throws DV_ERR_NO_DEVICE / DV_ERR_CUDA
+
+// ---------------------------------------------------------------------------
+// matrices
+// ---------------------------------------------------------------------------
+struct DuviHost {   // host copy of the SoA encoding (export / parity)
+    std::vector<uint32_t> row_to_col, row_to_dist, col_idx, vidx;
+    std::vector<uint8_t> dist;
+    std::vector<double> values;
+    int vi_bits = 8;
+};
+
+struct dv_matrix {
+    dv_context *ctx = nullptr;
+    int32_t n_rows = 0, n_cols = 0;
+    int64_t nnz = 0;
+    int format = DV_FORMAT_CSR;
+    int precision = DV_F64;
+    // CSR
+    DevMem rowptr, col, val;
+    int csr_tpr = 16;          // threads per row (autotuned)
+    // DuVi SoA
+    int vi_bits = 8;
+    int64_t nblocks = 0, nuniq = 0;
+    DevMem row_to_col, row_to_dist, col_idx, dist, vidx, values;
+    DevMem bundles;            // int32 row starts of row bundles (+ sentinel)
+    int32_t nbundles = 0;
+    DuviHost host;             // kept for export
+    // shared
+    DevMem diag;               // FP64 diagonal (0 where absent)
+    std::vector<double> host_diag;
+    int64_t device_bytes = 0;
+};
+
+// Row bundles for the staged DuVi kernel: at most kBundleRows rows and at most
+// kBundleBytes entry bytes / kBundleBlocks blocks (a longer single row forms its own bundle).
+constexpr int kBundleRows = 32;
+constexpr int kBundleBytes = 3008;    // entries (+ up to 32 bytes of 16-byte alignment slack)
+constexpr int kBundleBlocks = 480;    // block column starts (+ alignment slack)
+
+// Host helpers (dv_host.cpp)
+void dv_encode_duvi(const dv_csr_host &a, double tol, int force_bits, DuviHost &out);
+void dv_make_bundles(const DuviHost &h, int32_t n_rows, int vi_bits, std::vector<int32_t> &bundles);
+void dv_extract_diag(const dv_csr_host &a, std::vector<double> &diag);
+// Row-ratio bound max_i sum_j |a_ij| / max_j |a_ij| (GeometricMultigridSolver.cs:144-151).
+double dv_row_ratio_bound(const dv_csr_host &a);
+// Dense inverse of an SPD matrix via LDL^T (no pivoting); returns false on a tiny pivot.
+bool dv_dense_inverse(int32_t n, std::vector<double> &a, double pivot_tol);
+// Greedy coloring of node blocks (bs consecutive rows) for multicolor Gauss-Seidel.
+int dv_block_coloring(const dv_csr_host &a, int bs, std::vector<int32_t> &color_of_block);
+// Level sets of the forward Gauss-Seidel dependency graph (row i depends on j < i).
+int dv_gs_level_sets(const dv_csr_host &a, std::vector<int32_t> &perm, std::vector<int32_t> &offsets);
+
+// Matrix creation (dv_matrix.cu)
+dv_matrix *dv_matrix_build(dv_context *ctx, const dv_csr_host &a, int format, int precision,
+                           int vi_bits, double tol);

@@ -1,0 +1,542 @@
+// Device kernels of libduvigpu.so for sm_100a.
+//
+// The sparse path is HBM-bound integer/byte decode plus FMAs (about 0.1 flop
+// per byte), so there are no tensor-core tiles here: the kernels are built
+// around coalesced 16-byte staging of the index/byte streams into shared
+// memory, L2-resident gathers of the vector, warp-shuffle reductions and
+// epilogues that fuse the vector updates of each algorithm step into the
+// pass over the matrix.
+#pragma once
+
+#include "dv_internal.cuh"
+
+#include <cuda_runtime.h>
+
+namespace dvk {
+
+constexpr int kThreads = 256;            // CSR and vector kernels
+constexpr int kDuviWarps = 8;            // warps per block, staged DuVi kernel (8/16-bit indices)
+constexpr int kDuviWarps32 = 4;          // 32-bit value indices (larger stage)
+constexpr int kStageD = 3072;            // per-warp stage of entry bytes (>= kBundleBytes + 32)
+constexpr int kStageC = 512;             // per-warp stage of block column starts (>= kBundleBlocks + 8)
+constexpr int kMaxRed = 4;               // doubles per block in a grid reduction
+
+static_assert(kStageD >= kBundleBytes + 32, "stage too small");
+static_assert(kStageC >= kBundleBlocks + 8, "column stage too small");
+
+// ---------------------------------------------------------------------------
+// reductions
+// ---------------------------------------------------------------------------
+template <class T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+// Sum over aligned groups of W lanes (all lanes of a group must be converged).
+template <int W, class T>
+__device__ __forceinline__ T group_sum(T v) {
+    if constexpr (W == 1) {
+        return v;
+    } else {
+        const unsigned lane = threadIdx.x & 31u;
+        const unsigned mask = (W == 32) ? 0xffffffffu : (((1u << W) - 1u) << (lane & ~(unsigned)(W - 1)));
+#pragma unroll
+        for (int o = W / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o);
+        return v;
+    }
+}
+
+// Block reduction of N doubles: bit i of MAXMASK selects max instead of sum.
+// Result valid in thread 0.  All threads of the block must call it.
+template <int N, unsigned MAXMASK>
+__device__ void block_reduce(double (&v)[N]) {
+    __shared__ double sh[kMaxRed][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+        double t = ((MAXMASK >> i) & 1u) ? warp_max(v[i]) : warp_sum(v[i]);
+        if (lane == 0) sh[i][warp] = t;
+    }
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+            double t = lane < nw ? sh[i][lane] : 0.0;
+            v[i] = ((MAXMASK >> i) & 1u) ? warp_max(t) : warp_sum(t);
+        }
+    }
+    __syncthreads();
+}
+
+// Deterministic grid reduction: per-block partials, then the last block to
+// arrive sums them in block order.  Returns true in thread 0 of the last block,
+// with the totals in out.  Resets the ticket for the next launch.
+template <int N, unsigned MAXMASK>
+__device__ bool grid_reduce(double (&v)[N], double *partials, unsigned *ticket, double (&out)[N]) {
+    block_reduce<N, MAXMASK>(v);
+    __shared__ int is_last;
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int i = 0; i < N; ++i) partials[(size_t)blockIdx.x * N + i] = v[i];
+        __threadfence();
+        unsigned t = atomicAdd(ticket, 1u);
+        is_last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!is_last) return false;
+    __threadfence();
+    double acc[N];
+#pragma unroll
+    for (int i = 0; i < N; ++i) acc[i] = 0.0;
+    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x)
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+            double p = __ldcg(partials + (size_t)b * N + i);
+            acc[i] = ((MAXMASK >> i) & 1u) ? fmax(acc[i], p) : acc[i] + p;
+        }
+    block_reduce<N, MAXMASK>(acc);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int i = 0; i < N; ++i) out[i] = acc[i];
+        *ticket = 0;
+        return true;
+    }
+    return false;
+}
+
+// ---------------------------------------------------------------------------
+// gathers: value of the vector at a column (the x of y = A x)
+// ---------------------------------------------------------------------------
+template <class XT, class AT>
+struct GatherVec {
+    const XT *__restrict__ x;
+    __device__ __forceinline__ AT operator()(uint32_t c) const { return (AT)__ldg(x + c); }
+};
+// x = w .* b on the fly: the first Jacobi sweep from a zero guess fused into the second.
+template <class T>
+struct GatherWB {
+    const T *__restrict__ w;
+    const T *__restrict__ b;
+    __device__ __forceinline__ T operator()(uint32_t c) const { return __ldg(w + c) * __ldg(b + c); }
+};
+
+// Multiply-add policy: FP64 paths round the product and the sum separately
+// (bit-identical to the reference's sequential kernels and to the .NET CPU
+// code); FP32 V-cycle paths contract to FMA.
+template <class AT>
+__device__ __forceinline__ AT madd(AT acc, AT a, AT b);
+template <>
+__device__ __forceinline__ double madd<double>(double acc, double a, double b) { return __dadd_rn(acc, __dmul_rn(a, b)); }
+template <>
+__device__ __forceinline__ float madd<float>(float acc, float a, float b) { return fmaf(a, b, acc); }
+
+// ---------------------------------------------------------------------------
+// epilogues (row operators).  Each has NRED reduction slots and MAXMASK.
+// ---------------------------------------------------------------------------
+struct NoRed {
+    static constexpr int NRED = 0;
+    static constexpr unsigned MAXMASK = 0;
+    __device__ void finish(const double *) const {}
+};
+
+// y = A x (clear) or y += A x, accumulating onto the old y in entry order.
+template <class YT, class AT>
+struct OpSpmv : NoRed {
+    YT *__restrict__ y;
+    int clear;
+    __device__ __forceinline__ AT init(int32_t r) const { return clear ? AT(0) : (AT)y[r]; }
+    __device__ __forceinline__ void row(int32_t r, AT s, double *) const { y[r] = (YT)s; }
+};
+
+// r = b - A x
+template <class T>
+struct OpResid : NoRed {
+    const T *__restrict__ b;
+    T *__restrict__ r;
+    __device__ __forceinline__ T init(int32_t) const { return T(0); }
+    __device__ __forceinline__ void row(int32_t i, T s, double *) const { r[i] = b[i] - s; }
+};
+
+// y = x + w .* (b - A x)  (jacobi_iteration, CsrGeometricMultigrid.cl:176-194)
+template <class T>
+struct OpJacobi : NoRed {
+    const T *__restrict__ x;
+    const T *__restrict__ w;
+    const T *__restrict__ b;
+    T *__restrict__ y;
+    __device__ __forceinline__ T init(int32_t) const { return T(0); }
+    __device__ __forceinline__ void row(int32_t i, T s, double *) const { y[i] = x[i] + w[i] * (b[i] - s); }
+};
+// Second sweep from a zero guess: x1 = w .* b, y = x1 + w .* (b - A x1).
+template <class T>
+struct OpJacobiFromZero : NoRed {
+    const T *__restrict__ w;
+    const T *__restrict__ b;
+    T *__restrict__ y;
+    __device__ __forceinline__ T init(int32_t) const { return T(0); }
+    __device__ __forceinline__ void row(int32_t i, T s, double *) const {
+        T wi = w[i], bi = b[i];
+        y[i] = wi * bi + wi * (bi - s);
+    }
+};
+
+// Device scalars shared by the solver kernels of one solve.
+struct SolverScalars {
+    double rz, rz_new, pap, alpha, beta;   // Jacobi PCG
+    double zr, zq, pq;                     // flexible CG
+    double rr, bb, tol2, res_max, res_norm2;
+    int it, max_it, done, converged, failed, restart, cycle, pad;
+};
+
+// PCG: Ap = A p and p.Ap; alpha = rz / pAp (dot_finalize_and_calc_a, CsrCG.cl:223-241).
+struct OpPcgAp {
+    static constexpr int NRED = 1;
+    static constexpr unsigned MAXMASK = 0;
+    const double *__restrict__ p;
+    double *__restrict__ ap;
+    SolverScalars *sc;
+    __device__ __forceinline__ double init(int32_t) const { return 0.0; }
+    __device__ __forceinline__ void row(int32_t i, double s, double *red) const {
+        ap[i] = s;
+        red[0] = __dadd_rn(red[0], __dmul_rn(p[i], s));
+    }
+    __device__ void finish(const double *t) const {
+        sc->pap = t[0];
+        sc->alpha = sc->rz / t[0];
+    }
+};
+
+// Flexible CG outer product: s = (A z)_i, q = s + beta q, p = z + beta p, p.q.
+template <class ZT>
+struct OpFcg {
+    static constexpr int NRED = 1;
+    static constexpr unsigned MAXMASK = 0;
+    const ZT *__restrict__ z;
+    double *__restrict__ p;
+    double *__restrict__ q;
+    SolverScalars *sc;
+    double beta;   // unused placeholder: beta is read from sc in row()
+    __device__ __forceinline__ double init(int32_t) const { return 0.0; }
+    __device__ __forceinline__ void row(int32_t i, double s, double *red) const {
+        double bt = sc->beta;
+        double qi = s + bt * q[i];
+        double pi = (double)z[i] + bt * p[i];
+        q[i] = qi;
+        p[i] = pi;
+        red[0] += pi * qi;
+    }
+    __device__ void finish(const double *t) const {
+        sc->pq = t[0];
+        sc->alpha = sc->zr / t[0];
+    }
+};
+
+// r = b - A x with the max-norm / NaN check of residual_with_check
+// (CsrGeometricMultigrid.cl:121-141): converged when all |r_i| <= tol, failed
+// on NaN or |r_i| > 1e50.  Also ||r||^2.  The last block updates the cycle
+// counter and the stop decision of the V-cycle driver.
+struct OpResidCheck {
+    static constexpr int NRED = 3;
+    static constexpr unsigned MAXMASK = 0b011;
+    const double *__restrict__ b;
+    double *__restrict__ r;
+    SolverScalars *sc;
+    double tol;
+    __device__ __forceinline__ double init(int32_t) const { return 0.0; }
+    __device__ __forceinline__ void row(int32_t i, double s, double *red) const {
+        double ri = __dsub_rn(b[i], s);
+        r[i] = ri;
+        double c = fabs(ri);
+        if (isnan(ri) || c > 1e50) red[1] = 1.0;
+        else red[0] = fmax(red[0], c);
+        red[2] += ri * ri;
+    }
+    __device__ void finish(const double *t) const {
+        bool failed = t[1] != 0.0;
+        bool converged = !failed && t[0] <= tol;
+        sc->res_max = t[0];
+        sc->res_norm2 = sqrt(t[2]);
+        sc->converged = converged;
+        sc->failed = failed;
+        if (converged || failed || sc->cycle > sc->max_it) sc->done = 1;
+        else sc->cycle += 1;
+    }
+};
+
+// ---------------------------------------------------------------------------
+// CSR row kernel: TPR threads per row, grid-stride over rows
+// ---------------------------------------------------------------------------
+template <int TPR, class MT, class AT, class Gather, class Op>
+__global__ void __launch_bounds__(kThreads) k_csr(const int32_t *__restrict__ rp, const int32_t *__restrict__ ci,
+                                                  const MT *__restrict__ va, int32_t n, Gather g, Op op,
+                                                  const int *__restrict__ done, double *partials, unsigned *ticket) {
+    if (done && *(volatile const int *)done) return;
+    double red[Op::NRED > 0 ? Op::NRED : 1];
+#pragma unroll
+    for (int i = 0; i < (Op::NRED > 0 ? Op::NRED : 1); ++i) red[i] = 0.0;
+    const int sub = threadIdx.x % TPR;
+    const int gpb = kThreads / TPR;
+    for (int32_t row = blockIdx.x * gpb + threadIdx.x / TPR; row < n; row += gridDim.x * gpb) {
+        const int32_t s0 = __ldg(rp + row), s1 = __ldg(rp + row + 1);
+        AT s = (TPR == 1) ? op.init(row) : AT(0);
+#pragma unroll 4
+        for (int32_t k = s0 + sub; k < s1; k += TPR) s = madd<AT>(s, (AT)__ldg(va + k), g((uint32_t)__ldg(ci + k)));
+        s = group_sum<TPR>(s);
+        if (TPR > 1) s = op.init(row) + s;
+        if (sub == 0) op.row(row, s, red);
+    }
+    if constexpr (Op::NRED > 0) {
+        double tot[Op::NRED];
+        if (grid_reduce<Op::NRED, Op::MAXMASK>(red, partials, ticket, tot)) op.finish(tot);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// DuVi row-bundle kernel
+//
+// One warp per bundle of <= 32 consecutive rows.  The warp copies the
+// bundle's entry bytes (Distances), value indices and block column starts into
+// its shared-memory stage with 16-byte loads (ranges widened to 16-byte
+// boundaries; device arrays carry tail padding), then each lane walks one row
+// of the stage in the order of DuViGeometricMultigrid.cl:84-98.  Tables of at
+// most 256 distinct values are staged per block.
+// ---------------------------------------------------------------------------
+struct DuviArgs {
+    const uint32_t *__restrict__ row_to_col;
+    const uint32_t *__restrict__ row_to_dist;
+    const uint32_t *__restrict__ col_idx;
+    const uint8_t *__restrict__ dist;
+    const void *__restrict__ vidx;
+    const void *__restrict__ values;
+    const int32_t *__restrict__ bundles;
+    int32_t nbundles;
+    int32_t nuniq;
+};
+
+template <class VI>
+__device__ __forceinline__ void copy16(void *dst, const void *src, int nbytes16, int lane) {
+    const uint4 *s = static_cast<const uint4 *>(src);
+    uint4 *d = static_cast<uint4 *>(dst);
+    for (int i = lane; i < nbytes16; i += 32) d[i] = __ldg(s + i);
+}
+
+template <class VI, class AT, class Gather, class Op, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) k_duvi(DuviArgs A, Gather g, Op op, const int *__restrict__ done,
+                                                     double *partials, unsigned *ticket) {
+    if (done && *(volatile const int *)done) return;
+    extern __shared__ __align__(16) unsigned char smem[];
+    constexpr bool kSmemTable = sizeof(VI) == 1;
+    AT *tab = reinterpret_cast<AT *>(smem);
+    unsigned char *wbase = smem + (kSmemTable ? 256 * sizeof(AT) : 0);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned char *sdist = wbase + (size_t)warp * (kStageD + kStageD * sizeof(VI) + kStageC * 4);
+    VI *svi = reinterpret_cast<VI *>(sdist + kStageD);
+    uint32_t *scol = reinterpret_cast<uint32_t *>(sdist + kStageD + kStageD * sizeof(VI));
+    const AT *gtab = static_cast<const AT *>(A.values);
+    const VI *gvi = static_cast<const VI *>(A.vidx);
+    if (kSmemTable) {
+        for (int i = threadIdx.x; i < A.nuniq; i += blockDim.x) tab[i] = gtab[i];
+        __syncthreads();
+    }
+    double red[Op::NRED > 0 ? Op::NRED : 1];
+#pragma unroll
+    for (int i = 0; i < (Op::NRED > 0 ? Op::NRED : 1); ++i) red[i] = 0.0;
+
+    for (int32_t bi = blockIdx.x * WARPS + warp; bi < A.nbundles; bi += gridDim.x * WARPS) {
+        const int32_t r0 = __ldg(A.bundles + bi), r1 = __ldg(A.bundles + bi + 1);
+        const int32_t rl = min(r0 + lane, r1);
+        const uint32_t rd_l = __ldg(A.row_to_dist + rl), rc_l = __ldg(A.row_to_col + rl);
+        const uint32_t d0 = __shfl_sync(0xffffffffu, rd_l, 0), c0 = __shfl_sync(0xffffffffu, rc_l, 0);
+        const uint32_t d1 = __ldg(A.row_to_dist + r1), c1 = __ldg(A.row_to_col + r1);
+        const int32_t row = r0 + lane;
+        if (d1 - d0 <= (uint32_t)kBundleBytes && c1 - c0 <= (uint32_t)kBundleBlocks) {
+            // stage
+            const uint32_t a0 = d0 & ~15u;
+            const int nd16 = (int)((d1 - a0 + 15u) >> 4);
+            copy16<VI>(sdist, A.dist + a0, nd16, lane);
+            const uint64_t vb0 = ((uint64_t)d0 * sizeof(VI)) & ~(uint64_t)15;
+            const int nv16 = (int)(((uint64_t)d1 * sizeof(VI) - vb0 + 15u) >> 4);
+            copy16<VI>(svi, reinterpret_cast<const unsigned char *>(gvi) + vb0, nv16, lane);
+            const uint32_t ca0 = c0 & ~3u;
+            const int nc16 = (int)((c1 - ca0 + 3u) >> 2);
+            copy16<VI>(scol, A.col_idx + ca0, nc16, lane);
+            __syncwarp();
+            if (row < r1) {
+                uint32_t di = rd_l - a0;
+                uint32_t dv = rd_l - (uint32_t)(vb0 / sizeof(VI));
+                const uint32_t b_end = __ldg(A.row_to_col + row + 1) - ca0;
+                AT s = op.init(row);
+                for (uint32_t b = rc_l - ca0; b < b_end; ++b) {
+                    uint32_t c = scol[b];
+                    int cnt = sdist[di];
+                    AT v = kSmemTable ? tab[svi[dv]] : __ldg(gtab + svi[dv]);
+                    s = madd<AT>(s, v, g(c));
+                    for (int k = 0; k < cnt; ++k) {
+                        ++di;
+                        ++dv;
+                        c += sdist[di] + 1u;
+                        v = kSmemTable ? tab[svi[dv]] : __ldg(gtab + svi[dv]);
+                        s = madd<AT>(s, v, g(c));
+                    }
+                    ++di;
+                    ++dv;
+                }
+                op.row(row, s, red);
+            }
+            __syncwarp();
+        } else if (lane == 0) {
+            // a row longer than the stage: walk it from global memory
+            for (int32_t rr = r0; rr < r1; ++rr) {
+                uint32_t di = __ldg(A.row_to_dist + rr);
+                const uint32_t be = __ldg(A.row_to_col + rr + 1);
+                AT s = op.init(rr);
+                for (uint32_t b = __ldg(A.row_to_col + rr); b < be; ++b) {
+                    uint32_t c = __ldg(A.col_idx + b);
+                    int cnt = __ldg(A.dist + di);
+                    s = madd<AT>(s, kSmemTable ? tab[__ldg(gvi + di)] : __ldg(gtab + __ldg(gvi + di)), g(c));
+                    for (int k = 0; k < cnt; ++k) {
+                        ++di;
+                        c += __ldg(A.dist + di) + 1u;
+                        s = madd<AT>(s, kSmemTable ? tab[__ldg(gvi + di)] : __ldg(gtab + __ldg(gvi + di)), g(c));
+                    }
+                    ++di;
+                }
+                op.row(rr, s, red);
+            }
+        }
+    }
+    if constexpr (Op::NRED > 0) {
+        double tot[Op::NRED];
+        if (grid_reduce<Op::NRED, Op::MAXMASK>(red, partials, ticket, tot)) op.finish(tot);
+    }
+}
+
+template <class VI, class AT>
+constexpr size_t duvi_smem_bytes(int warps) {
+    return (sizeof(VI) == 1 ? 256 * sizeof(AT) : 0) + (size_t)warps * (kStageD + kStageD * sizeof(VI) + kStageC * 4);
+}
+
+// ---------------------------------------------------------------------------
+// launch dispatch
+// ---------------------------------------------------------------------------
+struct LaunchEnv {
+    dv_context *ctx;
+    cudaStream_t stream;
+    const int *done;
+    double *partials;
+    unsigned *ticket;
+    int max_blocks;
+};
+
+template <class VI, class AT, class Gather, class Op>
+void launch_duvi_vi(const LaunchEnv &e, const dv_matrix *m, Gather g, Op op) {
+    constexpr int W = sizeof(VI) == 4 ? kDuviWarps32 : kDuviWarps;
+    const size_t smem = duvi_smem_bytes<VI, AT>(W);
+    auto kern = k_duvi<VI, AT, Gather, Op, W>;
+    static bool attr_set = false;   // per instantiation
+    if (!attr_set) {
+        DV_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr_set = true;
+    }
+    DuviArgs a;
+    a.row_to_col = m->row_to_col.as<uint32_t>();
+    a.row_to_dist = m->row_to_dist.as<uint32_t>();
+    a.col_idx = m->col_idx.as<uint32_t>();
+    a.dist = m->dist.as<uint8_t>();
+    a.vidx = m->vidx.p;
+    a.values = m->values.p;
+    a.bundles = m->bundles.as<int32_t>();
+    a.nbundles = m->nbundles;
+    a.nuniq = (int32_t)m->nuniq;
+    int blocks = (m->nbundles + W - 1) / W;
+    if (blocks > e.max_blocks) blocks = e.max_blocks;
+    if (blocks < 1) blocks = 1;
+    kern<<<blocks, W * 32, smem, e.stream>>>(a, g, op, e.done, e.partials, e.ticket);
+    DV_CUDA(cudaGetLastError());
+    e.ctx->count();
+}
+
+template <int TPR, class AT, class Gather, class Op>
+void launch_csr_tpr(const LaunchEnv &e, const dv_matrix *m, Gather g, Op op) {
+    const int gpb = kThreads / TPR;
+    int blocks = (m->n_rows + gpb - 1) / gpb;
+    if (blocks > e.max_blocks) blocks = e.max_blocks;
+    if (blocks < 1) blocks = 1;
+    k_csr<TPR, AT, AT, Gather, Op><<<blocks, kThreads, 0, e.stream>>>(
+        m->rowptr.as<int32_t>(), m->col.as<int32_t>(), static_cast<const AT *>(m->val.p), m->n_rows, g, op, e.done,
+        e.partials, e.ticket);
+    DV_CUDA(cudaGetLastError());
+    e.ctx->count();
+}
+
+// Runs op over every row of m with the accumulator type AT (= value precision).
+template <class AT, class Gather, class Op>
+void launch_rows(const LaunchEnv &e, const dv_matrix *m, Gather g, Op op) {
+    if (m->format == DV_FORMAT_DUVI) {
+        if (m->vi_bits == 8) launch_duvi_vi<uint8_t, AT>(e, m, g, op);
+        else if (m->vi_bits == 16) launch_duvi_vi<uint16_t, AT>(e, m, g, op);
+        else launch_duvi_vi<uint32_t, AT>(e, m, g, op);
+        return;
+    }
+    switch (m->csr_tpr) {
+        case 1: launch_csr_tpr<1, AT>(e, m, g, op); break;
+        case 4: launch_csr_tpr<4, AT>(e, m, g, op); break;
+        case 8: launch_csr_tpr<8, AT>(e, m, g, op); break;
+        case 16: launch_csr_tpr<16, AT>(e, m, g, op); break;
+        default: launch_csr_tpr<32, AT>(e, m, g, op); break;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// vector kernels
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void k_scale(const T *__restrict__ w, const T *__restrict__ b, T *__restrict__ x, int32_t n,
+                        const int *__restrict__ done) {
+    if (done && *(volatile const int *)done) return;
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] = w[i] * b[i];
+}
+template <class T>
+__global__ void k_copy(const T *__restrict__ a, T *__restrict__ b, int32_t n, const int *__restrict__ done) {
+    if (done && *(volatile const int *)done) return;
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) b[i] = a[i];
+}
+template <class T>
+__global__ void k_fill(T *__restrict__ a, T v, int32_t n, const int *__restrict__ done) {
+    if (done && *(volatile const int *)done) return;
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) a[i] = v;
+}
+template <class A, class B>
+__global__ void k_convert(const A *__restrict__ a, B *__restrict__ b, int32_t n) {
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) b[i] = (B)a[i];
+}
+// x += y
+template <class T>
+__global__ void k_axpy1(const T *__restrict__ y, T *__restrict__ x, int32_t n, const int *__restrict__ done) {
+    if (done && *(volatile const int *)done) return;
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] = x[i] + y[i];
+}
+
+// Dense y = Ainv b (coarse solve), one warp per row.
+template <class T>
+__global__ void k_dense_gemv(const T *__restrict__ a, const T *__restrict__ b, T *__restrict__ y, int32_t n,
+                             const int *__restrict__ done) {
+    if (done && *(volatile const int *)done) return;
+    const int lane = threadIdx.x & 31;
+    const int32_t nw = (gridDim.x * blockDim.x) >> 5;
+    for (int32_t r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < n; r += nw) {
+        const T *ar = a + (size_t)r * n;
+        T s = 0;
+        for (int32_t k = lane; k < n; k += 32) s += ar[k] * __ldg(b + k);
+        s = warp_sum(s);
+        if (lane == 0) y[r] = s;
+    }
+}
+
+}  // namespace dvk

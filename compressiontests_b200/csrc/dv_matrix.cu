@@ -1,0 +1,411 @@
+// Context, matrix upload and the SpMV/SpMM entry points of libduvigpu.so.
+#include "dv_kernels.cuh"
+
+#include <algorithm>
+#include <cstdio>
+#include <mutex>
+
+static thread_local std::string g_last_error;
+void dv_set_last_error(const std::string &m) { g_last_error = m; }
+
+extern "C" DV_API const char *dv_last_error(void) { return g_last_error.c_str(); }
+extern "C" DV_API int dv_version(void) { return 10000; }
+extern "C" DV_API const char *dv_status_string(int s) {
+    switch (s) {
+        case DV_OK: return "ok";
+        case DV_ERR_ARG: return "invalid argument";
+        case DV_ERR_CUDA: return "CUDA error";
+        case DV_ERR_NOT_INITIALIZED: return "not initialized";
+        case DV_ERR_UNSUPPORTED: return "unsupported";
+        case DV_ERR_NOMEM: return "out of memory";
+        case DV_ERR_FORMAT: return "format error";
+        case DV_ERR_NO_DEVICE: return "no CUDA device";
+        case DV_ERR_SINGULAR: return "singular matrix";
+        case DV_ERR_TIMEOUT: return "device wait timed out";
+        default: return "unknown status";
+    }
+}
+
+void dv_ctx_check(dv_context *ctx) {
+    DV_REQUIRE(ctx != nullptr, DV_ERR_NOT_INITIALIZED, "null context");
+    DV_CUDA(cudaSetDevice(ctx->device));
+}
+
+extern "C" DV_API int dv_context_create(int device, dv_context **out) {
+    return dv_guard([&] {
+        DV_REQUIRE(out != nullptr, DV_ERR_ARG, "null output");
+        *out = nullptr;
+        int n = 0;
+        cudaError_t e = cudaGetDeviceCount(&n);
+        DV_REQUIRE(e == cudaSuccess && n > 0, DV_ERR_NO_DEVICE,
+                   std::string("no usable CUDA device: ") + cudaGetErrorString(e));
+        DV_REQUIRE(device >= 0 && device < n, DV_ERR_ARG, "device ordinal out of range");
+        DV_CUDA(cudaSetDevice(device));
+        cudaDeviceProp prop;
+        DV_CUDA(cudaGetDeviceProperties(&prop, device));
+        DV_REQUIRE(prop.major >= 10, DV_ERR_UNSUPPORTED, "this library is built for sm_100a (B200)");
+        auto ctx = std::make_unique<dv_context>();
+        ctx->device = device;
+        ctx->num_sms = prop.multiProcessorCount;
+        ctx->max_smem_optin = (int)prop.sharedMemPerBlockOptin;
+        DV_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+        ctx->status.alloc(64);
+        *out = ctx.release();
+    });
+}
+
+extern "C" DV_API int dv_context_destroy(dv_context *ctx) {
+    return dv_guard([&] {
+        if (!ctx) return;
+        cudaSetDevice(ctx->device);
+        cudaStreamSynchronize(ctx->stream);
+        ctx->status.release();
+        cudaStreamDestroy(ctx->stream);
+        delete ctx;
+    });
+}
+extern "C" DV_API int dv_context_synchronize(dv_context *ctx) {
+    return dv_guard([&] {
+        dv_ctx_check(ctx);
+        DV_CUDA(cudaStreamSynchronize(ctx->stream));
+    });
+}
+extern "C" DV_API void *dv_context_stream(dv_context *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+extern "C" DV_API int64_t dv_context_launch_count(const dv_context *ctx) { return ctx ? ctx->launches : -1; }
+
+// ---------------------------------------------------------------------------
+// matrix build
+// ---------------------------------------------------------------------------
+static void upload(DevMem &d, const void *h, size_t bytes, cudaStream_t s) {
+    d.alloc(bytes);
+    if (bytes) DV_CUDA(cudaMemcpyAsync(d.p, h, bytes, cudaMemcpyHostToDevice, s));
+}
+
+static void check_csr(const dv_csr_host &a) {
+    DV_REQUIRE(a.n_rows >= 0 && a.n_cols >= 0, DV_ERR_ARG, "negative dimensions");
+    DV_REQUIRE(a.rowptr != nullptr, DV_ERR_ARG, "null rowptr");
+    DV_REQUIRE(a.rowptr[0] == 0, DV_ERR_FORMAT, "rowptr[0] must be 0");
+    int64_t nnz = a.rowptr[a.n_rows];
+    DV_REQUIRE(nnz == 0 || (a.col && a.val), DV_ERR_ARG, "null col/val");
+    for (int32_t i = 0; i < a.n_rows; ++i) {
+        DV_REQUIRE(a.rowptr[i + 1] >= a.rowptr[i], DV_ERR_FORMAT, "rowptr not monotone");
+        for (int32_t k = a.rowptr[i]; k < a.rowptr[i + 1]; ++k) {
+            DV_REQUIRE(a.col[k] >= 0 && a.col[k] < a.n_cols, DV_ERR_FORMAT, "column index out of range");
+            DV_REQUIRE(k == a.rowptr[i] || a.col[k] > a.col[k - 1], DV_ERR_FORMAT,
+                       "columns must be strictly increasing within a row");
+        }
+    }
+}
+
+static int pick_tpr(double mean_nnz) {
+    if (mean_nnz < 6) return 4;
+    if (mean_nnz < 20) return 8;
+    if (mean_nnz < 48) return 16;
+    return 32;
+}
+
+static void finish_duvi_upload(dv_matrix *m, cudaStream_t s) {
+    const DuviHost &h = m->host;
+    m->vi_bits = h.vi_bits;
+    m->nblocks = (int64_t)h.col_idx.size();
+    m->nuniq = (int64_t)h.values.size();
+    upload(m->row_to_col, h.row_to_col.data(), 4 * h.row_to_col.size(), s);
+    upload(m->row_to_dist, h.row_to_dist.data(), 4 * h.row_to_dist.size(), s);
+    upload(m->col_idx, h.col_idx.data(), 4 * h.col_idx.size(), s);
+    upload(m->dist, h.dist.data(), h.dist.size(), s);
+    // value indices at their storage width
+    size_t nnz = h.vidx.size();
+    if (m->vi_bits == 8) {
+        std::vector<uint8_t> v(nnz);
+        for (size_t i = 0; i < nnz; ++i) v[i] = (uint8_t)h.vidx[i];
+        upload(m->vidx, v.data(), nnz, s);
+        DV_CUDA(cudaStreamSynchronize(s));
+    } else if (m->vi_bits == 16) {
+        std::vector<uint16_t> v(nnz);
+        for (size_t i = 0; i < nnz; ++i) v[i] = (uint16_t)h.vidx[i];
+        upload(m->vidx, v.data(), 2 * nnz, s);
+        DV_CUDA(cudaStreamSynchronize(s));
+    } else {
+        upload(m->vidx, h.vidx.data(), 4 * nnz, s);
+    }
+    if (m->precision == DV_F64) {
+        upload(m->values, h.values.data(), 8 * h.values.size(), s);
+    } else {
+        std::vector<float> f(h.values.size());
+        for (size_t i = 0; i < f.size(); ++i) f[i] = (float)h.values[i];
+        upload(m->values, f.data(), 4 * f.size(), s);
+        DV_CUDA(cudaStreamSynchronize(s));
+    }
+    std::vector<int32_t> b;
+    dv_make_bundles(h, m->n_rows, m->vi_bits, b);
+    m->nbundles = (int32_t)b.size() - 1;
+    upload(m->bundles, b.data(), 4 * b.size(), s);
+    DV_CUDA(cudaStreamSynchronize(s));
+    const size_t vs = m->precision == DV_F64 ? 8 : 4;
+    m->device_bytes = (int64_t)(m->nnz * (1 + m->vi_bits / 8) + 4 * m->nblocks + 8 * ((int64_t)m->n_rows + 1) +
+                                vs * m->nuniq);
+}
+
+dv_matrix *dv_matrix_build(dv_context *ctx, const dv_csr_host &a, int format, int precision, int vi_bits, double tol) {
+    dv_ctx_check(ctx);
+    check_csr(a);
+    DV_REQUIRE(format == DV_FORMAT_CSR || format == DV_FORMAT_DUVI, DV_ERR_ARG, "unknown format");
+    DV_REQUIRE(precision == DV_F64 || precision == DV_F32, DV_ERR_ARG, "precision must be DV_F64 or DV_F32");
+    auto m = std::make_unique<dv_matrix>();
+    m->ctx = ctx;
+    m->n_rows = a.n_rows;
+    m->n_cols = a.n_cols;
+    m->nnz = a.rowptr[a.n_rows];
+    m->format = format;
+    m->precision = precision;
+    cudaStream_t s = ctx->stream;
+    if (format == DV_FORMAT_CSR) {
+        upload(m->rowptr, a.rowptr, 4 * ((size_t)a.n_rows + 1), s);
+        upload(m->col, a.col, 4 * (size_t)m->nnz, s);
+        if (precision == DV_F64) {
+            upload(m->val, a.val, 8 * (size_t)m->nnz, s);
+            DV_CUDA(cudaStreamSynchronize(s));
+        } else {
+            std::vector<float> f(m->nnz);
+            for (int64_t i = 0; i < m->nnz; ++i) f[i] = (float)a.val[i];
+            upload(m->val, f.data(), 4 * (size_t)m->nnz, s);
+            DV_CUDA(cudaStreamSynchronize(s));
+        }
+        m->csr_tpr = pick_tpr(a.n_rows ? (double)m->nnz / a.n_rows : 1.0);
+        m->device_bytes = m->nnz * (4 + (precision == DV_F64 ? 8 : 4)) + 4 * ((int64_t)a.n_rows + 1);
+    } else {
+        dv_encode_duvi(a, tol, vi_bits, m->host);
+        finish_duvi_upload(m.get(), s);
+    }
+    if (a.n_rows == a.n_cols) {
+        dv_extract_diag(a, m->host_diag);
+        upload(m->diag, m->host_diag.data(), 8 * m->host_diag.size(), s);
+        DV_CUDA(cudaStreamSynchronize(s));
+    }
+    return m.release();
+}
+
+extern "C" DV_API int dv_matrix_create_csr(dv_context *ctx, const dv_csr_host *a, int32_t precision, dv_matrix **out) {
+    return dv_guard([&] {
+        DV_REQUIRE(a && out, DV_ERR_ARG, "null argument");
+        *out = dv_matrix_build(ctx, *a, DV_FORMAT_CSR, precision, 0, 0.0);
+    });
+}
+
+extern "C" DV_API int dv_matrix_create_duvi(dv_context *ctx, const dv_csr_host *a, int32_t precision,
+                                            int32_t value_index_bits, double dedup_tol, dv_matrix **out) {
+    return dv_guard([&] {
+        DV_REQUIRE(a && out, DV_ERR_ARG, "null argument");
+        *out = dv_matrix_build(ctx, *a, DV_FORMAT_DUVI, precision, value_index_bits, dedup_tol);
+    });
+}
+
+extern "C" DV_API int dv_matrix_create_duvi_soa(dv_context *ctx, int32_t n_rows, int32_t n_cols, const uint32_t *rc,
+                                                const uint32_t *rd, const uint32_t *ci, int64_t nblocks,
+                                                const uint8_t *dist, int64_t nnz, const void *vidx, int32_t bits,
+                                                const double *values, int64_t nuniq, int32_t precision,
+                                                dv_matrix **out) {
+    return dv_guard([&] {
+        dv_ctx_check(ctx);
+        DV_REQUIRE(out && rc && rd && (nblocks == 0 || ci) && (nnz == 0 || (dist && vidx)) && (nuniq == 0 || values),
+                   DV_ERR_ARG, "null argument");
+        DV_REQUIRE(bits == 8 || bits == 16 || bits == 32, DV_ERR_ARG, "value_index_bits must be 8, 16 or 32");
+        DV_REQUIRE(precision == DV_F64 || precision == DV_F32, DV_ERR_ARG, "bad precision");
+        DV_REQUIRE(n_rows >= 0 && n_cols >= 0 && rc[0] == 0 && rd[0] == 0 && rc[n_rows] == (uint64_t)nblocks &&
+                       rd[n_rows] == (uint64_t)nnz, DV_ERR_FORMAT, "inconsistent DuVi offsets");
+        auto m = std::make_unique<dv_matrix>();
+        m->ctx = ctx;
+        m->n_rows = n_rows;
+        m->n_cols = n_cols;
+        m->nnz = nnz;
+        m->format = DV_FORMAT_DUVI;
+        m->precision = precision;
+        DuviHost &h = m->host;
+        h.row_to_col.assign(rc, rc + n_rows + 1);
+        h.row_to_dist.assign(rd, rd + n_rows + 1);
+        h.col_idx.assign(ci, ci + nblocks);
+        h.dist.assign(dist, dist + nnz);
+        h.vidx.resize(nnz);
+        for (int64_t i = 0; i < nnz; ++i)
+            h.vidx[i] = bits == 8 ? ((const uint8_t *)vidx)[i] : bits == 16 ? ((const uint16_t *)vidx)[i] : ((const uint32_t *)vidx)[i];
+        h.values.assign(values, values + nuniq);
+        h.vi_bits = bits;
+        // validate the walk of every row (no read outside the arrays on the device)
+        for (int32_t r = 0; r < n_rows; ++r) {
+            DV_REQUIRE(rc[r + 1] >= rc[r] && rd[r + 1] >= rd[r], DV_ERR_FORMAT, "offsets not monotone");
+            uint64_t di = rd[r];
+            for (uint32_t b = rc[r]; b < rc[r + 1]; ++b) {
+                DV_REQUIRE(di < rd[r + 1], DV_ERR_FORMAT, "block runs past its row");
+                uint64_t c = ci[b];
+                uint64_t end = di + dist[di] + 1;
+                DV_REQUIRE(end <= rd[r + 1], DV_ERR_FORMAT, "block runs past its row");
+                DV_REQUIRE(c < (uint64_t)n_cols, DV_ERR_FORMAT, "column out of range");
+                for (uint64_t k = di + 1; k < end; ++k) {
+                    c += dist[k] + 1u;
+                    DV_REQUIRE(c < (uint64_t)n_cols, DV_ERR_FORMAT, "column out of range");
+                }
+                di = end;
+            }
+            DV_REQUIRE(di == rd[r + 1], DV_ERR_FORMAT, "row entries not covered by its blocks");
+        }
+        for (int64_t i = 0; i < nnz; ++i) DV_REQUIRE(h.vidx[i] < (uint64_t)nuniq, DV_ERR_FORMAT, "value index out of range");
+        m->nuniq = nuniq;
+        finish_duvi_upload(m.get(), ctx->stream);
+        *out = m.release();
+    });
+}
+
+extern "C" DV_API int dv_matrix_get_info(const dv_matrix *m, dv_matrix_info *info) {
+    return dv_guard([&] {
+        DV_REQUIRE(m && info, DV_ERR_ARG, "null argument");
+        info->n_rows = m->n_rows;
+        info->n_cols = m->n_cols;
+        info->nnz = m->nnz;
+        info->nblocks = m->format == DV_FORMAT_DUVI ? m->nblocks : 0;
+        info->nuniq = m->format == DV_FORMAT_DUVI ? m->nuniq : 0;
+        info->format = m->format;
+        info->precision = m->precision;
+        info->value_index_bits = m->format == DV_FORMAT_DUVI ? m->vi_bits : 0;
+        info->kernel_variant = m->format == DV_FORMAT_CSR ? m->csr_tpr : m->nbundles;
+        info->device_bytes = m->device_bytes;
+    });
+}
+
+extern "C" DV_API int dv_matrix_export_duvi(const dv_matrix *m, uint32_t *rc, uint32_t *rd, uint32_t *ci, uint8_t *dist,
+                                            uint32_t *vidx, double *values) {
+    return dv_guard([&] {
+        DV_REQUIRE(m != nullptr, DV_ERR_ARG, "null matrix");
+        DV_REQUIRE(m->format == DV_FORMAT_DUVI, DV_ERR_UNSUPPORTED, "not a DuVi matrix");
+        // Read back what the device holds (not the host copy), widening the indices.
+        dv_ctx_check(m->ctx);
+        cudaStream_t s = m->ctx->stream;
+        if (rc) DV_CUDA(cudaMemcpyAsync(rc, m->row_to_col.p, 4 * ((size_t)m->n_rows + 1), cudaMemcpyDeviceToHost, s));
+        if (rd) DV_CUDA(cudaMemcpyAsync(rd, m->row_to_dist.p, 4 * ((size_t)m->n_rows + 1), cudaMemcpyDeviceToHost, s));
+        if (ci) DV_CUDA(cudaMemcpyAsync(ci, m->col_idx.p, 4 * (size_t)m->nblocks, cudaMemcpyDeviceToHost, s));
+        if (dist) DV_CUDA(cudaMemcpyAsync(dist, m->dist.p, (size_t)m->nnz, cudaMemcpyDeviceToHost, s));
+        std::vector<unsigned char> raw;
+        if (vidx) {
+            raw.resize((size_t)m->nnz * (m->vi_bits / 8));
+            DV_CUDA(cudaMemcpyAsync(raw.data(), m->vidx.p, raw.size(), cudaMemcpyDeviceToHost, s));
+        }
+        std::vector<unsigned char> tab((size_t)m->nuniq * (m->precision == DV_F64 ? 8 : 4));
+        if (values && !tab.empty()) DV_CUDA(cudaMemcpyAsync(tab.data(), m->values.p, tab.size(), cudaMemcpyDeviceToHost, s));
+        DV_CUDA(cudaStreamSynchronize(s));
+        if (vidx)
+            for (int64_t i = 0; i < m->nnz; ++i)
+                vidx[i] = m->vi_bits == 8 ? raw[i] : m->vi_bits == 16 ? ((uint16_t *)raw.data())[i] : ((uint32_t *)raw.data())[i];
+        if (values)
+            for (int64_t i = 0; i < m->nuniq; ++i)
+                values[i] = m->precision == DV_F64 ? ((double *)tab.data())[i] : (double)((float *)tab.data())[i];
+    });
+}
+
+extern "C" DV_API int dv_matrix_destroy(dv_matrix *m) {
+    return dv_guard([&] {
+        if (!m) return;
+        cudaSetDevice(m->ctx->device);
+        cudaStreamSynchronize(m->ctx->stream);
+        delete m;
+    });
+}
+
+// ---------------------------------------------------------------------------
+// products
+// ---------------------------------------------------------------------------
+namespace {
+struct CtxReduce {   // per-context default reduction workspace (lazily created)
+    DevMem mem;
+};
+std::mutex g_ws_mutex;
+std::vector<std::pair<dv_context *, std::unique_ptr<CtxReduce>>> g_ws;
+
+dvk::LaunchEnv env_for(dv_context *ctx, const int *done = nullptr) {
+    std::lock_guard<std::mutex> lk(g_ws_mutex);
+    CtxReduce *w = nullptr;
+    for (auto &p : g_ws) if (p.first == ctx) w = p.second.get();
+    if (!w) {
+        auto n = std::make_unique<CtxReduce>();
+        n->mem.alloc(sizeof(double) * dvk::kMaxRed * ctx->num_sms * 16 + 64);
+        w = n.get();
+        g_ws.emplace_back(ctx, std::move(n));
+    }
+    dvk::LaunchEnv e;
+    e.ctx = ctx;
+    e.stream = ctx->stream;
+    e.done = done;
+    e.ticket = reinterpret_cast<unsigned *>(w->mem.as<char>());
+    e.partials = reinterpret_cast<double *>(w->mem.as<char>() + 64);
+    e.max_blocks = ctx->num_sms * 16;
+    return e;
+}
+}  // namespace
+
+dvk::LaunchEnv dv_default_env(dv_context *ctx) { return env_for(ctx); }
+
+static void spmv_device(dv_matrix *m, const void *x, void *y, int vprec, int clear) {
+    auto e = env_for(m->ctx);
+    if (m->precision == DV_F64) {
+        DV_REQUIRE(vprec == DV_F64, DV_ERR_ARG, "FP64 matrix needs FP64 vectors");
+        dvk::OpSpmv<double, double> op;
+        op.y = static_cast<double *>(y);
+        op.clear = clear;
+        dvk::launch_rows<double>(e, m, dvk::GatherVec<double, double>{static_cast<const double *>(x)}, op);
+    } else {
+        DV_REQUIRE(vprec == DV_F32, DV_ERR_ARG, "FP32 matrix needs FP32 vectors");
+        dvk::OpSpmv<float, float> op;
+        op.y = static_cast<float *>(y);
+        op.clear = clear;
+        dvk::launch_rows<float>(e, m, dvk::GatherVec<float, float>{static_cast<const float *>(x)}, op);
+    }
+}
+
+extern "C" DV_API int dv_spmv_device(dv_matrix *m, const void *x, void *y, int32_t vprec, int32_t clear) {
+    return dv_guard([&] {
+        DV_REQUIRE(m && x && y, DV_ERR_ARG, "null argument");
+        dv_ctx_check(m->ctx);
+        spmv_device(m, x, y, vprec, clear);
+    });
+}
+
+extern "C" DV_API int dv_residual_device(dv_matrix *m, const void *b, const void *x, void *r, int32_t vprec) {
+    return dv_guard([&] {
+        DV_REQUIRE(m && b && x && r, DV_ERR_ARG, "null argument");
+        dv_ctx_check(m->ctx);
+        auto e = env_for(m->ctx);
+        if (m->precision == DV_F64) {
+            DV_REQUIRE(vprec == DV_F64, DV_ERR_ARG, "FP64 matrix needs FP64 vectors");
+            dvk::OpResid<double> op{{}, static_cast<const double *>(b), static_cast<double *>(r)};
+            dvk::launch_rows<double>(e, m, dvk::GatherVec<double, double>{static_cast<const double *>(x)}, op);
+        } else {
+            DV_REQUIRE(vprec == DV_F32, DV_ERR_ARG, "FP32 matrix needs FP32 vectors");
+            dvk::OpResid<float> op{{}, static_cast<const float *>(b), static_cast<float *>(r)};
+            dvk::launch_rows<float>(e, m, dvk::GatherVec<float, float>{static_cast<const float *>(x)}, op);
+        }
+    });
+}
+
+extern "C" DV_API int dv_spmv(dv_matrix *m, const double *x, double *y, int32_t clear) {
+    return dv_guard([&] {
+        DV_REQUIRE(m && x && y, DV_ERR_ARG, "null argument");
+        dv_ctx_check(m->ctx);
+        cudaStream_t s = m->ctx->stream;
+        const size_t vs = m->precision == DV_F64 ? 8 : 4;
+        DevMem dx(vs * (size_t)m->n_cols), dy(vs * (size_t)m->n_rows);
+        if (m->precision == DV_F64) {
+            DV_CUDA(cudaMemcpyAsync(dx.p, x, 8 * (size_t)m->n_cols, cudaMemcpyHostToDevice, s));
+            if (!clear) DV_CUDA(cudaMemcpyAsync(dy.p, y, 8 * (size_t)m->n_rows, cudaMemcpyHostToDevice, s));
+            spmv_device(m, dx.p, dy.p, DV_F64, clear);
+            DV_CUDA(cudaMemcpyAsync(y, dy.p, 8 * (size_t)m->n_rows, cudaMemcpyDeviceToHost, s));
+        } else {
+            std::vector<float> hx(x, x + m->n_cols), hy(m->n_rows);
+            if (!clear) for (int32_t i = 0; i < m->n_rows; ++i) hy[i] = (float)y[i];
+            DV_CUDA(cudaMemcpyAsync(dx.p, hx.data(), 4 * hx.size(), cudaMemcpyHostToDevice, s));
+            DV_CUDA(cudaMemcpyAsync(dy.p, hy.data(), 4 * hy.size(), cudaMemcpyHostToDevice, s));
+            spmv_device(m, dx.p, dy.p, DV_F32, clear);
+            DV_CUDA(cudaMemcpyAsync(hy.data(), dy.p, 4 * hy.size(), cudaMemcpyDeviceToHost, s));
+            DV_CUDA(cudaStreamSynchronize(s));
+            for (int32_t i = 0; i < m->n_rows; ++i) y[i] = hy[i];
+        }
+        DV_CUDA(cudaStreamSynchronize(s));
+    });
+}

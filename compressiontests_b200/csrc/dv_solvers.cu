@@ -1,0 +1,734 @@
+// Solvers of libduvigpu.so: Jacobi PCG (OpenCLCsrPcgSolver semantics) and the
+// multigrid-preconditioned flexible CG in FP64 or mixed precision.
+//
+// Every solver keeps its scalars (alpha, beta, dot products, stop flags) in
+// device memory: no kernel result goes through the host inside an iteration.
+// A chunk of iterations is captured once into a CUDA graph and replayed; each
+// kernel returns at entry once the device-side `done` flag is set, so the
+// iterate is frozen at the iteration that met the stop test and the host reads
+// the flag once per chunk.
+#include "dv_kernels.cuh"
+#include "dv_solvers.cuh"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <type_traits>
+
+using namespace dvk;
+
+dvk::LaunchEnv dv_default_env(dv_context *ctx);
+
+// ---------------------------------------------------------------------------
+// shared pieces
+// ---------------------------------------------------------------------------
+SolverWs::SolverWs(dv_context *c) : ctx(c) {
+    red.alloc(sizeof(double) * kMaxRed * c->num_sms * 16 + 64);
+    scal.alloc(sizeof(SolverScalars));
+    DV_CUDA(cudaMallocHost(&host_scal, sizeof(SolverScalars)));
+}
+SolverWs::~SolverWs() {
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    if (host_scal) cudaFreeHost(host_scal);
+}
+LaunchEnv SolverWs::env(bool with_done) const {
+    LaunchEnv e;
+    e.ctx = ctx;
+    e.stream = ctx->stream;
+    e.done = with_done ? &sc()->done : nullptr;
+    e.ticket = reinterpret_cast<unsigned *>(red.as<char>());
+    e.partials = reinterpret_cast<double *>(red.as<char>() + 64);
+    e.max_blocks = ctx->num_sms * 16;
+    return e;
+}
+void SolverWs::pull() {
+    DV_CUDA(cudaMemcpyAsync(host_scal, scal.p, sizeof(SolverScalars), cudaMemcpyDeviceToHost, ctx->stream));
+    DV_CUDA(cudaStreamSynchronize(ctx->stream));
+}
+void SolverWs::push() {
+    DV_CUDA(cudaMemcpyAsync(scal.p, host_scal, sizeof(SolverScalars), cudaMemcpyHostToDevice, ctx->stream));
+}
+// Runs `body` once eagerly (first call: sets kernel attributes, validates) and
+// afterwards through a captured graph of the same launches.
+void SolverWs::run_chunk(const std::function<void()> &body, bool use_graph, int64_t launches_per_chunk) {
+    cudaStream_t s = ctx->stream;
+    if (!use_graph || !warmed) {
+        body();
+        warmed = true;
+        return;
+    }
+    if (!graph_exec) {
+        cudaGraph_t g;
+        int64_t before = ctx->launches;
+        DV_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        try {
+            body();
+        } catch (...) {
+            cudaStreamEndCapture(s, &g);
+            throw;
+        }
+        DV_CUDA(cudaStreamEndCapture(s, &g));
+        graph_launches = ctx->launches - before;
+        ctx->launches = before;
+        DV_CUDA(cudaGraphInstantiate(&graph_exec, g, 0));
+        cudaGraphDestroy(g);
+    }
+    DV_CUDA(cudaGraphLaunch(graph_exec, s));
+    ctx->count(graph_launches);
+    (void)launches_per_chunk;
+}
+
+static int grid_for(dv_context *ctx, int64_t n) {
+    int64_t b = (n + kThreads - 1) / kThreads;
+    return (int)std::max<int64_t>(1, std::min<int64_t>(b, ctx->num_sms * 8));
+}
+
+// ---------------------------------------------------------------------------
+// vector kernels with reductions
+// ---------------------------------------------------------------------------
+// z = M r; p = z; rz = r.z   (initialize0 + dot, CsrCG.cl:165-176)
+__global__ void k_pcg_init(const double *__restrict__ M, const double *__restrict__ r, double *__restrict__ z,
+                           double *__restrict__ p, int32_t n, SolverScalars *sc, double *partials, unsigned *ticket) {
+    double red[1] = {0.0};
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double zi = M[i] * r[i];
+        z[i] = zi;
+        p[i] = zi;
+        red[0] += r[i] * zi;
+    }
+    double tot[1];
+    if (grid_reduce<1, 0>(red, partials, ticket, tot)) sc->rz = tot[0];
+}
+
+// x += a p; r -= a Ap; z = M r; convergence flags; r.z (update_x_r_z_check_r,
+// CsrCG.cl:257-277, then dot_finalize_and_calc_b, :289-301).
+__global__ void k_pcg_update(const double *__restrict__ M, const double *__restrict__ ap, const double *__restrict__ p,
+                             double *__restrict__ x, double *__restrict__ r, double *__restrict__ z, int32_t n,
+                             double tol, SolverScalars *sc, const int *__restrict__ done, double *partials,
+                             unsigned *ticket) {
+    if (*(volatile const int *)done) return;
+    const double a = sc->alpha;
+    double red[4] = {0.0, 0.0, 0.0, 0.0};   // max|r|, failed flag, r.z, r.r
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        x[i] = x[i] + a * p[i];
+        double ri = r[i] - a * ap[i];
+        r[i] = ri;
+        double zi = M[i] * ri;
+        z[i] = zi;
+        double c = fabs(ri);
+        if (isnan(ri) || c > 1e50) red[1] = 1.0;
+        else red[0] = fmax(red[0], c);
+        red[2] += ri * zi;
+        red[3] += ri * ri;
+    }
+    double t[4];
+    if (grid_reduce<4, 0b0011>(red, partials, ticket, t)) {
+        bool failed = t[1] != 0.0;
+        bool converged = !failed && t[0] <= tol;
+        sc->res_max = t[0];
+        sc->res_norm2 = sqrt(t[3]);
+        sc->converged = converged;
+        sc->failed = failed;
+        if (converged || failed || sc->it > sc->max_it) {
+            sc->done = 1;
+        } else {
+            sc->beta = t[2] / sc->rz;
+            sc->rz = t[2];
+            sc->it += 1;
+        }
+    }
+}
+
+// p = z + beta p (update_p, CsrCG.cl:311-320)
+__global__ void k_pcg_p(const double *__restrict__ z, double *__restrict__ p, int32_t n, const SolverScalars *sc,
+                        const int *__restrict__ done) {
+    if (*(volatile const int *)done) return;
+    const double b = sc->beta;
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = z[i] + b * p[i];
+}
+
+// Flexible CG: beta = -(z.q)/(p.q) (FCG(1) orthogonalisation), z.r for alpha.
+template <class ZT>
+__global__ void k_fcg_red(const ZT *__restrict__ z, const double *__restrict__ q, const double *__restrict__ r,
+                          int32_t n, SolverScalars *sc, const int *__restrict__ done, double *partials,
+                          unsigned *ticket) {
+    if (*(volatile const int *)done) return;
+    double red[2] = {0.0, 0.0};
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double zi = (double)z[i];
+        red[0] += zi * q[i];
+        red[1] += zi * r[i];
+    }
+    double t[2];
+    if (grid_reduce<2, 0>(red, partials, ticket, t)) {
+        sc->zq = t[0];
+        sc->zr = t[1];
+        sc->beta = sc->restart ? 0.0 : -t[0] / sc->pq;
+        sc->restart = 0;
+    }
+}
+
+// x += alpha p; r -= alpha q; r32 = r (mixed); ||r||^2 and the stop decision.
+template <class RT>
+__global__ void k_fcg_update(double *__restrict__ x, double *__restrict__ r, RT *__restrict__ rlow,
+                             const double *__restrict__ p, const double *__restrict__ q, int32_t n, SolverScalars *sc,
+                             const int *__restrict__ done, double *partials, unsigned *ticket) {
+    if (*(volatile const int *)done) return;
+    const double a = sc->alpha;
+    double red[1] = {0.0};
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        x[i] = x[i] + a * p[i];
+        double ri = r[i] - a * q[i];
+        r[i] = ri;
+        if (rlow) rlow[i] = (RT)ri;
+        red[0] += ri * ri;
+    }
+    double t[1];
+    if (grid_reduce<1, 0>(red, partials, ticket, t)) {
+        sc->rr = t[0];
+        sc->it += 1;
+        if (!(t[0] <= sc->tol2 * sc->bb) && !isnan(t[0])) {
+            if (sc->it >= sc->max_it) sc->done = 1;
+        } else {
+            sc->done = 1;
+            sc->converged = !isnan(t[0]);
+            sc->failed = isnan(t[0]);
+        }
+    }
+}
+
+// ||v||^2 into sc->bb (slot 0) or sc->rr (slot 1)
+__global__ void k_norm2(const double *__restrict__ v, int32_t n, SolverScalars *sc, int slot, double *partials,
+                        unsigned *ticket) {
+    double red[1] = {0.0};
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) red[0] += v[i] * v[i];
+    double t[1];
+    if (grid_reduce<1, 0>(red, partials, ticket, t)) {
+        if (slot == 0) sc->bb = t[0];
+        else sc->rr = t[0];
+    }
+}
+
+// Power-method step for the spectral radius of D^-1 A: y = D^-1 A x (epilogue) and ||y||^2.
+template <class T>
+struct OpPower {
+    static constexpr int NRED = 1;
+    static constexpr unsigned MAXMASK = 0;
+    const double *__restrict__ dinv;
+    T *__restrict__ y;
+    SolverScalars *sc;
+    __device__ __forceinline__ T init(int32_t) const { return T(0); }
+    __device__ __forceinline__ void row(int32_t i, T s, double *red) const {
+        T v = (T)(dinv[i] * (double)s);
+        y[i] = v;
+        red[0] += (double)v * (double)v;
+    }
+    __device__ void finish(const double *t) const { sc->rr = t[0]; }
+};
+template <class T>
+__global__ void k_power_normalize(const T *__restrict__ y, T *__restrict__ x, int32_t n, const SolverScalars *sc) {
+    const double s = 1.0 / sqrt(sc->rr);
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] = (T)(y[i] * s);
+}
+
+template <class T>
+__global__ void k_make_weights(const double *__restrict__ diag, T *__restrict__ w, double omega, int32_t n) {
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        w[i] = (T)(omega / diag[i]);
+}
+
+// Spectral radius estimate of D^-1 A by the power method (iters steps from a
+// fixed pseudo-random start); returns ||D^-1 A x|| for the last unit x.
+double dv_power_estimate(dv_context *ctx, SolverWs &ws, dv_matrix *A, int iters) {
+    int32_t n = A->n_rows;
+    const bool f64 = A->precision == DV_F64;
+    const size_t vs = f64 ? 8 : 4;
+    DevMem x(vs * n), y(vs * n);
+    std::vector<double> h(n);
+    uint64_t st = 0x9E3779B97F4A7C15ull;
+    double nn = 0;
+    for (int32_t i = 0; i < n; ++i) {
+        st ^= st << 13; st ^= st >> 7; st ^= st << 17;
+        h[i] = 0.5 + (double)(st >> 11) * (1.0 / 9007199254740992.0);
+        nn += h[i] * h[i];
+    }
+    for (auto &v : h) v /= std::sqrt(nn);
+    cudaStream_t s = ctx->stream;
+    if (f64) DV_CUDA(cudaMemcpyAsync(x.p, h.data(), 8 * n, cudaMemcpyHostToDevice, s));
+    else {
+        std::vector<float> f(h.begin(), h.end());
+        DV_CUDA(cudaMemcpyAsync(x.p, f.data(), 4 * n, cudaMemcpyHostToDevice, s));
+        DV_CUDA(cudaStreamSynchronize(s));
+    }
+    LaunchEnv e = ws.env(false);
+    for (int it = 0; it < iters; ++it) {
+        if (f64) {
+            OpPower<double> op{A->diag.as<double>(), y.as<double>(), ws.sc()};
+            launch_rows<double>(e, A, GatherVec<double, double>{x.as<double>()}, op);
+            k_power_normalize<double><<<grid_for(ctx, n), kThreads, 0, s>>>(y.as<double>(), x.as<double>(), n, ws.sc());
+        } else {
+            OpPower<float> op{A->diag.as<double>(), y.as<float>(), ws.sc()};
+            launch_rows<float>(e, A, GatherVec<float, float>{x.as<float>()}, op);
+            k_power_normalize<float><<<grid_for(ctx, n), kThreads, 0, s>>>(y.as<float>(), x.as<float>(), n, ws.sc());
+        }
+        DV_CUDA(cudaGetLastError());
+        ctx->count();
+    }
+    ws.pull();
+    return std::sqrt(ws.host_scal->rr);
+}
+
+// ---------------------------------------------------------------------------
+// Jacobi PCG (OpenCLCsrPcgSolver)
+// ---------------------------------------------------------------------------
+struct dv_pcg {
+    dv_context *ctx = nullptr;
+    std::unique_ptr<dv_matrix> A;
+    std::unique_ptr<SolverWs> ws;
+    int32_t n = 0, max_iter = 0;
+    double tol = 0;
+    DevMem M, b, x, r, z, p, ap;
+};
+
+extern "C" DV_API int dv_pcg_create(dv_context *ctx, const dv_csr_host *A, int32_t format, int32_t max_iter,
+                                    double tol, dv_pcg **out) {
+    return dv_guard([&] {
+        DV_REQUIRE(A && out, DV_ERR_ARG, "null argument");
+        DV_REQUIRE(A->n_rows == A->n_cols, DV_ERR_ARG, "matrix must be square");
+        DV_REQUIRE(max_iter >= 0 && tol >= 0, DV_ERR_ARG, "bad iteration limit or tolerance");
+        auto s = std::make_unique<dv_pcg>();
+        s->ctx = ctx;
+        s->A.reset(dv_matrix_build(ctx, *A, format, DV_F64, 0, 1e-10));
+        s->ws = std::make_unique<SolverWs>(ctx);
+        s->n = A->n_rows;
+        s->max_iter = max_iter;
+        s->tol = tol;
+        std::vector<double> minv(s->n);
+        for (int32_t i = 0; i < s->n; ++i) {
+            DV_REQUIRE(s->A->host_diag[i] != 0.0, DV_ERR_SINGULAR, "zero diagonal entry");
+            minv[i] = 1 / s->A->host_diag[i];   // JacobiPreconditioner (GeometricMultigridSolver.cs:128-134)
+        }
+        size_t nb = 8 * (size_t)s->n;
+        s->M.alloc(nb);
+        DV_CUDA(cudaMemcpyAsync(s->M.p, minv.data(), nb, cudaMemcpyHostToDevice, ctx->stream));
+        s->b.alloc(nb); s->x.alloc(nb); s->r.alloc(nb); s->z.alloc(nb); s->p.alloc(nb); s->ap.alloc(nb);
+        DV_CUDA(cudaStreamSynchronize(ctx->stream));
+        *out = s.release();
+    });
+}
+
+extern "C" DV_API int dv_pcg_solve(dv_pcg *s, const double *b, const double *x0, double *xout, dv_stats *stats) {
+    return dv_guard([&] {
+        DV_REQUIRE(s != nullptr, DV_ERR_NOT_INITIALIZED, "You must call Initialize(model) first");
+        DV_REQUIRE(b && xout, DV_ERR_ARG, "null argument");
+        dv_context *ctx = s->ctx;
+        dv_ctx_check(ctx);
+        cudaStream_t st = ctx->stream;
+        const int32_t n = s->n;
+        const size_t nb = 8 * (size_t)n;
+        cudaEvent_t e0, e1;
+        DV_CUDA(cudaEventCreate(&e0));
+        DV_CUDA(cudaEventCreate(&e1));
+        DV_CUDA(cudaMemcpyAsync(s->b.p, b, nb, cudaMemcpyHostToDevice, st));
+        if (x0) DV_CUDA(cudaMemcpyAsync(s->x.p, x0, nb, cudaMemcpyHostToDevice, st));
+        DV_CUDA(cudaEventRecord(e0, st));
+        LaunchEnv e = s->ws->env(false);
+        SolverScalars &h = *s->ws->host_scal;
+        std::memset(&h, 0, sizeof(h));
+        h.max_it = s->max_iter;
+        s->ws->push();
+        if (x0) {   // initialize: r = b - A x0 (CsrCG.cl:191-211)
+            OpResid<double> op{{}, s->b.as<double>(), s->r.as<double>()};
+            launch_rows<double>(e, s->A.get(), GatherVec<double, double>{s->x.as<double>()}, op);
+        } else {
+            DV_CUDA(cudaMemsetAsync(s->x.p, 0, nb, st));
+            DV_CUDA(cudaMemcpyAsync(s->r.p, s->b.p, nb, cudaMemcpyDeviceToDevice, st));
+        }
+        const int g = grid_for(ctx, n);
+        k_pcg_init<<<g, kThreads, 0, st>>>(s->M.as<double>(), s->r.as<double>(), s->z.as<double>(), s->p.as<double>(), n,
+                                          s->ws->sc(), e.partials, e.ticket);
+        DV_CUDA(cudaGetLastError());
+        ctx->count();
+        LaunchEnv ed = s->ws->env(true);
+        const int chunk = 16;
+        auto body = [&] {
+            for (int k = 0; k < chunk; ++k) {
+                OpPcgAp op{s->p.as<double>(), s->ap.as<double>(), s->ws->sc()};
+                launch_rows<double>(ed, s->A.get(), GatherVec<double, double>{s->p.as<double>()}, op);
+                k_pcg_update<<<g, kThreads, 0, st>>>(s->M.as<double>(), s->ap.as<double>(), s->p.as<double>(),
+                                                     s->x.as<double>(), s->r.as<double>(), s->z.as<double>(), n, s->tol,
+                                                     s->ws->sc(), ed.done, ed.partials, ed.ticket);
+                DV_CUDA(cudaGetLastError());
+                k_pcg_p<<<g, kThreads, 0, st>>>(s->z.as<double>(), s->p.as<double>(), n, s->ws->sc(), ed.done);
+                DV_CUDA(cudaGetLastError());
+                ctx->count(2);
+            }
+        };
+        for (;;) {
+            s->ws->run_chunk(body, true, 3 * chunk);
+            s->ws->pull();
+            if (h.done) break;
+        }
+        DV_CUDA(cudaEventRecord(e1, st));
+        DV_CUDA(cudaMemcpyAsync(xout, s->x.p, nb, cudaMemcpyDeviceToHost, st));
+        DV_CUDA(cudaStreamSynchronize(st));
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (stats) {
+            stats->iterations = h.it;
+            stats->converged = h.converged;
+            stats->failed = h.failed;
+            stats->device_status = 0;
+            stats->residual_max = h.res_max;
+            stats->residual_norm2 = h.res_norm2;
+            stats->relative_residual = NAN;
+            stats->solve_ms = ms;
+        }
+    });
+}
+
+extern "C" DV_API int dv_pcg_destroy(dv_pcg *s) {
+    return dv_guard([&] {
+        if (!s) return;
+        cudaSetDevice(s->ctx->device);
+        cudaStreamSynchronize(s->ctx->stream);
+        delete s;
+    });
+}
+
+// ---------------------------------------------------------------------------
+// multigrid-preconditioned flexible CG
+// ---------------------------------------------------------------------------
+template <class T>
+struct VLevel {
+    std::unique_ptr<dv_matrix> A, R, P;
+    DevMem w, b, x, t, r;
+    int32_t n = 0;
+};
+
+template <class T>
+struct VCycle {
+    dv_context *ctx = nullptr;
+    std::vector<VLevel<T>> lv;   // all but the coarsest
+    int32_t nc = 0;
+    DevMem ainv, bc, xc;
+    int nu = 2;
+
+    // x_0 = V(b_0); returns the buffer that holds the result (level-0 x or t).
+    T *run(const LaunchEnv &e, const T *b0) { return level(e, 0, b0); }
+
+    T *level(const LaunchEnv &e, size_t l, const T *b) {
+        cudaStream_t s = e.stream;
+        if (l == lv.size()) {
+            k_dense_gemv<T><<<std::max(1, std::min(nc / 8 + 1, ctx->num_sms * 8)), kThreads, 0, s>>>(
+                ainv.template as<T>(), b, xc.template as<T>(), nc, e.done);
+            DV_CUDA(cudaGetLastError());
+            ctx->count();
+            return xc.template as<T>();
+        }
+        VLevel<T> &L = lv[l];
+        T *x = L.x.template as<T>(), *t = L.t.template as<T>();
+        const T *w = L.w.template as<T>();
+        if (nu == 1) {
+            k_scale<T><<<grid_for(ctx, L.n), kThreads, 0, s>>>(w, b, x, L.n, e.done);
+            DV_CUDA(cudaGetLastError());
+            ctx->count();
+        } else {
+            OpJacobiFromZero<T> op{{}, w, b, x};
+            launch_rows<T>(e, L.A.get(), GatherWB<T>{w, b}, op);
+            for (int k = 2; k < nu; ++k) {
+                OpJacobi<T> oj{{}, x, w, b, t};
+                launch_rows<T>(e, L.A.get(), GatherVec<T, T>{x}, oj);
+                std::swap(x, t);
+            }
+        }
+        OpResid<T> orr{{}, b, L.r.template as<T>()};
+        launch_rows<T>(e, L.A.get(), GatherVec<T, T>{x}, orr);
+        T *bn = l + 1 < lv.size() ? lv[l + 1].b.template as<T>() : bc.template as<T>();
+        OpSpmv<T, T> orst;
+        orst.y = bn;
+        orst.clear = 1;
+        launch_rows<T>(e, L.R.get(), GatherVec<T, T>{L.r.template as<T>()}, orst);
+        T *xn = level(e, l + 1, bn);
+        OpSpmv<T, T> opro;
+        opro.y = x;
+        opro.clear = 0;
+        launch_rows<T>(e, L.P.get(), GatherVec<T, T>{xn}, opro);
+        for (int k = 0; k < nu; ++k) {
+            OpJacobi<T> oj{{}, x, w, b, t};
+            launch_rows<T>(e, L.A.get(), GatherVec<T, T>{x}, oj);
+            std::swap(x, t);
+        }
+        return x;
+    }
+};
+
+struct dv_mgpcg {
+    dv_context *ctx = nullptr;
+    dv_mgpcg_config cfg{};
+    std::unique_ptr<dv_matrix> Aout;   // FP64 operator of the outer loop
+    std::unique_ptr<VCycle<float>> v32;
+    std::unique_ptr<VCycle<double>> v64;
+    std::unique_ptr<SolverWs> ws;
+    int32_t n = 0;
+    DevMem b, x, r, r32, p, q;
+    std::vector<double> omega_eff;
+    int64_t launches_last = 0;
+};
+
+// CSR transpose on the host (restriction = P^T).
+static void csr_transpose(const dv_csr_host &a, std::vector<int32_t> &rp, std::vector<int32_t> &ci, std::vector<double> &va) {
+    int64_t nnz = a.rowptr[a.n_rows];
+    rp.assign(a.n_cols + 1, 0);
+    ci.resize(nnz);
+    va.resize(nnz);
+    for (int64_t k = 0; k < nnz; ++k) rp[a.col[k] + 1]++;
+    for (int32_t i = 0; i < a.n_cols; ++i) rp[i + 1] += rp[i];
+    std::vector<int32_t> fill(rp.begin(), rp.end() - 1);
+    for (int32_t r = 0; r < a.n_rows; ++r)
+        for (int32_t k = a.rowptr[r]; k < a.rowptr[r + 1]; ++k) {
+            int32_t c = a.col[k];
+            ci[fill[c]] = r;
+            va[fill[c]] = a.val[k];
+            fill[c]++;
+        }
+}
+
+template <class T>
+static std::unique_ptr<VCycle<T>> build_vcycle(dv_context *ctx, SolverWs &ws, int32_t L, const dv_csr_host *A,
+                                               const dv_csr_host *P, const dv_mgpcg_config &cfg,
+                                               std::vector<double> &omega_eff) {
+    auto v = std::make_unique<VCycle<T>>();
+    v->ctx = ctx;
+    v->nu = cfg.nu;
+    const int prec = sizeof(T) == 8 ? DV_F64 : DV_F32;
+    cudaStream_t s = ctx->stream;
+    v->lv.resize(L - 1);
+    for (int32_t l = 0; l < L - 1; ++l) {
+        VLevel<T> &lv = v->lv[l];
+        DV_REQUIRE(A[l].n_rows == A[l].n_cols, DV_ERR_ARG, "level operators must be square");
+        DV_REQUIRE(P[l].n_rows == A[l].n_rows && P[l].n_cols == A[l + 1].n_rows, DV_ERR_ARG,
+                   "prolongation shape does not match the levels");
+        lv.n = A[l].n_rows;
+        lv.A.reset(dv_matrix_build(ctx, A[l], cfg.format, prec, 0, 1e-10));
+        lv.P.reset(dv_matrix_build(ctx, P[l], cfg.format, prec, 0, 1e-10));
+        std::vector<int32_t> rp, ci;
+        std::vector<double> va;
+        csr_transpose(P[l], rp, ci, va);
+        dv_csr_host rt{P[l].n_cols, P[l].n_rows, rp.data(), ci.data(), va.data()};
+        lv.R.reset(dv_matrix_build(ctx, rt, cfg.format, prec, 0, 1e-10));
+        for (double d : lv.A->host_diag) DV_REQUIRE(d != 0.0, DV_ERR_SINGULAR, "zero diagonal entry");
+        double om = cfg.omega;
+        if (cfg.omega_mode == DV_OMEGA_SPECTRAL) {
+            double lam = dv_power_estimate(ctx, ws, lv.A.get(), 40);
+            om = cfg.omega * 2.0 / (1.1 * lam);
+        }
+        omega_eff.push_back(om);
+        const size_t vs = sizeof(T) * (size_t)lv.n;
+        lv.w.alloc(vs); lv.b.alloc(vs); lv.x.alloc(vs); lv.t.alloc(vs); lv.r.alloc(vs);
+        k_make_weights<T><<<grid_for(ctx, lv.n), kThreads, 0, s>>>(lv.A->diag.template as<double>(), lv.w.template as<T>(), om, lv.n);
+        DV_CUDA(cudaGetLastError());
+    }
+    const dv_csr_host &Ac = A[L - 1];
+    v->nc = Ac.n_rows;
+    DV_REQUIRE(v->nc <= 16384, DV_ERR_UNSUPPORTED, "coarsest level above 16384 dofs (dense inverse)");
+    std::vector<double> dense((size_t)v->nc * v->nc, 0.0);
+    for (int32_t r = 0; r < v->nc; ++r)
+        for (int32_t k = Ac.rowptr[r]; k < Ac.rowptr[r + 1]; ++k) dense[(size_t)r * v->nc + Ac.col[k]] = Ac.val[k];
+    DV_REQUIRE(dv_dense_inverse(v->nc, dense, 1e-300), DV_ERR_SINGULAR, "coarse matrix is singular");
+    v->ainv.alloc(sizeof(T) * dense.size());
+    if (sizeof(T) == 8) {
+        DV_CUDA(cudaMemcpyAsync(v->ainv.p, dense.data(), 8 * dense.size(), cudaMemcpyHostToDevice, s));
+        DV_CUDA(cudaStreamSynchronize(s));
+    } else {
+        std::vector<float> f(dense.begin(), dense.end());
+        DV_CUDA(cudaMemcpyAsync(v->ainv.p, f.data(), 4 * f.size(), cudaMemcpyHostToDevice, s));
+        DV_CUDA(cudaStreamSynchronize(s));
+    }
+    v->bc.alloc(sizeof(T) * v->nc);
+    v->xc.alloc(sizeof(T) * v->nc);
+    return v;
+}
+
+extern "C" DV_API int dv_mgpcg_create(dv_context *ctx, int32_t L, const dv_csr_host *A, const dv_csr_host *P,
+                                      const dv_mgpcg_config *cfg, dv_mgpcg **out) {
+    return dv_guard([&] {
+        DV_REQUIRE(A && cfg && out && L >= 1 && (L == 1 || P), DV_ERR_ARG, "null argument");
+        DV_REQUIRE(cfg->precision == DV_F64 || cfg->precision == DV_MIXED, DV_ERR_ARG, "precision must be DV_F64 or DV_MIXED");
+        DV_REQUIRE(cfg->nu >= 1 && cfg->max_iterations >= 1 && cfg->tol > 0, DV_ERR_ARG, "bad smoothing or stop parameters");
+        DV_REQUIRE(L >= 2, DV_ERR_ARG, "need at least two levels");
+        dv_ctx_check(ctx);
+        auto s = std::make_unique<dv_mgpcg>();
+        s->ctx = ctx;
+        s->cfg = *cfg;
+        s->ws = std::make_unique<SolverWs>(ctx);
+        s->n = A[0].n_rows;
+        s->Aout.reset(dv_matrix_build(ctx, A[0], cfg->outer_format, DV_F64, 0, 1e-10));
+        if (cfg->precision == DV_MIXED) s->v32 = build_vcycle<float>(ctx, *s->ws, L, A, P, *cfg, s->omega_eff);
+        else s->v64 = build_vcycle<double>(ctx, *s->ws, L, A, P, *cfg, s->omega_eff);
+        const size_t nb = 8 * (size_t)s->n;
+        s->b.alloc(nb); s->x.alloc(nb); s->r.alloc(nb); s->p.alloc(nb); s->q.alloc(nb);
+        if (cfg->precision == DV_MIXED) s->r32.alloc(4 * (size_t)s->n);
+        DV_CUDA(cudaStreamSynchronize(ctx->stream));
+        *out = s.release();
+    });
+}
+
+// One outer iteration of FCG(1) given z (the V-cycle output of the previous
+// step), then the V-cycle for the next z.  Returns the buffer of the new z.
+template <class T>
+static const T *fcg_step(dv_mgpcg *s, const LaunchEnv &e, VCycle<T> &vc, const T *z, T *rin) {
+    cudaStream_t st = e.stream;
+    const int g = grid_for(s->ctx, s->n);
+    k_fcg_red<T><<<g, kThreads, 0, st>>>(z, s->q.as<double>(), s->r.as<double>(), s->n, s->ws->sc(), e.done,
+                                         e.partials, e.ticket);
+    DV_CUDA(cudaGetLastError());
+    s->ctx->count();
+    OpFcg<T> op{z, s->p.as<double>(), s->q.as<double>(), s->ws->sc(), 0.0};
+    launch_rows<double>(e, s->Aout.get(), GatherVec<T, double>{z}, op);
+    T *rl = std::is_same<T, float>::value ? reinterpret_cast<T *>(s->r32.p) : nullptr;
+    k_fcg_update<T><<<g, kThreads, 0, st>>>(s->x.as<double>(), s->r.as<double>(), rl, s->p.as<double>(),
+                                            s->q.as<double>(), s->n, s->ws->sc(), e.done, e.partials, e.ticket);
+    DV_CUDA(cudaGetLastError());
+    s->ctx->count();
+    return vc.run(e, rin);
+}
+
+template <class T>
+static void mgpcg_solve_impl(dv_mgpcg *s, VCycle<T> &vc, dv_stats *stats) {
+    dv_context *ctx = s->ctx;
+    cudaStream_t st = ctx->stream;
+    const int32_t n = s->n;
+    const size_t nb = 8 * (size_t)n;
+    SolverWs &ws = *s->ws;
+    SolverScalars &h = *ws.host_scal;
+    LaunchEnv e0 = ws.env(false), ed = ws.env(true);
+    cudaEvent_t ev0, ev1;
+    DV_CUDA(cudaEventCreate(&ev0));
+    DV_CUDA(cudaEventCreate(&ev1));
+    DV_CUDA(cudaEventRecord(ev0, st));
+    std::memset(&h, 0, sizeof(h));
+    h.max_it = s->cfg.max_iterations;
+    h.tol2 = s->cfg.tol * s->cfg.tol;
+    h.restart = 1;
+    h.pq = 1.0;
+    ws.push();
+    const int g = grid_for(ctx, n);
+    k_norm2<<<g, kThreads, 0, st>>>(s->b.as<double>(), n, ws.sc(), 0, e0.partials, e0.ticket);
+    DV_CUDA(cudaGetLastError());
+    ctx->count();
+    DV_CUDA(cudaMemsetAsync(s->x.p, 0, nb, st));
+    DV_CUDA(cudaMemcpyAsync(s->r.p, s->b.p, nb, cudaMemcpyDeviceToDevice, st));
+    T *rin;
+    if (std::is_same<T, float>::value) {
+        k_convert<double, float><<<g, kThreads, 0, st>>>(s->b.as<double>(), s->r32.as<float>(), n);
+        DV_CUDA(cudaGetLastError());
+        ctx->count();
+        rin = reinterpret_cast<T *>(s->r32.p);
+    } else {
+        rin = reinterpret_cast<T *>(s->r.p);
+    }
+    const T *z = vc.run(ed, rin);
+    const int per = s->cfg.iterations_per_sync > 0 ? s->cfg.iterations_per_sync : 4;
+    const T *zfinal = z;
+    auto body = [&] {
+        const T *zz = z;
+        for (int k = 0; k < per; ++k) zz = fcg_step<T>(s, ed, vc, zz, rin);
+        zfinal = zz;
+    };
+    int refinements = 0;
+    for (;;) {
+        ws.run_chunk(body, s->cfg.use_graphs != 0, 0);
+        DV_REQUIRE(zfinal == z, DV_ERR_ARG, "V-cycle output buffer is not stable across iterations");
+        ws.pull();
+        if (!h.done) continue;
+        if (!h.converged) break;
+        // FP64 verification of the true residual; restart from it if the
+        // recurrence drifted (iterative refinement).
+        OpResid<double> orr{{}, s->b.as<double>(), s->p.as<double>()};
+        launch_rows<double>(e0, s->Aout.get(), GatherVec<double, double>{s->x.as<double>()}, orr);
+        k_norm2<<<g, kThreads, 0, st>>>(s->p.as<double>(), n, ws.sc(), 1, e0.partials, e0.ticket);
+        DV_CUDA(cudaGetLastError());
+        ctx->count();
+        ws.pull();
+        if (h.rr <= h.tol2 * h.bb || refinements >= 4 || h.it >= h.max_it) {
+            h.converged = h.rr <= h.tol2 * h.bb;
+            break;
+        }
+        ++refinements;
+        DV_CUDA(cudaMemcpyAsync(s->r.p, s->p.p, nb, cudaMemcpyDeviceToDevice, st));
+        if (std::is_same<T, float>::value) {
+            k_convert<double, float><<<g, kThreads, 0, st>>>(s->r.as<double>(), s->r32.as<float>(), n);
+            DV_CUDA(cudaGetLastError());
+            ctx->count();
+        }
+        h.done = 0;
+        h.converged = 0;
+        h.restart = 1;
+        ws.push();
+        z = vc.run(ed, rin);
+    }
+    // final true residual (FP64)
+    OpResid<double> orr{{}, s->b.as<double>(), s->p.as<double>()};
+    launch_rows<double>(e0, s->Aout.get(), GatherVec<double, double>{s->x.as<double>()}, orr);
+    k_norm2<<<g, kThreads, 0, st>>>(s->p.as<double>(), n, ws.sc(), 1, e0.partials, e0.ticket);
+    DV_CUDA(cudaGetLastError());
+    ctx->count();
+    DV_CUDA(cudaEventRecord(ev1, st));
+    ws.pull();
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ev0, ev1);
+    cudaEventDestroy(ev0);
+    cudaEventDestroy(ev1);
+    if (stats) {
+        stats->iterations = h.it;
+        stats->converged = h.converged;
+        stats->failed = h.failed;
+        stats->device_status = 0;
+        stats->residual_max = NAN;
+        stats->residual_norm2 = std::sqrt(h.rr);
+        stats->relative_residual = std::sqrt(h.rr / h.bb);
+        stats->solve_ms = ms;
+    }
+}
+
+extern "C" DV_API int dv_mgpcg_solve_device(dv_mgpcg *s, const double *d_b, double *d_x, dv_stats *stats) {
+    return dv_guard([&] {
+        DV_REQUIRE(s != nullptr, DV_ERR_NOT_INITIALIZED, "solver not created");
+        DV_REQUIRE(d_b && d_x, DV_ERR_ARG, "null argument");
+        dv_ctx_check(s->ctx);
+        cudaStream_t st = s->ctx->stream;
+        const size_t nb = 8 * (size_t)s->n;
+        DV_CUDA(cudaMemcpyAsync(s->b.p, d_b, nb, cudaMemcpyDeviceToDevice, st));
+        if (s->v32) mgpcg_solve_impl<float>(s, *s->v32, stats);
+        else mgpcg_solve_impl<double>(s, *s->v64, stats);
+        DV_CUDA(cudaMemcpyAsync(d_x, s->x.p, nb, cudaMemcpyDeviceToDevice, st));
+        DV_CUDA(cudaStreamSynchronize(st));
+    });
+}
+
+extern "C" DV_API int dv_mgpcg_solve(dv_mgpcg *s, const double *b, double *x, dv_stats *stats) {
+    return dv_guard([&] {
+        DV_REQUIRE(s != nullptr, DV_ERR_NOT_INITIALIZED, "solver not created");
+        DV_REQUIRE(b && x, DV_ERR_ARG, "null argument");
+        dv_ctx_check(s->ctx);
+        cudaStream_t st = s->ctx->stream;
+        const size_t nb = 8 * (size_t)s->n;
+        DV_CUDA(cudaMemcpyAsync(s->b.p, b, nb, cudaMemcpyHostToDevice, st));
+        if (s->v32) mgpcg_solve_impl<float>(s, *s->v32, stats);
+        else mgpcg_solve_impl<double>(s, *s->v64, stats);
+        DV_CUDA(cudaMemcpyAsync(x, s->x.p, nb, cudaMemcpyDeviceToHost, st));
+        DV_CUDA(cudaStreamSynchronize(st));
+    });
+}
+
+extern "C" DV_API int dv_mgpcg_destroy(dv_mgpcg *s) {
+    return dv_guard([&] {
+        if (!s) return;
+        cudaSetDevice(s->ctx->device);
+        cudaStreamSynchronize(s->ctx->stream);
+        delete s;
+    });
+}

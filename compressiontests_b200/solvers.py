@@ -1,0 +1,280 @@
+"""Solver classes with the interface of the reference's GPU solvers.
+
+  CudaCsrGeometricMultigridSolver / CudaDuViGeometricMultigridSolver
+      <- OpenCLCsrGeometricMultigridSolver / OpenCLDuViGeometricMultigridSolver
+         (CreateSimpleV, CreateDeepV, Solve, ReleaseOpenCLResources;
+          OpenCLCsrGeometricMultigridSolver.cs:55-83, 334-536)
+  CudaCsrPcgSolver <- OpenCLCsrPcgSolver (OpenCLCsrPcgSolver.cs:40-45, 84-218, 250-331)
+  MultigridPcgSolver: build-defined FP64 / mixed-precision flexible CG with a
+      V-cycle preconditioner, composed from the same kernels.
+
+Solve returns (x, IterativeStatistics, level_times) like
+IGeometricMultigridSolver.Solve (IGeometricMultigridSolver.cs:8).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+import scipy.sparse as sp
+
+from . import _native as N
+from .sparse import CudaContext, _csr_arrays
+
+MAX_CIRCLE_ITERATIONS = 10000   # GeometricMultigridSolver.cs:35
+
+
+@dataclass
+class IterativeStatistics:
+    NumIterationsRequired: int
+    HasConverged: bool
+    ConvergenceCriterion: tuple
+    Failed: bool = False
+    ResidualMaxNorm: float = float("nan")
+    ResidualNorm2: float = float("nan")
+    RelativeResidual: float = float("nan")
+    SolveMilliseconds: float = float("nan")
+
+
+def _stats(s: N.Stats, label="max-norm of residual"):
+    return IterativeStatistics(int(s.iterations), bool(s.converged), (label, float(s.residual_max)), bool(s.failed),
+                               float(s.residual_max), float(s.residual_norm2), float(s.relative_residual),
+                               float(s.solve_ms))
+
+
+def _hosts(mats):
+    arr = (N.CsrHost * max(1, len(mats)))()
+    keep = []
+    for i, m in enumerate(mats):
+        rp, ci, va, shape = _csr_arrays(m)
+        h, k = N.csr_host(rp, ci, va, shape)
+        arr[i] = h
+        keep.append(k)
+    return arr, keep
+
+
+def make_path(level_down):
+    """MakePath (GeometricMultigridSolver.cs:178-201)."""
+    ld = [bool(v) for v in level_down]
+    cur, total, first = 0, 1, 0
+    for d in ld:
+        if d:
+            cur += 1
+            if cur == total:
+                total += 1
+        elif cur == 0:
+            first += 1
+            total += 1
+        else:
+            cur -= 1
+    if cur > first:
+        ld += [False] * (cur - first)
+    elif cur < first:
+        ld += [True] * (first - cur)
+    return ld, total, first
+
+
+class _GeometricMultigridBase:
+    FORMAT = N.FORMAT_CSR
+
+    def __init__(self, context: CudaContext, maxCircleIterations, convergenceTolerance, levelDown, levelIterations,
+                 GaussSeidel=True, gauss_seidel_ordering="lexicographic", cycles_per_sync=16):
+        self.context = context
+        self.GaussSeidel = GaussSeidel
+        self.LevelDown = list(levelDown)
+        self.LevelIterations = [4] if levelIterations is None else list(levelIterations)
+        self.MaxIterations = maxCircleIterations
+        self.ConvergenceTolerance = convergenceTolerance
+        self.ordering = gauss_seidel_ordering
+        self.cycles_per_sync = cycles_per_sync
+        self.h = None
+        self.b = None
+        self.LevelDoFs = None
+
+    @classmethod
+    def CreateSimpleV(cls, context, model, GaussSeidel=True, maxCircleIterations=MAX_CIRCLE_ITERATIONS,
+                      coarseRelaxation=True, convergenceTolerance=1e-6, levelIterations=4, **kw):
+        s = cls(context, maxCircleIterations, convergenceTolerance, [True, False], [levelIterations], GaussSeidel, **kw)
+        s.Initialize(model, coarseRelaxation)
+        return s
+
+    @classmethod
+    def CreateDeepV(cls, context, model, GaussSeidel=True, maxCircleIterations=MAX_CIRCLE_ITERATIONS,
+                    coarseRelaxation=True, convergenceTolerance=1e-6, depth=2, levelIterations=4, **kw):
+        s = cls(context, maxCircleIterations, convergenceTolerance, [True] * depth + [False] * depth,
+                [levelIterations], GaussSeidel, **kw)
+        s.Initialize(model, coarseRelaxation)
+        return s
+
+    def Initialize(self, model, coarseRelaxation=True, rhs=None):
+        """Build the level hierarchy from the model (OpenCLCsrGeometricMultigridSolver.cs:145-285)."""
+        path, total, first = make_path(self.LevelDown)
+        if first != 0:
+            raise N.NotImplementedFeatureError(N.DV_ERR_UNSUPPORTED, "firstLevel != 0 is not implementent yet")
+        A, R, P = [], [], []
+        Am, b = model.CreateLinearSystem()
+        self.b = np.asarray(b if rhs is None else rhs, np.float64)
+        A.append(Am)
+        m = model
+        for _ in range(total - 1):
+            c = m.CreateCoarserModel()
+            r, p = m.transfer_to(c)
+            R.append(r)
+            P.append(p)
+            Ac, _ = c.CreateLinearSystem()
+            A.append(Ac)
+            m = c
+        self.initialize_from_levels(A, R, P, coarseRelaxation, path)
+
+    def initialize_from_levels(self, A, R, P, coarseRelaxation=True, path=None):
+        path = self.LevelDown if path is None else path
+        ah, ka = _hosts(A)
+        rh, kr = _hosts(R)
+        ph, kp = _hosts(P)
+        ld = np.array(path, np.uint8)
+        li = np.array(self.LevelIterations, np.int32)
+        smoother = N.SMOOTHER_JACOBI
+        if self.GaussSeidel:
+            smoother = N.SMOOTHER_GS_LEX if self.ordering == "lexicographic" else N.SMOOTHER_GS_COLOR
+        cfg = N.GmgConfig(smoother, self.FORMAT, self.MaxIterations, 1 if coarseRelaxation else 0,
+                          self.ConvergenceTolerance, len(ld), N.ptr(ld), len(li), N.ptr(li), self.cycles_per_sync)
+        h = C.c_void_p()
+        N.check(N.lib().dv_gmg_create(self.context.h, len(A), ah, rh, ph, C.byref(cfg), C.byref(h)))
+        del ka, kr, kp
+        self.h = h
+        self.LevelDoFs = [a.shape[0] for a in A]
+
+    def omega(self, level):
+        w = C.c_double()
+        N.check(N.lib().dv_gmg_omega(self.h, level, C.byref(w)))
+        return w.value
+
+    def Solve(self, xInitialGuess=None, b=None):
+        if self.h is None:
+            raise N.NotInitializedError(N.DV_ERR_NOT_INITIALIZED, "You must call Initialize(model) first")
+        b = self.b if b is None else np.ascontiguousarray(b, np.float64)
+        x = np.empty(self.LevelDoFs[0])
+        x0 = None if xInitialGuess is None else np.ascontiguousarray(xInitialGuess, np.float64)
+        st = N.Stats()
+        N.check(N.lib().dv_gmg_solve(self.h, N.ptr(b), N.ptr(x0), N.ptr(x), C.byref(st)))
+        return x, _stats(st), np.zeros(len(self.LevelDoFs))
+
+    def ReleaseCudaResources(self):
+        if self.h is not None:
+            N.lib().dv_gmg_destroy(self.h)
+            self.h = None
+
+    ReleaseOpenCLResources = ReleaseCudaResources
+
+    def __del__(self):
+        try:
+            self.ReleaseCudaResources()
+        except Exception:
+            pass
+
+
+class CudaCsrGeometricMultigridSolver(_GeometricMultigridBase):
+    FORMAT = N.FORMAT_CSR
+
+
+class CudaDuViGeometricMultigridSolver(_GeometricMultigridBase):
+    FORMAT = N.FORMAT_DUVI
+
+
+class CudaCsrPcgSolver:
+    """Jacobi-preconditioned CG, FP64, stop when every |r_i| <= tol."""
+
+    FORMAT = N.FORMAT_CSR
+
+    def __init__(self, context: CudaContext, maxIterations, convergenceTolerance, fmt="csr"):
+        self.context = context
+        self.MaxIterations = maxIterations
+        self.ConvergenceTolerance = convergenceTolerance
+        self.fmt = N.FORMAT_DUVI if fmt == "duvi" else N.FORMAT_CSR
+        self.h = None
+        self.DoFs = 0
+
+    def Initialize(self, model=None, A=None, b=None):
+        if model is not None:
+            A, b = model.CreateLinearSystem()
+        (ah, keep) = _hosts([A])
+        h = C.c_void_p()
+        N.check(N.lib().dv_pcg_create(self.context.h, ah, self.fmt, self.MaxIterations, self.ConvergenceTolerance,
+                                      C.byref(h)))
+        del keep
+        self.h = h
+        self.b = None if b is None else np.asarray(b, np.float64)
+        self.DoFs = A.shape[0]
+        return self
+
+    def Solve(self, xInitialGuess=None, b=None):
+        if self.h is None:
+            raise N.NotInitializedError(N.DV_ERR_NOT_INITIALIZED, "You must call Initialize(model) first")
+        b = self.b if b is None else np.ascontiguousarray(b, np.float64)
+        x = np.empty(self.DoFs)
+        x0 = None if xInitialGuess is None else np.ascontiguousarray(xInitialGuess, np.float64)
+        st = N.Stats()
+        N.check(N.lib().dv_pcg_solve(self.h, N.ptr(b), N.ptr(x0), N.ptr(x), C.byref(st)))
+        return x, _stats(st)
+
+    def ReleaseCudaResources(self):
+        if self.h is not None:
+            N.lib().dv_pcg_destroy(self.h)
+            self.h = None
+
+    ReleaseOpenCLResources = ReleaseCudaResources
+
+    def __del__(self):
+        try:
+            self.ReleaseCudaResources()
+        except Exception:
+            pass
+
+
+class MultigridPcgSolver:
+    """Flexible CG preconditioned by a V(nu, nu) weighted-Jacobi cycle.
+
+    precision='mixed': FP32 V-cycle (values, vectors, accumulation) inside an
+    FP64 outer loop; precision='f64': everything FP64.  Stop: ||r||/||b|| <= tol,
+    verified on the true FP64 residual at exit.
+    """
+
+    def __init__(self, context: CudaContext, A_levels, P_levels, precision="mixed", fmt="duvi", outer_fmt=None,
+                 nu=2, omega=2.0 / 3.0, omega_mode="spectral", tol=1e-8, max_iterations=500, iterations_per_sync=4,
+                 use_graphs=True):
+        self.context = context
+        ah, ka = _hosts(A_levels)
+        ph, kp = _hosts(P_levels)
+        f = {"csr": N.FORMAT_CSR, "duvi": N.FORMAT_DUVI}
+        cfg = N.MgpcgConfig({"mixed": N.MIXED, "f64": N.F64}[precision], f[fmt], f[outer_fmt or fmt], nu, omega,
+                            {"absolute": N.OMEGA_ABSOLUTE, "spectral": N.OMEGA_SPECTRAL}[omega_mode], max_iterations,
+                            tol, iterations_per_sync, 1 if use_graphs else 0)
+        h = C.c_void_p()
+        N.check(N.lib().dv_mgpcg_create(context.h, len(A_levels), ah, ph, C.byref(cfg), C.byref(h)))
+        del ka, kp
+        self.h = h
+        self.n = A_levels[0].shape[0]
+
+    def Solve(self, b):
+        b = np.ascontiguousarray(b, np.float64)
+        x = np.empty(self.n)
+        st = N.Stats()
+        N.check(N.lib().dv_mgpcg_solve(self.h, N.ptr(b), N.ptr(x), C.byref(st)))
+        return x, _stats(st, "relative residual")
+
+    def solve_device(self, b_ptr, x_ptr):
+        st = N.Stats()
+        N.check(N.lib().dv_mgpcg_solve_device(self.h, b_ptr, x_ptr, C.byref(st)))
+        return _stats(st, "relative residual")
+
+    def release(self):
+        if getattr(self, "h", None) is not None:
+            N.lib().dv_mgpcg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass

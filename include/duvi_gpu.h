@@ -1,0 +1,249 @@
+/*
+ * duvi_gpu.h -- C ABI of the B200 sparse solver path (libduvigpu.so).
+ *
+ * Drop-in replacement for the OpenCL layer of nickreserved/CompressionTests
+ * (src/MGroup.OCL/*.cl and the three solver classes that drive it), callable
+ * from C# through [DllImport] or from any C FFI.  Plain pointers and sizes
+ * only.  One CUDA device per context, one stream per context; every call that
+ * takes host arrays copies them and returns after the device work finished
+ * (like the reference's blocking WriteBuffer/ReadBuffer).  Calls on one
+ * handle are not thread-safe.  There is no CPU fallback: without a usable
+ * GPU every compute call fails with DV_ERR_NO_DEVICE.
+ *
+ * Reference interfaces replaced (file:line inside the reference project):
+ *   OpenCLCsrGeometricMultigridSolver  src/MGroup.Solvers/Multigrid/OpenCLCsrGeometricMultigridSolver.cs:55-83,145-285,334-536
+ *   OpenCLDuViGeometricMultigridSolver src/MGroup.Solvers/Multigrid/OpenCLDuViGeometricMultigridSolver.cs:77-104,172-391,455-751
+ *   OpenCLCsrPcgSolver                 src/MGroup.Solvers/Multigrid/OpenCLCsrPcgSolver.cs:40-45,84-218,250-331
+ *   IGeometricMultigridSolver.Solve    src/MGroup.Solvers/Multigrid/IGeometricMultigridSolver.cs:8
+ *   IOpenCLGeometricMultigridSolver.ReleaseOpenCLResources  IOpenCLGeometricMultigridSolver.cs:5
+ *   DuViCompressedSparseMatrix.Multiply src/MGroup.LinearAlgebra/Matrices/DuViCompressedSparseMatrix.cs:419-441
+ *   OpenCL kernels                     src/MGroup.OCL/CsrCG.cl, CsrGeometricMultigrid.cl, DuViGeometricMultigrid.cl
+ */
+#ifndef DUVI_GPU_H
+#define DUVI_GPU_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define DV_API __attribute__((visibility("default")))
+#else
+#define DV_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ----------------------------------------------------------
+ * Mirrors the exceptions of the reference: DV_ERR_NOT_INITIALIZED for
+ * InvalidOperationException("You must call Initialize(model) first")
+ * (OpenCLCsrGeometricMultigridSolver.cs:336), DV_ERR_UNSUPPORTED for
+ * NotImplementedException (firstLevel != 0, :345), DV_ERR_CUDA for
+ * OpenCLException (OpenCLDuViGeometricMultigridSolver.cs:859). */
+enum {
+    DV_OK = 0,
+    DV_ERR_ARG = -1,
+    DV_ERR_CUDA = -2,
+    DV_ERR_NOT_INITIALIZED = -3,
+    DV_ERR_UNSUPPORTED = -4,
+    DV_ERR_NOMEM = -5,
+    DV_ERR_FORMAT = -6,
+    DV_ERR_NO_DEVICE = -7,
+    DV_ERR_SINGULAR = -8,
+    DV_ERR_TIMEOUT = -9
+};
+
+enum { DV_FORMAT_CSR = 0, DV_FORMAT_DUVI = 1 };
+enum { DV_F64 = 0, DV_F32 = 1, DV_MIXED = 2 };
+enum { DV_SMOOTHER_JACOBI = 0, DV_SMOOTHER_GS_LEX = 1, DV_SMOOTHER_GS_COLOR = 2 };
+enum { DV_TOL_ABS_MAX = 0, DV_TOL_REL_L2 = 1 };
+enum { DV_OMEGA_ABSOLUTE = 0, DV_OMEGA_SPECTRAL = 1 };
+
+typedef struct dv_context dv_context;
+typedef struct dv_matrix dv_matrix;
+typedef struct dv_gmg dv_gmg;
+typedef struct dv_pcg dv_pcg;
+typedef struct dv_mgpcg dv_mgpcg;
+
+/* Host CSR view (int32 indices, float64 values; columns sorted per row). */
+typedef struct {
+    int32_t n_rows, n_cols;
+    const int32_t *rowptr;
+    const int32_t *col;
+    const double *val;
+} dv_csr_host;
+
+typedef struct {
+    int32_t iterations;        /* NumIterationsRequired (cycles or PCG iterations) */
+    int32_t converged;         /* HasConverged: flag bit 1 of the reference kernels */
+    int32_t failed;            /* NaN or |r_i| > 1e50: flag bit 2 (CsrCG.cl:274-276) */
+    int32_t device_status;     /* 0, or DV_ERR_TIMEOUT when a bounded device wait expired */
+    double residual_max;       /* max_i |r_i| of the last checked residual */
+    double residual_norm2;     /* ||r||_2 of the last checked residual */
+    double relative_residual;  /* ||b - A x||_2 / ||b||_2, recomputed in FP64 at exit */
+    double solve_ms;           /* device time of the solve (CUDA events) */
+} dv_stats;
+
+DV_API const char *dv_status_string(int status);
+/* Message of the last failing call on this thread. */
+DV_API const char *dv_last_error(void);
+DV_API int dv_version(void);
+
+/* ---- context (replaces Platform/Device/Program/command queue,
+ *      src/MGroup.OCL/Platform.cs:26-46, Device.cs:32-57) ---------------- */
+DV_API int dv_context_create(int device_ordinal, dv_context **out);
+DV_API int dv_context_destroy(dv_context *ctx);
+DV_API int dv_context_synchronize(dv_context *ctx);
+/* The context's cudaStream_t, for callers that launch their own work. */
+DV_API void *dv_context_stream(dv_context *ctx);
+/* Number of device kernel launches issued by this context so far. */
+DV_API int64_t dv_context_launch_count(const dv_context *ctx);
+
+/* ---- matrices (buffers of OpenCL*Solver.Initialize) ----------------------- */
+typedef struct {
+    int32_t n_rows, n_cols;
+    int64_t nnz;
+    int64_t nblocks;           /* DuVi blocks (0 for CSR) */
+    int64_t nuniq;             /* DuVi distinct values (0 for CSR) */
+    int32_t format;            /* DV_FORMAT_* */
+    int32_t precision;         /* DV_F64 / DV_F32 value storage */
+    int32_t value_index_bits;  /* 8, 16, 32 (DuVi) */
+    int32_t kernel_variant;    /* autotuned launch shape */
+    int64_t device_bytes;      /* bytes one product reads from the matrix arrays */
+} dv_matrix_info;
+
+/* CSR upload (uint row offsets / column indices / double values of
+ * OpenCLCsrPcgSolver.cs:125-130).  precision selects FP64 or FP32 storage. */
+DV_API int dv_matrix_create_csr(dv_context *ctx, const dv_csr_host *a, int32_t precision, dv_matrix **out);
+/* DuVi encode on the host (FromDokRowMajor, OpenCLDuViGeometricMultigridSolver.cs:753-851)
+ * and upload.  value_index_bits: 0 = auto (8 up to 256 distinct values, 16 up
+ * to 65536, else 32); dedup_tol: ToleranceComparer tolerance (1e-10 in the
+ * reference; 0 = exact equality).  Up to 256 distinct values the arrays equal
+ * the reference encoder's bit for bit. */
+DV_API int dv_matrix_create_duvi(dv_context *ctx, const dv_csr_host *a, int32_t precision,
+                                 int32_t value_index_bits, double dedup_tol, dv_matrix **out);
+/* Upload an already encoded DuVi SoA (DuViMat8/16, :16-31). value_indices has
+ * value_index_bits per entry. */
+DV_API int dv_matrix_create_duvi_soa(dv_context *ctx, int32_t n_rows, int32_t n_cols,
+                                     const uint32_t *row_to_col, const uint32_t *row_to_dist,
+                                     const uint32_t *col_idx, int64_t nblocks, const uint8_t *dist,
+                                     int64_t nnz, const void *value_indices, int32_t value_index_bits,
+                                     const double *values, int64_t nuniq, int32_t precision,
+                                     dv_matrix **out);
+DV_API int dv_matrix_get_info(const dv_matrix *m, dv_matrix_info *info);
+/* Copy the DuVi arrays back (value indices widened to uint32). */
+DV_API int dv_matrix_export_duvi(const dv_matrix *m, uint32_t *row_to_col, uint32_t *row_to_dist,
+                                 uint32_t *col_idx, uint8_t *dist, uint32_t *value_indices,
+                                 double *values);
+DV_API int dv_matrix_destroy(dv_matrix *m);
+
+/* y = A x (clear != 0) or y += A x (matrix_vector_product, CsrGeometricMultigrid.cl:49-62,
+ * DuViGeometricMultigrid.cl:122-159).  Host vectors, FP64. */
+DV_API int dv_spmv(dv_matrix *m, const double *x, double *y, int32_t clear);
+/* Same on device pointers (vec_precision DV_F64 or DV_F32), asynchronous on
+ * the context stream. */
+DV_API int dv_spmv_device(dv_matrix *m, const void *x, void *y, int32_t vec_precision, int32_t clear);
+/* r = b - A x (residual, CsrGeometricMultigrid.cl:96-110), device pointers. */
+DV_API int dv_residual_device(dv_matrix *m, const void *b, const void *x, void *r, int32_t vec_precision);
+/* k right-hand sides at once: X and Y are n x k row-interleaved (X[i*k + j]);
+ * the matrix is read once per call.  Device pointers. */
+DV_API int dv_spmm_device(dv_matrix *m, int32_t k, const void *X, void *Y, int32_t vec_precision,
+                          int32_t clear);
+
+/* ---- geometric multigrid (stationary V-cycle, reference semantics) --------
+ * OpenCL{Csr,DuVi}GeometricMultigridSolver.CreateDeepV/CreateSimpleV + Solve.
+ * A has n_levels operators (level 0 finest, the last one is factorised and
+ * solved directly), R and P have n_levels - 1. */
+typedef struct {
+    int32_t smoother;               /* DV_SMOOTHER_* (GaussSeidel flag of the reference) */
+    int32_t format;                 /* DV_FORMAT_CSR / DV_FORMAT_DUVI */
+    int32_t max_cycles;             /* maxCircleIterations */
+    int32_t coarse_relaxation;      /* 1: w = 2/l, l = row-ratio bound of the coarsest A;
+                                       0: w = 2/(1.2 l), l from the power method per level */
+    double tol;                     /* convergenceTolerance, absolute max-norm */
+    int32_t n_steps;                /* length of level_down; 0 = deep V of depth n_levels-1 */
+    const uint8_t *level_down;      /* LevelDown path (true = go coarser) */
+    int32_t n_level_iterations;
+    const int32_t *level_iterations;/* levelIterations (last value repeats) */
+    int32_t cycles_per_sync;        /* cycles run per host convergence read (0 = 16) */
+} dv_gmg_config;
+
+DV_API int dv_gmg_create(dv_context *ctx, int32_t n_levels, const dv_csr_host *A,
+                         const dv_csr_host *R, const dv_csr_host *P, const dv_gmg_config *cfg,
+                         dv_gmg **out);
+/* b: level-0 right-hand side; x0 may be NULL (zero initial guess). */
+DV_API int dv_gmg_solve(dv_gmg *g, const double *b, const double *x0, double *x, dv_stats *stats);
+/* Relaxation factor w applied to D^-1 on level l (for parity checks). */
+DV_API int dv_gmg_omega(const dv_gmg *g, int32_t level, double *omega);
+DV_API int dv_gmg_destroy(dv_gmg *g);
+
+/* ---- Jacobi PCG (OpenCLCsrPcgSolver, FP64, absolute max-norm stop) ------- */
+DV_API int dv_pcg_create(dv_context *ctx, const dv_csr_host *A, int32_t format, int32_t max_iterations,
+                         double tol, dv_pcg **out);
+DV_API int dv_pcg_solve(dv_pcg *p, const double *b, const double *x0, double *x, dv_stats *stats);
+DV_API int dv_pcg_destroy(dv_pcg *p);
+
+/* ---- multigrid-preconditioned flexible PCG (FP64 or mixed precision) ------
+ * Build-defined extension of the reference pieces: an FP64 flexible CG
+ * (FCG(1)) outer loop with true-residual refinement restarts, preconditioned
+ * by one V(nu,nu) cycle of weighted Jacobi.  DV_MIXED runs the V-cycle on
+ * FP32 values and vectors with FP32 accumulation; the outer residual, the
+ * alpha/beta dot products and the solution update stay FP64.  Restriction is
+ * P^T.  The coarsest level is solved with a dense inverse computed from an
+ * LDL^T factorisation. */
+typedef struct {
+    int32_t precision;          /* DV_F64 or DV_MIXED */
+    int32_t format;             /* V-cycle operators: DV_FORMAT_CSR / DV_FORMAT_DUVI */
+    int32_t outer_format;       /* FP64 operator of the outer loop */
+    int32_t nu;                 /* pre- and post-smoothing sweeps */
+    double omega;               /* Jacobi weight */
+    int32_t omega_mode;         /* DV_OMEGA_ABSOLUTE: x += omega D^-1 r;
+                                   DV_OMEGA_SPECTRAL: x += omega (2/l) D^-1 r, l = spectral
+                                   radius estimate of D^-1 A per level */
+    int32_t max_iterations;
+    double tol;                 /* relative 2-norm */
+    int32_t iterations_per_sync;/* outer iterations per host convergence read (0 = 4) */
+    int32_t use_graphs;         /* capture the iteration sequence in a CUDA graph */
+} dv_mgpcg_config;
+
+DV_API int dv_mgpcg_create(dv_context *ctx, int32_t n_levels, const dv_csr_host *A,
+                           const dv_csr_host *P, const dv_mgpcg_config *cfg, dv_mgpcg **out);
+DV_API int dv_mgpcg_solve(dv_mgpcg *s, const double *b, double *x, dv_stats *stats);
+/* Device-resident right-hand side and solution (FP64), context stream. */
+DV_API int dv_mgpcg_solve_device(dv_mgpcg *s, const double *d_b, double *d_x, dv_stats *stats);
+DV_API int dv_mgpcg_destroy(dv_mgpcg *s);
+
+/* ---- structured hex workload generator (FemCantilever3D on unit cubes) ----
+ * Free dofs: all nodes with x index > 0 (FemCantileverBase.cs:137-158), node
+ * ids x-fastest, VTK hexa corner order.  Entry (i,j) = sum over elements in
+ * increasing id of (scale * E_e) * Ke_ij, the summation order of the DOK
+ * assembly (FemCantileverBase.cs:87-104, DokRowMajor.cs:182-207). */
+DV_API int dv_hex_csr_size(const int32_t *ne, int32_t *n_rows, int64_t *nnz);
+DV_API int dv_hex_assemble(const int32_t *ne, const double *elem_E, double scale, double E, double nu,
+                           int32_t *rowptr, int32_t *col, double *val);
+/* Trilinear prolongation between factor-2 grids (fine free x coarse free). */
+DV_API int dv_hex_trilinear_size(const int32_t *ne_fine, int32_t *n_rows, int32_t *n_cols, int64_t *nnz);
+DV_API int dv_hex_trilinear(const int32_t *ne_fine, int32_t *rowptr, int32_t *col, double *val);
+
+/* Restriction and interpolation between two structured Cartesian meshes
+ * (IGeometricMultigridModel.CreateRestrictionAndInterpolationMatrix,
+ * src/MGroup.Solvers/Multigrid/IGeometricMultigridModel.cs:76-194): radial
+ * weights 1 - |(w - c) / h| over the fine nodes in a window around each coarse
+ * node, rows normalised to sum 1 before the fixed dofs are removed, then the
+ * free-dof submatrices (rows/columns in the order of the free-dof lists).
+ * Node ids are x-fastest; dof = dofs_per_node * node + component.  Outputs are
+ * sorted CSR: R is n_coarse_free x n_fine_free, P is n_fine_free x n_coarse_free. */
+DV_API int dv_cartesian_transfer_size(int32_t dim, const int32_t *ne_fine, const int32_t *ne_coarse,
+                                      int32_t dofs_per_node, int32_t n_fine_free, const int32_t *fine_free,
+                                      int32_t n_coarse_free, const int32_t *coarse_free, int64_t *nnz_r,
+                                      int64_t *nnz_p);
+DV_API int dv_cartesian_transfer(int32_t dim, const int32_t *ne_fine, const int32_t *ne_coarse,
+                                 int32_t dofs_per_node, int32_t n_fine_free, const int32_t *fine_free,
+                                 int32_t n_coarse_free, const int32_t *coarse_free, int32_t *r_rowptr,
+                                 int32_t *r_col, double *r_val, int32_t *p_rowptr, int32_t *p_col,
+                                 double *p_val);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DUVI_GPU_H */

@@ -1,0 +1,445 @@
+// CPU oracle: Jacobi weights, LDL^T, MakePath, the CPU geometric multigrid
+// solver, Jacobi PCG, and the FP64 checkers of the build-defined extensions.
+// Test infrastructure only (see oracle.h).
+#include "oracle_internal.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <memory>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+static double norm2(const std::vector<double> &v) {
+    double s = 0.0;
+    for (double a : v) s += a * a;
+    return std::sqrt(s);
+}
+
+// EigenValueUpperBound (power method), GeometricMultigridSolver.cs:80-103.
+extern "C" double or_power_bound(const or_csr *A, const double *inv_diag) {
+    const double percent = 0.05;
+    int32_t n = A->n_rows;
+    std::vector<double> x(n, 1 / std::sqrt((double)n)), y(n);
+    double l = 1;
+    for (;;) {
+        or_csr_spmv(A, x.data(), y.data());
+        for (int32_t i = 0; i < n; ++i) y[i] *= inv_diag[i];
+        double l2 = norm2(y);
+        double s = 1 / l2;
+        for (int32_t i = 0; i < n; ++i) x[i] = y[i] * s;
+        double ratio = l2 / l;
+        if (ratio > 1 - percent && ratio < 1 + percent) {
+            l = ratio > 1 ? l2 * std::pow(ratio, 1 / std::sqrt(percent)) : (l2 * 9 + l) / 10;
+            break;
+        } else l = l2;
+    }
+    return l;
+}
+
+// Dense LDL^T without pivoting (the role of SkylineMatrix.FactorLdl, which is
+// external: GeometricMultigridSolver.cs:255).  Column-oriented; L unit lower in
+// the strict lower triangle, D on the diagonal.
+extern "C" int or_ldl_factor(int32_t n, double *a, double tol) {
+    std::vector<double> v(n);
+    for (int32_t j = 0; j < n; ++j) {
+        double d = a[(size_t)j * n + j];
+        for (int32_t k = 0; k < j; ++k) {
+            v[k] = a[(size_t)j * n + k] * a[(size_t)k * n + k];
+            d -= a[(size_t)j * n + k] * v[k];
+        }
+        if (std::fabs(d) < tol) return -1;
+        a[(size_t)j * n + j] = d;
+        for (int32_t i = j + 1; i < n; ++i) {
+            double s = a[(size_t)i * n + j];
+            for (int32_t k = 0; k < j; ++k) s -= a[(size_t)i * n + k] * v[k];
+            a[(size_t)i * n + j] = s / d;
+        }
+    }
+    return 0;
+}
+extern "C" void or_ldl_solve(int32_t n, const double *f, const double *b, double *x) {
+    for (int32_t i = 0; i < n; ++i) {
+        double s = b[i];
+        for (int32_t k = 0; k < i; ++k) s -= f[(size_t)i * n + k] * x[k];
+        x[i] = s;
+    }
+    for (int32_t i = 0; i < n; ++i) x[i] /= f[(size_t)i * n + i];
+    for (int32_t i = n - 1; i >= 0; --i) {
+        double s = x[i];
+        for (int32_t k = i + 1; k < n; ++k) s -= f[(size_t)k * n + i] * x[k];
+        x[i] = s;
+    }
+}
+
+// MakePath (GeometricMultigridSolver.cs:178-201).
+extern "C" int32_t or_make_path(uint8_t *ld, int32_t n, int32_t cap, int32_t *total_levels, int32_t *first_level) {
+    int32_t cur = 0, tl = 1, fl = 0;
+    for (int32_t i = 0; i < n; ++i) {
+        if (ld[i]) { ++cur; if (cur == tl) ++tl; }
+        else if (cur == 0) { ++fl; ++tl; }
+        else --cur;
+    }
+    int32_t m = n;
+    if (cur > fl) { for (int32_t k = 0; k < cur - fl && m < cap; ++k) ld[m++] = 0; }
+    else if (cur < fl) { for (int32_t k = 0; k < fl - cur && m < cap; ++k) ld[m++] = 1; }
+    *total_levels = tl;
+    *first_level = fl;
+    return m;
+}
+
+// ---------------------------------------------------------------------------
+// GeometricMultigridSolver (CPU), GeometricMultigridSolver.cs:216-418
+// ---------------------------------------------------------------------------
+struct Level {
+    or_csr *A = nullptr, *R = nullptr, *P = nullptr;
+    or_units *Au = nullptr, *Ru = nullptr, *Pu = nullptr;
+    std::vector<double> D;   // relaxed Jacobi preconditioner w * D^-1
+    ~Level() { or_csr_free(A); or_csr_free(R); or_csr_free(P); or_units_free(Au); or_units_free(Ru); or_units_free(Pu); }
+};
+
+struct or_gmg {
+    int gs = 0, duvi = 0;
+    int32_t max_iter = 0;
+    double tol = 0;
+    std::vector<uint8_t> level_down;
+    std::vector<int32_t> level_iter;
+    int32_t total_levels = 0, first_level = 0;
+    std::vector<std::unique_ptr<Level>> lv;
+    std::vector<double> coarse_f;   // dense LDL factor
+    int32_t nc = 0;
+    std::vector<double> b;
+    std::vector<double> omega_scale;
+    bool ok = true;
+};
+
+static void mult(const Level &L, int which, const double *x, double *y, bool duvi) {
+    // which: 0 = A, 1 = R, 2 = P
+    if (duvi) {
+        const or_units *u = which == 0 ? L.Au : which == 1 ? L.Ru : L.Pu;
+        or_units_multiply(u, x, y);
+    } else {
+        const or_csr *a = which == 0 ? L.A : which == 1 ? L.R : L.P;
+        or_csr_spmv(a, x, y);
+    }
+}
+
+extern "C" or_gmg *or_gmg_create(int dim, const int32_t *ne, const double *len, double E, double nu,
+                                 int gauss_seidel, int duvi, int32_t max_cycles, int coarse_relaxation,
+                                 double tol, const uint8_t *level_down, int32_t n_steps,
+                                 const int32_t *level_iterations, int32_t n_li) {
+    or_gmg *g = new or_gmg;
+    g->gs = gauss_seidel; g->duvi = duvi; g->max_iter = max_cycles; g->tol = tol;
+    std::vector<uint8_t> ld(level_down, level_down + n_steps);
+    ld.resize(n_steps + 64);
+    int32_t m = or_make_path(ld.data(), n_steps, (int32_t)ld.size(), &g->total_levels, &g->first_level);
+    ld.resize(m);
+    g->level_down = ld;
+    g->level_iter.assign(level_iterations, level_iterations + n_li);
+    int32_t cur_ne[3] = {ne[0], ne[1], dim == 3 ? ne[2] : 1};
+    or_model *model = or_model_create(dim, cur_ne, len, E, nu, 1.0, nullptr);
+    g->b.resize(or_model_num_free(model));
+    or_model_rhs(model, g->b.data());
+    for (int32_t i = 0; i < g->total_levels - 1; ++i) {
+        auto L = std::make_unique<Level>();
+        const or_csr *K = or_model_kff(model);
+        L->A = or_csr_create(K->n_rows, K->n_cols, K->rowptr.data(), K->col.data(), K->val.data());
+        if (!gauss_seidel) {
+            L->D.resize(K->n_rows);
+            for (int32_t r = 0; r < K->n_rows; ++r) {
+                double d = 0;
+                for (int32_t k = K->rowptr[r]; k < K->rowptr[r + 1]; ++k) if (K->col[k] == r) d = K->val[k];
+                L->D[r] = 1 / d;   // JacobiPreconditioner (:128-134)
+            }
+            if (!coarse_relaxation) {   // RelaxedJacobiPreconditioner (:109-121)
+                double l = 1.2 * or_power_bound(L->A, L->D.data());
+                double s = 2 / l;
+                for (double &v : L->D) v *= s;
+                g->omega_scale.push_back(s);
+            }
+        }
+        int32_t coarse_ne[3] = {cur_ne[0], cur_ne[1], cur_ne[2]};
+        for (int a = 0; a < dim; ++a) if (coarse_ne[a] > 1) coarse_ne[a] >>= 1;   // MakeCartesianCoarserElementsPerAxis
+        or_transfer_create(dim, cur_ne, coarse_ne, &L->R, &L->P);
+        if (duvi) {
+            L->Au = or_units_from_csr(L->A, 1e-10);
+            L->Ru = or_units_from_csr(L->R, 1e-10);
+            L->Pu = or_units_from_csr(L->P, 1e-10);
+        }
+        g->lv.push_back(std::move(L));
+        or_model_free(model);
+        std::copy(coarse_ne, coarse_ne + 3, cur_ne);
+        model = or_model_create(dim, cur_ne, len, E, nu, 1.0, nullptr);
+    }
+    if (!gauss_seidel && coarse_relaxation) {   // RelaxateJacobiPreconditioners (:209-214)
+        double l = or_model_row_ratio_bound(model);
+        double s = 2 / l;
+        for (auto &L : g->lv) for (double &v : L->D) v *= s;
+        g->omega_scale.assign(g->lv.size(), s);
+    }
+    const or_csr *K = or_model_kff(model);
+    g->nc = K->n_rows;
+    g->coarse_f.assign((size_t)g->nc * g->nc, 0.0);
+    for (int32_t r = 0; r < g->nc; ++r)
+        for (int32_t k = K->rowptr[r]; k < K->rowptr[r + 1]; ++k) g->coarse_f[(size_t)r * g->nc + K->col[k]] = K->val[k];
+    if (or_ldl_factor(g->nc, g->coarse_f.data(), 1e-15) != 0) g->ok = false;
+    or_model_free(model);
+    return g;
+}
+extern "C" void or_gmg_free(or_gmg *g) { delete g; }
+extern "C" int32_t or_gmg_num_levels(const or_gmg *g) { return g->total_levels; }
+extern "C" double or_gmg_omega_scale(const or_gmg *g, int32_t l) {
+    return l < (int32_t)g->omega_scale.size() ? g->omega_scale[l] : 0.0;
+}
+
+extern "C" void or_gmg_solve(or_gmg *g, const double *x0, double *xout, int32_t *stats, double *res) {
+    int32_t TL = g->total_levels;
+    stats[0] = 0; stats[1] = 0; stats[2] = 0;
+    if (!g->ok || g->first_level != 0) { stats[2] = 1; return; }
+    int32_t n0 = g->lv[0]->A->n_rows;
+    std::vector<std::vector<double>> x(TL - 1), r(TL);
+    x[0].assign(n0, 0.0);
+    if (x0) std::copy(x0, x0 + n0, x[0].begin());
+    r[0] = g->b;
+    for (int32_t iterations = 0;; ++iterations) {
+        int32_t cur = g->first_level;
+        for (size_t step = 0; step < g->level_down.size(); ++step) {
+            if (cur == TL - 1) {
+                std::vector<double> ec(g->nc);
+                or_ldl_solve(g->nc, g->coarse_f.data(), r[cur].data(), ec.data());
+                Level &L = *g->lv.back();
+                std::vector<double> ef(L.A->n_rows);
+                mult(L, 2, ec.data(), ef.data(), g->duvi);
+                for (size_t i = 0; i < ef.size(); ++i) x[cur - 1][i] = x[cur - 1][i] + ef[i];
+            } else {
+                Level &L = *g->lv[cur];
+                int32_t li = g->level_iter[std::min<size_t>(cur, g->level_iter.size() - 1)];
+                int32_t n = L.A->n_rows;
+                std::vector<double> tmp(n);
+                for (int32_t it = 0; it < li; ++it) {
+                    if (g->gs) {
+                        if (g->duvi) or_units_gs(L.Au, r[cur].data(), x[cur].data());
+                        else or_csr_gs_forward(L.A, r[cur].data(), x[cur].data());
+                    } else {
+                        mult(L, 0, x[cur].data(), tmp.data(), g->duvi);
+                        for (int32_t j = 0; j < n; ++j) tmp[j] = tmp[j] - r[cur][j];
+                        for (int32_t j = 0; j < n; ++j) x[cur][j] -= tmp[j] * L.D[j];
+                    }
+                }
+                if (g->level_down[step]) {
+                    mult(L, 0, x[cur].data(), tmp.data(), g->duvi);
+                    std::vector<double> rf(n);
+                    for (int32_t j = 0; j < n; ++j) rf[j] = r[cur][j] - tmp[j];
+                    if (cur == 0) {
+                        bool converged = true, failed = false;
+                        double mx = 0;
+                        for (int32_t i = 0; i < n; ++i) {
+                            double p = std::fabs(rf[i]);
+                            if (std::isnan(p) || p > 1e50) { failed = true; converged = false; break; }
+                            else if (p > g->tol) { converged = false; break; }
+                        }
+                        for (int32_t i = 0; i < n; ++i) mx = std::max(mx, std::fabs(rf[i]));
+                        if (converged || failed || iterations > g->max_iter) {
+                            stats[0] = iterations; stats[1] = converged; stats[2] = failed;
+                            res[0] = mx; res[1] = norm2(rf);
+                            std::copy(x[0].begin(), x[0].end(), xout);
+                            return;
+                        }
+                    }
+                    r[cur + 1].assign(cur + 1 < TL - 1 ? g->lv[cur + 1]->A->n_rows : g->nc, 0.0);
+                    mult(L, 1, rf.data(), r[cur + 1].data(), g->duvi);
+                    if (cur < TL - 2) x[cur + 1].assign(r[cur + 1].size(), 0.0);
+                } else {
+                    Level &Lp = *g->lv[cur - 1];
+                    std::vector<double> ef(Lp.A->n_rows);
+                    mult(Lp, 2, x[cur].data(), ef.data(), g->duvi);
+                    for (size_t i = 0; i < ef.size(); ++i) x[cur - 1][i] = x[cur - 1][i] + ef[i];
+                }
+            }
+            cur += g->level_down[step] ? 1 : -1;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Jacobi PCG, GMCantileverTests.cs:400-433
+// ---------------------------------------------------------------------------
+extern "C" int32_t or_pcg_jacobi(const or_csr *A, const double *b, double *x, int32_t iterations, double tol) {
+    int32_t n = A->n_rows;
+    std::vector<double> M(n), r(n), z(n), p(n), Ap(n), tmp(n);
+    for (int32_t i = 0; i < n; ++i) {
+        double d = 0;
+        for (int32_t k = A->rowptr[i]; k < A->rowptr[i + 1]; ++k) if (A->col[k] == i) d = A->val[k];
+        M[i] = 1 / d;
+    }
+    or_csr_spmv(A, x, tmp.data());
+    for (int32_t i = 0; i < n; ++i) r[i] = b[i] - tmp[i];
+    for (int32_t i = 0; i < n; ++i) z[i] = M[i] * r[i];
+    p = z;
+    double rz = 0.0;
+    for (int32_t i = 0; i < n; ++i) rz += r[i] * z[i];
+    for (int32_t it = 0; it < iterations; ++it) {
+        or_csr_spmv(A, p.data(), Ap.data());
+        double pap = 0.0;
+        for (int32_t i = 0; i < n; ++i) pap += p[i] * Ap[i];
+        double a = rz / pap;
+        for (int32_t i = 0; i < n; ++i) x[i] = x[i] + p[i] * a;
+        for (int32_t i = 0; i < n; ++i) r[i] = r[i] + Ap[i] * -a;
+        bool nobreak = false;
+        for (int32_t i = 0; i < n; ++i) if (std::fabs(r[i]) > tol) nobreak = true;
+        if (!nobreak) return it;
+        for (int32_t i = 0; i < n; ++i) z[i] = M[i] * r[i];
+        double rz2 = 0.0;
+        for (int32_t i = 0; i < n; ++i) rz2 += r[i] * z[i];
+        double beta = rz2 / rz;
+        for (int32_t i = 0; i < n; ++i) p[i] = p[i] * beta;
+        for (int32_t i = 0; i < n; ++i) p[i] = p[i] + z[i];
+        rz = rz2;
+    }
+    return -1;
+}
+
+// ---------------------------------------------------------------------------
+// Build-defined FP64 checkers
+// ---------------------------------------------------------------------------
+struct McLevel {
+    const or_csr *A, *P;
+    std::vector<double> w;   // omega_eff / a_ii
+};
+
+static void vcycle(std::vector<McLevel> &lv, const std::vector<double> &cf, int32_t nc, int l, int nu,
+                   const double *b, double *x) {
+    if (l == (int)lv.size() - 1) { or_ldl_solve(nc, cf.data(), b, x); return; }
+    const or_csr *A = lv[l].A;
+    int32_t n = A->n_rows;
+    const std::vector<double> &w = lv[l].w;
+    std::vector<double> t(n);
+    for (int32_t i = 0; i < n; ++i) x[i] = w[i] * b[i];
+    for (int s = 1; s < nu; ++s) {
+        or_csr_spmv(A, x, t.data());
+        for (int32_t i = 0; i < n; ++i) x[i] = x[i] + w[i] * (b[i] - t[i]);
+    }
+    or_csr_spmv(A, x, t.data());
+    for (int32_t i = 0; i < n; ++i) t[i] = b[i] - t[i];
+    const or_csr *P = lv[l].P;
+    int32_t m = P->n_cols;
+    std::vector<double> bc(m, 0.0), xc(m);
+    for (int32_t i = 0; i < n; ++i)      // restriction P^T r, rows of P in order
+        for (int32_t k = P->rowptr[i]; k < P->rowptr[i + 1]; ++k) bc[P->col[k]] += P->val[k] * t[i];
+    vcycle(lv, cf, nc, l + 1, nu, bc.data(), xc.data());
+    or_csr_spmv(P, xc.data(), t.data());
+    for (int32_t i = 0; i < n; ++i) x[i] = x[i] + t[i];
+    for (int s = 0; s < nu; ++s) {
+        or_csr_spmv(A, x, t.data());
+        for (int32_t i = 0; i < n; ++i) x[i] = x[i] + w[i] * (b[i] - t[i]);
+    }
+}
+
+static double dot(const std::vector<double> &a, const std::vector<double> &b) {
+    double s = 0.0;
+    for (size_t i = 0; i < a.size(); ++i) s += a[i] * b[i];
+    return s;
+}
+
+extern "C" int32_t or_mg_fcg(int32_t L, or_csr *const *A, or_csr *const *P, double omega_eff, int32_t nu,
+                             const double *b, double *x, int32_t max_iter, double tol, double *relres) {
+    std::vector<McLevel> lv(L);
+    for (int32_t l = 0; l < L; ++l) {
+        lv[l].A = A[l];
+        lv[l].P = l < L - 1 ? P[l] : nullptr;
+        int32_t n = A[l]->n_rows;
+        lv[l].w.resize(n);
+        for (int32_t i = 0; i < n; ++i) {
+            double d = 0;
+            for (int32_t k = A[l]->rowptr[i]; k < A[l]->rowptr[i + 1]; ++k) if (A[l]->col[k] == i) d = A[l]->val[k];
+            lv[l].w[i] = omega_eff / d;
+        }
+    }
+    int32_t nc = A[L - 1]->n_rows;
+    std::vector<double> cf((size_t)nc * nc, 0.0);
+    for (int32_t r = 0; r < nc; ++r)
+        for (int32_t k = A[L - 1]->rowptr[r]; k < A[L - 1]->rowptr[r + 1]; ++k) cf[(size_t)r * nc + A[L - 1]->col[k]] = A[L - 1]->val[k];
+    if (or_ldl_factor(nc, cf.data(), 1e-300) != 0) return -2;
+    int32_t n = A[0]->n_rows;
+    std::vector<double> xv(n, 0.0), r(b, b + n), z(n), p(n, 0.0), q(n, 0.0), w(n);
+    double nb = norm2(r);
+    double pq = 1.0;
+    int32_t it = 0;
+    bool restart = true;
+    *relres = 1.0;
+    while (it < max_iter) {
+        vcycle(lv, cf, nc, 0, nu, r.data(), z.data());
+        double beta = 0.0;
+        if (!restart) beta = -dot(z, q) / pq;
+        double zr = dot(z, r);
+        or_csr_spmv(A[0], z.data(), w.data());
+        for (int32_t i = 0; i < n; ++i) { p[i] = z[i] + beta * p[i]; q[i] = w[i] + beta * q[i]; }
+        pq = dot(p, q);
+        double alpha = zr / pq;
+        for (int32_t i = 0; i < n; ++i) { xv[i] = xv[i] + alpha * p[i]; r[i] = r[i] - alpha * q[i]; }
+        ++it;
+        restart = false;
+        if (norm2(r) / nb <= tol) {
+            or_csr_spmv(A[0], xv.data(), w.data());
+            for (int32_t i = 0; i < n; ++i) w[i] = b[i] - w[i];
+            double rel = norm2(w) / nb;
+            *relres = rel;
+            if (rel <= tol) { std::copy(xv.begin(), xv.end(), x); return it; }
+            r = w;   // refinement restart from the true residual
+            restart = true;
+        }
+    }
+    std::copy(xv.begin(), xv.end(), x);
+    return -1;
+}
+
+extern "C" void or_rho_to_modulus(int64_t n, const double *rho, double *E) {
+    for (int64_t i = 0; i < n; ++i) E[i] = rho[i] * rho[i] * rho[i];
+}
+
+extern "C" void or_adjoint_element_gradient(const int32_t *ne, double E0, double nu, const double *rho,
+                                            const double *u, const double *lam, double *grad) {
+    std::vector<double> ke = element_stiffness(3, E0, nu);
+    int32_t nx = ne[0] + 1, ny = ne[1] + 1;
+    int32_t nel = ne[0] * ne[1] * ne[2];
+    static const int off[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0}, {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};
+    for (int32_t e = 0; e < nel; ++e) {
+        int32_t a = e % ne[0], b = (e / ne[0]) % ne[1], c = e / (ne[0] * ne[1]);
+        double ue[24], le[24];
+        for (int q = 0; q < 8; ++q) {
+            int32_t i = a + off[q][0], j = b + off[q][1], k = c + off[q][2];
+            for (int d = 0; d < 3; ++d) {
+                if (i == 0) { ue[3 * q + d] = 0; le[3 * q + d] = 0; continue; }
+                int32_t f = 3 * ((i - 1) + (nx - 1) * (j + ny * k)) + d;
+                ue[3 * q + d] = u[f]; le[3 * q + d] = lam[f];
+            }
+        }
+        double s = 0.0;
+        for (int i = 0; i < 24; ++i) {
+            double t = 0.0;
+            for (int j = 0; j < 24; ++j) t += ke[i * 24 + j] * ue[j];
+            s += le[i] * t;
+        }
+        grad[e] = -3.0 * rho[e] * rho[e] * s;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Parallel restatement (timed CPU baseline on all host cores)
+// ---------------------------------------------------------------------------
+extern "C" void or_csr_spmv_omp(const or_csr *a, const double *x, double *y) {
+#pragma omp parallel for schedule(static)
+    for (int32_t i = 0; i < a->n_rows; ++i) {
+        double s = 0.0;
+        for (int32_t k = a->rowptr[i]; k < a->rowptr[i + 1]; ++k) s += a->val[k] * x[a->col[k]];
+        y[i] = s;
+    }
+}
+extern "C" int or_omp_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}

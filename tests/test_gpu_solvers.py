@@ -1,0 +1,179 @@
+"""GPU solvers against the CPU oracle.
+
+Reference-semantics solvers (Jacobi PCG, stationary V-cycle GMG with Jacobi
+and Gauss-Seidel) must stop after the same number of iterations as the oracle
+(+-1 where the warp-split SpMV reorders sums) and return the same iterate to
+1e-8 relative.  The multigrid-preconditioned flexible CG (FP64 and mixed)
+must reach the requested FP64 relative residual and agree with the oracle's
+FP64 solution to the stated tolerance.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return np.max(np.abs(a - b)) / np.max(np.abs(b))
+
+
+@pytest.mark.parametrize("fmt", ["csr", "duvi"])
+def test_pcg_matches_oracle(ctx, native, oracle, fmt):
+    m = oracle.Model((16, 4, 4), (20, 1, 1))
+    A, b = m.kff.to_scipy(), m.rhs()
+    x_ref, it_ref = oracle.pcg_jacobi(m.kff, b, 2000, 1e-8)
+    s = native.CudaCsrPcgSolver(ctx, 2000, 1e-8, fmt=fmt).Initialize(A=A, b=b)
+    x, st = s.Solve()
+    assert st.HasConverged and not st.Failed
+    assert abs(st.NumIterationsRequired - it_ref) <= 1
+    assert rel(x, x_ref) < 1e-7
+    assert st.ResidualMaxNorm <= 1e-8
+    # warm start (initialize with x0, CsrCG.cl:191-211)
+    x2, st2 = s.Solve(xInitialGuess=x)
+    assert st2.NumIterationsRequired <= 1
+    s.ReleaseCudaResources()
+
+
+def test_pcg_max_iterations_and_not_initialized(ctx, native, oracle):
+    m = oracle.Model((8, 2, 2), (20, 1, 1))
+    s = native.CudaCsrPcgSolver(ctx, 3, 1e-14).Initialize(A=m.kff.to_scipy(), b=m.rhs())
+    x, st = s.Solve()
+    assert not st.HasConverged and st.NumIterationsRequired == 4   # stops when currentIteration > MaxIterations
+    s.ReleaseCudaResources()
+    with pytest.raises(native.NotInitializedError):
+        s.Solve()
+
+
+def test_pcg_nan_input_fails_not_hangs(ctx, native, oracle):
+    m = oracle.Model((8, 2, 2), (20, 1, 1))
+    b = m.rhs()
+    b[3] = np.nan
+    s = native.CudaCsrPcgSolver(ctx, 100, 1e-8).Initialize(A=m.kff.to_scipy(), b=b)
+    x, st = s.Solve()
+    assert st.Failed and not st.HasConverged
+
+
+def _levels_from_oracle(oracle, ne, depth):
+    A, R, P = [], [], []
+    cur = list(ne)
+    for d in range(depth + 1):
+        A.append(oracle.Model(cur, (20, 1, 1)).kff.to_scipy())
+        if d < depth:
+            nxt = [v >> 1 if v > 1 else v for v in cur]
+            r, p = oracle.transfer(cur, nxt)
+            R.append(r.to_scipy())
+            P.append(p.to_scipy())
+            cur = nxt
+    return A, R, P
+
+
+GMG_CASES = [
+    ("jacobi", "csr", False), ("jacobi", "duvi", False), ("gs", "csr", False), ("gs", "duvi", False),
+    ("jacobi", "csr", True), ("gs", "duvi", True),
+]
+
+
+@pytest.mark.parametrize("smoother,fmt,coarse_relax", GMG_CASES)
+def test_gmg_matches_oracle(ctx, native, oracle, smoother, fmt, coarse_relax):
+    ne, depth, li = (16, 4, 4), 2, 4
+    gs = smoother == "gs"
+    g = oracle.Gmg(ne, (20, 1, 1), gauss_seidel=gs, duvi=(fmt == "duvi"), max_cycles=3000,
+                   coarse_relaxation=coarse_relax, tol=1e-5, depth=depth, level_iterations=li)
+    x_ref, st_ref = g.solve()
+    A, R, P = _levels_from_oracle(oracle, ne, depth)
+    cls = native.CudaDuViGeometricMultigridSolver if fmt == "duvi" else native.CudaCsrGeometricMultigridSolver
+    s = cls(ctx, 3000, 1e-5, [True] * depth + [False] * depth, [li], GaussSeidel=gs)
+    s.b = oracle.Model(ne, (20, 1, 1)).rhs()
+    s.initialize_from_levels(A, R, P, coarse_relax)
+    x, st, _ = s.Solve()
+    assert st.HasConverged == st_ref["converged"] and st.HasConverged
+    tolc = 0 if gs else 1
+    assert abs(st.NumIterationsRequired - st_ref["cycles"]) <= max(tolc, 1)
+    assert rel(x, x_ref) < 1e-6
+    if not gs:
+        assert abs(s.omega(0) / g.omega_scale(0) - 1) < 1e-12
+
+
+def test_gmg_multicolor_converges(ctx, native, oracle):
+    ne = (16, 4, 4)
+    A, R, P = _levels_from_oracle(oracle, ne, 2)
+    s = native.CudaCsrGeometricMultigridSolver(ctx, 3000, 1e-5, [True, True, False, False], [4], GaussSeidel=True,
+                                               gauss_seidel_ordering="multicolor")
+    m = oracle.Model(ne, (20, 1, 1))
+    s.b = m.rhs()
+    s.initialize_from_levels(A, R, P, False)
+    x, st, _ = s.Solve()
+    assert st.HasConverged
+    u = m.uf()
+    assert rel(x, u) < 1e-3
+
+
+def test_gmg_from_model_interface(ctx, native):
+    # CreateDeepV from the product's own model (IGeometricMultigridModel contract)
+    model = native.FemCantilever3D((16, 4, 4), (20, 1, 1))
+    s = native.CudaDuViGeometricMultigridSolver.CreateDeepV(ctx, model, GaussSeidel=False, maxCircleIterations=3000,
+                                                             coarseRelaxation=False, convergenceTolerance=1e-5,
+                                                             depth=2, levelIterations=4)
+    x, st, times = s.Solve()
+    assert st.HasConverged and len(times) == 3
+    u = model.free_displacements()
+    assert rel(x, u) < 1e-3
+    s.ReleaseOpenCLResources()
+    with pytest.raises(native.NotInitializedError):
+        s.Solve()
+
+
+def test_gmg_first_level_not_zero_unsupported(ctx, native):
+    model = native.FemCantilever3D((8, 2, 2))
+    s = native.CudaCsrGeometricMultigridSolver(ctx, 10, 1e-5, [False, True], [2])
+    with pytest.raises(native.NotImplementedFeatureError):
+        s.Initialize(model)
+
+
+@pytest.mark.parametrize("precision,fmt", [("f64", "csr"), ("f64", "duvi"), ("mixed", "duvi"), ("mixed", "csr")])
+def test_mgpcg_matches_oracle(ctx, native, oracle, precision, fmt):
+    ne = (16, 16, 16)
+    A, P = native.hex_hierarchy(ne, coarse_ne=4)
+    b = native.traction_rhs(ne)
+    Ao = [oracle.Csr.from_scipy(a) for a in A]
+    Po = [oracle.Csr.from_scipy(p) for p in P]
+    s = native.MultigridPcgSolver(ctx, A, P, precision=precision, fmt=fmt, nu=2, omega=2 / 3, omega_mode="spectral",
+                                  tol=1e-10, max_iterations=200)
+    x, st = s.Solve(b)
+    assert st.HasConverged and st.RelativeResidual <= 1e-10
+    r = b - A[0] @ x
+    assert np.linalg.norm(r) / np.linalg.norm(b) <= 1e-10
+    x_ref, it_ref, rel_ref = oracle.mg_fcg(Ao, Po, b, 4 / (3 * 3.09), 2, 200, 1e-10)
+    assert it_ref > 0
+    assert rel(x, x_ref) < 1e-8
+    assert st.NumIterationsRequired <= it_ref + 6
+
+
+def test_mgpcg_absolute_omega_and_nu1(ctx, native):
+    ne = (16, 16, 16)
+    A, P = native.hex_hierarchy(ne, coarse_ne=4)
+    b = native.traction_rhs(ne)
+    for nu, mode, om in ((1, "spectral", 2 / 3), (2, "absolute", 0.4), (3, "spectral", 2 / 3)):
+        s = native.MultigridPcgSolver(ctx, A, P, precision="mixed", fmt="duvi", nu=nu, omega=om, omega_mode=mode,
+                                      tol=1e-8, max_iterations=300)
+        x, st = s.Solve(b)
+        assert st.HasConverged and st.RelativeResidual <= 1e-8, (nu, mode)
+
+
+def test_mgpcg_device_api_and_repeat(ctx, native):
+    import torch
+    ne = (16, 16, 16)
+    A, P = native.hex_hierarchy(ne, coarse_ne=4)
+    b = native.traction_rhs(ne)
+    s = native.MultigridPcgSolver(ctx, A, P, precision="mixed", fmt="duvi", tol=1e-8)
+    db = torch.from_numpy(b).cuda()
+    dx = torch.zeros_like(db)
+    torch.cuda.synchronize()
+    its = []
+    for _ in range(3):   # first call eager, later calls through the captured graph
+        st = s.solve_device(db.data_ptr(), dx.data_ptr())
+        its.append(st.NumIterationsRequired)
+        assert st.HasConverged
+    assert its[0] == its[1] == its[2]
+    x = dx.cpu().numpy()
+    assert np.linalg.norm(b - A[0] @ x) / np.linalg.norm(b) <= 1e-8

@@ -1,0 +1,170 @@
+"""GPU SpMV/SpMM and DuVi encoding against the CPU oracle.
+
+Bar: DuVi structure and value indices bit-exact with the oracle encoder
+(FromDokRowMajor, OpenCLDuViGeometricMultigridSolver.cs:753-851); FP64 DuVi
+products bit-exact with the oracle's kernel-order walk
+(DuViGeometricMultigrid.cl:84-98); FP64 CSR products within 1e-12 relative per
+row (the warp-split summation reorders the sum); FP32 within 1e-5 relative to
+the FP64 oracle.
+"""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+pytestmark = pytest.mark.gpu
+
+REL64 = 1e-12
+REL32 = 1e-5
+
+
+def rowwise_rel(y, ref, A_abs, x):
+    scale = np.abs(A_abs) @ np.abs(x) + 1e-300
+    return np.max(np.abs(y - ref) / scale)
+
+
+def random_csr(rng, n, m, density, empty_rows=()):
+    A = sp.random(n, m, density=density, random_state=np.random.RandomState(7), format="csr")
+    A.data = rng.standard_normal(A.nnz)
+    A = A.tolil()
+    for r in empty_rows:
+        A[r, :] = 0
+    A = A.tocsr()
+    A.eliminate_zeros()
+    A.sort_indices()
+    return A
+
+
+@pytest.fixture(scope="module")
+def cantilever(oracle):
+    m = oracle.Model((16, 4, 4), (20, 1, 1))
+    return m, m.kff.to_scipy()
+
+
+def test_diagonal_kat(ctx, native):
+    # GMCantileverOpenCLTests.cs:16-52
+    v = np.arange(16, 0, -1.0)
+    A = sp.csr_matrix((v, np.arange(16), np.arange(17)), shape=(16, 16))
+    for fmt in ("csr", "duvi"):
+        M = native.SparseMatrix(ctx, A, fmt)
+        np.testing.assert_array_equal(M.Multiply(v), v * v)
+
+
+def test_duvi_2x1024_kat(ctx, native):
+    # CompressedSparseMatrixTests.cs:15-39 through the GPU SoA format
+    w = 1024
+    A = sp.csr_matrix(([1, 1, 1, 2, 2, 3, 3.0], [5, 6, 8, w - 24, w - 1, 50, w - 4], [0, 5, 7]), shape=(2, w))
+    x = A.toarray()[0].copy()
+    for fmt in ("csr", "duvi"):
+        y = native.SparseMatrix(ctx, A, fmt).Multiply(x)
+        assert y[0] == 11 and y[1] == 0
+
+
+@pytest.mark.parametrize("bits", [0, 16, 32])
+def test_duvi_encoding_bit_exact(ctx, native, oracle, cantilever, bits):
+    m, A = cantilever
+    M = native.SparseMatrix(ctx, A, "duvi", value_index_bits=bits)
+    got = M.export_duvi()
+    ref = oracle.DuVi(m.kff, 1e-10, bits).arrays()
+    for k in ("row_to_col", "row_to_dist", "col_idx", "dist", "vidx", "values"):
+        np.testing.assert_array_equal(got[k], ref[k], err_msg=k)
+    assert got["vi_bits"] == (8 if bits == 0 else bits)
+
+
+def test_duvi_encoding_many_values(ctx, native, oracle, rng):
+    # moduli drawn log-uniform: ~nnz/2 distinct values, 16/32-bit indices
+    ne = (6, 4, 4)
+    E = 10.0 ** rng.uniform(-2, 0, size=int(np.prod(ne)))
+    A = native.hex_stiffness(ne, E)
+    M = native.SparseMatrix(ctx, A, "duvi")
+    got = M.export_duvi()
+    ref = oracle.DuVi(oracle.Csr.from_scipy(A), 1e-10, 0)
+    r = ref.arrays()
+    assert got["vi_bits"] == ref.vi_bits and ref.vi_bits in (16, 32)
+    for k in ("col_idx", "dist", "vidx", "values"):
+        np.testing.assert_array_equal(got[k], r[k], err_msg=k)
+    x = rng.standard_normal(A.shape[1])
+    np.testing.assert_array_equal(M.Multiply(x), ref.spmv(x))
+
+
+@pytest.mark.parametrize("fmt", ["csr", "duvi"])
+def test_spmv_f64_cantilever(ctx, native, oracle, cantilever, rng, fmt):
+    m, A = cantilever
+    x = rng.standard_normal(A.shape[1])
+    M = native.SparseMatrix(ctx, A, fmt)
+    y = M.Multiply(x)
+    if fmt == "duvi":
+        np.testing.assert_array_equal(y, oracle.DuVi(m.kff).spmv(x))
+        # accumulate mode (clear = 0): y += A x in the reference's order
+        y0 = rng.standard_normal(A.shape[0])
+        got = M.Multiply(x, y0.copy(), clear=False)
+        np.testing.assert_array_equal(got, oracle.DuVi(m.kff).spmv(x, y0.copy(), clear=False))
+    else:
+        assert rowwise_rel(y, m.kff.spmv(x), A, x) <= REL64
+
+
+@pytest.mark.parametrize("fmt", ["csr", "duvi"])
+def test_spmv_f32(ctx, native, cantilever, rng, fmt):
+    m, A = cantilever
+    x = rng.standard_normal(A.shape[1])
+    y = native.SparseMatrix(ctx, A, fmt, "f32").Multiply(x)
+    assert rowwise_rel(y, A @ x, A, x) <= REL32
+
+
+@pytest.mark.parametrize("fmt", ["csr", "duvi"])
+def test_spmv_random_with_empty_rows(ctx, native, oracle, rng, fmt):
+    A = random_csr(rng, 700, 900, 0.02, empty_rows=(0, 5, 699))
+    x = rng.standard_normal(900)
+    y = native.SparseMatrix(ctx, A, fmt, dedup_tol=0.0).Multiply(x)
+    ref = oracle.Csr.from_scipy(A)
+    if fmt == "duvi":
+        np.testing.assert_array_equal(y, oracle.DuVi(ref, 0.0).spmv(x))
+    else:
+        assert rowwise_rel(y, ref.spmv(x), A, x) <= REL64
+    assert y[0] == 0 and y[5] == 0 and y[699] == 0
+
+
+def test_duvi_long_rows_fallback(ctx, native, oracle, rng):
+    # rows longer than one stage (3008 entries) take the unstaged path
+    n, m = 40, 20000
+    rows, cols = [], []
+    for r in range(n):
+        k = 5000 if r in (3, 17) else 50
+        c = np.sort(rng.choice(m, size=k, replace=False))
+        rows += [r] * k
+        cols += list(c)
+    A = sp.csr_matrix((rng.standard_normal(len(rows)), (rows, cols)), shape=(n, m))
+    A.sort_indices()
+    x = rng.standard_normal(m)
+    y = native.SparseMatrix(ctx, A, "duvi", dedup_tol=0.0).Multiply(x)
+    np.testing.assert_array_equal(y, oracle.DuVi(oracle.Csr.from_scipy(A), 0.0).spmv(x))
+
+
+@pytest.mark.parametrize("fmt", ["csr", "duvi"])
+@pytest.mark.parametrize("k", [1, 7, 64, 130])
+def test_spmm(ctx, native, cantilever, rng, fmt, k):
+    import torch
+    m, A = cantilever
+    X = rng.standard_normal((A.shape[1], k))
+    M = native.SparseMatrix(ctx, A, fmt)
+    dX = torch.from_numpy(np.ascontiguousarray(X)).cuda()
+    dY = torch.zeros((A.shape[0], k), dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    M.multiply_many_device(k, dX.data_ptr(), dY.data_ptr())
+    ctx.synchronize()
+    Y = dY.cpu().numpy()
+    ref = A @ X
+    assert np.max(np.abs(Y - ref)) <= REL64 * np.max(np.abs(A) @ np.abs(X))
+
+
+def test_residual_device(ctx, native, cantilever, rng):
+    import torch
+    m, A = cantilever
+    x = rng.standard_normal(A.shape[1])
+    b = rng.standard_normal(A.shape[0])
+    M = native.SparseMatrix(ctx, A, "duvi")
+    dx, db = torch.from_numpy(x).cuda(), torch.from_numpy(b).cuda()
+    dr = torch.zeros_like(db)
+    torch.cuda.synchronize()
+    M.residual_device(db.data_ptr(), dx.data_ptr(), dr.data_ptr())
+    ctx.synchronize()
+    assert rowwise_rel(dr.cpu().numpy(), b - A @ x, A, x) <= REL64

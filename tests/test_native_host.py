@@ -1,0 +1,114 @@
+"""libduvigpu.so without a GPU: symbol exports and the host-side setup code.
+
+The structured assembly, the trilinear and the reference Cartesian transfer
+operators run on the host inside the product library; they must equal the
+oracle's restatement bit for bit, because they feed identical inputs to the
+GPU-vs-oracle parity tests.
+"""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+HEADER = os.path.join(os.path.dirname(__file__), "..", "include", "duvi_gpu.h")
+
+
+def declared_symbols():
+    txt = open(HEADER).read()
+    return sorted(set(re.findall(r"DV_API\s+[^;(]*?\b(dv_\w+)\s*\(", txt)))
+
+
+def test_library_exports_every_declared_symbol(native):
+    lib = native._native.lib()
+    syms = declared_symbols()
+    assert len(syms) >= 30
+    for s in syms:
+        assert hasattr(lib, s), s
+    # and the Python binding declares a signature for each of them
+    assert set(syms) <= set(native._native.exported_symbols()), set(syms) - set(native._native.exported_symbols())
+
+
+def test_status_strings(native):
+    lib = native._native.lib()
+    assert lib.dv_status_string(0) == b"ok"
+    assert lib.dv_status_string(-7) == b"no CUDA device"
+    assert lib.dv_version() >= 10000
+
+
+def test_context_without_device_fails_loudly(native):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(native.NoDeviceError):
+        native.CudaContext(0)
+
+
+@pytest.mark.parametrize("ne", [(4, 2, 2), (5, 3, 4), (8, 8, 8)])
+def test_hex_assembly_bit_exact(native, oracle, ne):
+    A = native.hex_stiffness(ne)
+    B = oracle.hex_stiffness(ne).arrays()
+    np.testing.assert_array_equal(A.indptr, B[0])
+    np.testing.assert_array_equal(A.indices, B[1])
+    np.testing.assert_array_equal(A.data, B[2])
+
+
+def test_hex_assembly_with_moduli_bit_exact(native, oracle, rng):
+    ne = (6, 4, 4)
+    E = 10.0 ** rng.uniform(-2, 0, size=int(np.prod(ne)))
+    A = native.hex_stiffness(ne, E, 2.0)
+    B = oracle.hex_stiffness(ne, E, 2.0).arrays()
+    np.testing.assert_array_equal(A.data, B[2])
+    # and equals the DOK restatement of FemCantileverBase.AssembleGlobalMatrix with densities
+    M = oracle.Model(ne, (6, 4, 4), densities=E * 2.0).kff.arrays()
+    np.testing.assert_array_equal(A.data, M[2])
+
+
+@pytest.mark.parametrize("ne", [(4, 4, 4), (8, 4, 2)])
+def test_trilinear_bit_exact(native, oracle, ne):
+    P = native.hex_trilinear(ne)
+    Q = oracle.hex_trilinear(ne).arrays()
+    np.testing.assert_array_equal(P.indptr, Q[0])
+    np.testing.assert_array_equal(P.indices, Q[1])
+    np.testing.assert_array_equal(P.data, Q[2])
+
+
+@pytest.mark.parametrize("fine,coarse", [((8, 4, 4), (4, 2, 2)), ((6, 2, 2), (3, 1, 1)), ((5, 3, 2), (2, 1, 1)),
+                                         ((16, 1, 2), (8, 1, 1))])
+def test_cartesian_transfer_bit_exact(native, oracle, fine, coarse):
+    mf = native.FemCantilever3D(fine)
+    mc = native.FemCantilever3D(coarse)
+    R, P = native.cartesian_transfer(3, fine, coarse, 3, mf.FindFreeDofs(), mc.FindFreeDofs())
+    Ro, Po = oracle.transfer(fine, coarse)
+    for M, O in ((R, Ro), (P, Po)):
+        a = O.arrays()
+        np.testing.assert_array_equal(M.indptr, a[0])
+        np.testing.assert_array_equal(M.indices, a[1])
+        np.testing.assert_array_equal(M.data, a[2])
+
+
+def test_cantilever_model_matches_oracle(native, oracle):
+    m = native.FemCantilever3D((8, 2, 2), (20, 1, 1))
+    o = oracle.Model((8, 2, 2), (20, 1, 1))
+    np.testing.assert_array_equal(m.FindFreeDofs(), o.free_dofs())
+    np.testing.assert_allclose(m.free_displacements(), o.uf(), rtol=0, atol=1e-15 * np.abs(o.uf()).max())
+    A, b = m.CreateLinearSystem()
+    np.testing.assert_allclose(b, o.rhs(), rtol=1e-12, atol=1e-12 * np.abs(o.rhs()).max())
+
+
+def test_traction_rhs_matches_oracle(native, oracle):
+    ne = (6, 4, 2)
+    np.testing.assert_array_equal(native.traction_rhs(ne), oracle.traction_rhs(ne, ne, (0, 0, -1.0)))
+
+
+def test_hierarchy_shapes(native):
+    A, P = native.hex_hierarchy((16, 16, 16), coarse_ne=4)
+    assert [a.shape[0] for a in A] == [3 * n * (n + 1) ** 2 for n in (16, 8, 4)]
+    for l, p in enumerate(P):
+        assert p.shape == (A[l].shape[0], A[l + 1].shape[0])
+
+
+def test_make_path_matches_oracle(native, oracle):
+    for ld in ([1, 1, 0, 0], [1, 1, 0], [1, 0, 1, 0], [1, 1, 1, 0, 0, 0]):
+        assert native.make_path(ld) == oracle.make_path(ld)
