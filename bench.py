@@ -1,0 +1,433 @@
+#!/usr/bin/env python
+"""Benchmark: multigrid-preconditioned CG time to 1e-8 relative residual on the
+128^3-element hexahedral elasticity cantilever, mixed precision vs FP64, plus
+SpMV HBM throughput of the CSR and DuVi formats on the same operator.
+
+Workload (all synthetic, seeded): unit-cube 8-node hexahedra, E = 1, nu = 0.3,
+3 dofs/node, all nodes of face x = 0 clamped, uniform unit traction (-z) on
+face x = 128 (6,390,144 free dofs, 509,597,550 stored entries).  Hierarchy:
+factor-2 re-discretised levels 128 -> 64 -> 32 -> 16 -> 8 with trilinear
+prolongation and restriction = its transpose, V(2,2) weighted Jacobi with the
+weight 2/3 of the spectrally normalised operator, dense coarse solve.
+
+  value       device time of one solve (b resident in HBM -> x in HBM), mixed
+              precision: FP32 DuVi V-cycle inside the FP64 flexible CG, max over ranks
+  e2e         the same solve through the host API (pinned host b in, host x out)
+  fp64        the plain FP64 path (CSR FP64 operators everywhere) for comparison
+  spmv        isolated SpMV of the finest operator per format/precision, GB/s of
+              the algorithmic bytes and the fraction of the measured HBM peak
+  roofline    the dominant kernel (DuVi FP32 row-bundle decode, the body of every
+              fine-level smoothing sweep), timed with CUDA events on its stream
+
+--impl reference times the CPU restatement of the reference's algorithm
+(oracle/, FP64, all host threads) on the same workload; each step is a
+bounded sample of one outer iteration, scaled to the iteration count.
+Multi-GPU (--gpus N under torchrun): independent replicas, one 128^3 solve per
+rank, no collective on the data path; timing is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "MG-PCG time to 1e-8 rel. residual (mixed FP32/FP64, 128^3 hex elasticity)"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--size", type=int, default=128)
+    p.add_argument("--tol", type=float, default=1e-8)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-fp64", action="store_true")
+    p.add_argument("--no-spmv", action="store_true")
+    p.add_argument("--spmv-only", default=None, metavar="FMT_PREC",
+                   help="only time the SpMV of the finest operator (duvi_f32, duvi_f64, csr_f32, csr_f64): "
+                        "the small case used for ncu captures")
+    return p.parse_args()
+
+
+def dist_init(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        backend = "nccl" if args.impl == "ours" else "gloo"
+        if backend == "nccl":
+            import torch
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    return ws, rank, local
+
+
+def max_over_ranks(v, ws):
+    if ws == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock, power and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = os.path.join("/tmp", f"bench_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """DRAM bytes per launch of the dominant kernel from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "duvi_f32_spmv_128.json")
+    if os.path.exists(p):
+        try:
+            return json.load(open(p)).get("dram_bytes_per_launch")
+        except Exception:
+            return None
+    return None
+
+
+def build_problem(n):
+    import compressiontests_b200 as cb
+    t = time.time()
+    A, P = cb.hex_hierarchy((n, n, n), coarse_ne=8)
+    b = cb.traction_rhs((n, n, n))
+    return A, P, b, time.time() - t
+
+
+def time_events(stream, fn, reps):
+    import torch
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        fn()
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def spmv_table(cb, ctx, A0, reps, peak):
+    import torch
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    out = {}
+    n = A0.shape[0]
+    dom = None
+    for fmt, prec in (("duvi", "f32"), ("duvi", "f64"), ("csr", "f32"), ("csr", "f64")):
+        M = cb.SparseMatrix(ctx, A0, fmt, prec)
+        info = M.info()
+        dt = torch.float32 if prec == "f32" else torch.float64
+        g = torch.Generator(device="cuda").manual_seed(20261203)
+        x = torch.randn(n, dtype=dt, device="cuda", generator=g)
+        y = torch.zeros_like(x)
+        torch.cuda.synchronize()
+        fn = lambda: M.multiply_device(x.data_ptr(), y.data_ptr(), prec)
+        for _ in range(3):
+            fn()
+        ctx.synchronize()
+        ms = time_events(stream, fn, reps)
+        vs = 4 if prec == "f32" else 8
+        alg = info["device_bytes"] + 2 * vs * n
+        gbs = alg / ms / 1e6
+        out[f"{fmt}_{prec}"] = {"ms": round(ms, 4), "algorithmic_bytes": int(alg), "GBps": round(gbs, 1),
+                                "frac_of_peak": round(gbs / peak, 3), "value_index_bits": info["value_index_bits"],
+                                "nblocks": info["nblocks"], "nuniq": info["nuniq"]}
+        if fmt == "duvi" and prec == "f32":
+            dom = (ms, alg)
+        M.release()
+        del x, y
+        torch.cuda.empty_cache()
+    return out, dom
+
+
+def cpu_baseline_sample(A, P, b, iters_needed, threads):
+    """One outer iteration of the oracle's FP64 MG-FCG at full size, scaled to iters_needed."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as O
+    O.build()
+    O.lib().or_set_threads(threads)
+    Ao = [O.Csr.from_scipy(a) for a in A]
+    Po = [O.Csr.from_scipy(p) for p in P]
+    O.mg_fcg(Ao, Po, b, 4 / (3 * 3.09), 2, 1, 1e-30)   # coarse factorisation + one outer iteration
+    return O.lib().or_last_solve_seconds(), 0.0
+
+
+def oracle_problem(O, n):
+    """The same workload built by the oracle's own structured restatement (no product code)."""
+    A, P = [], []
+    ne, scale = n, 1.0
+    while True:
+        A.append(O.hex_stiffness((ne, ne, ne), scale=scale))
+        if ne <= 8 or ne % 2:
+            break
+        P.append(O.hex_trilinear((ne, ne, ne)))
+        ne //= 2
+        scale *= 2.0
+    b = O.traction_rhs((n, n, n), (n, n, n), (0.0, 0.0, -1.0))
+    return A, P, b
+
+
+def run_reference(args):
+    ws, rank, _ = dist_init(args)
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as O
+    O.build()
+    threads = O.lib().or_omp_threads()
+    O.lib().or_set_threads(threads)
+    n = args.size
+    A, P, b = oracle_problem(O, n)
+    # iterations to tolerance of the same algorithm, measured at 32^3 (mesh-independent for multigrid)
+    As, Ps, bs = oracle_problem(O, 32)
+    _, its, _ = O.mg_fcg(As, Ps, bs, 4 / (3 * 3.09), 2, 200, args.tol)
+    times = []
+    for k in range(args.warmup + args.steps):
+        O.mg_fcg(A, P, b, 4 / (3 * 3.09), 2, 1, 1e-30)   # one outer iteration (after the coarse factorisation)
+        per_iter = O.lib().or_last_solve_seconds()
+        if k >= args.warmup:
+            times.append(per_iter * its * 1e3)
+    v = float(np.median(times))
+    line = {"impl": "reference", "metric": METRIC, "value": round(v, 1), "unit": "ms", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(v, 1), "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"mg-pcg hex elasticity {n}^3, V(2,2) Jacobi, FP64, CPU oracle",
+                       "n_dofs": int(A[0].shape[0]), "nnz": int(A[0].nnz), "iterations": int(its)},
+            "cpu_baseline": {"value": round(v, 1), "unit": "ms", "cores": threads, "kind": "port",
+                             "sample": f"one outer FCG iteration (V(2,2) cycle + FP64 SpMV) at {n}^3 per step, "
+                                       f"x {its} iterations (count of the same solver at 32^3)"},
+            "e2e": {"value": round(v, 1), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import torch
+    ws, rank, local = dist_init(args)
+    torch.cuda.set_device(local)
+    import compressiontests_b200 as cb
+    peak, peak_kind = measured_peaks()
+    n = args.size
+    A, P, b, t_build = build_problem(n)
+    ctx = cb.CudaContext(local)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    nf = A[0].shape[0]
+
+    def make(precision, fmt):
+        return cb.MultigridPcgSolver(ctx, A, P, precision=precision, fmt=fmt, outer_fmt=fmt, nu=2, omega=2 / 3,
+                                     omega_mode="spectral", tol=args.tol, max_iterations=500)
+
+    db = torch.from_numpy(b).to(f"cuda:{local}")
+    dx = torch.zeros_like(db)
+    torch.cuda.synchronize()
+
+    def timed(solver, steps, warmup):
+        st = None
+        for _ in range(warmup):
+            st = solver.solve_device(db.data_ptr(), dx.data_ptr())
+        barrier(ws)
+        torch.cuda.synchronize()
+        ctx.synchronize()
+        l0 = ctx.launch_count()
+        sampler = ClockSampler(local)
+        sampler.start()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        its, rel = [], []
+        for _ in range(steps):
+            st = solver.solve_device(db.data_ptr(), dx.data_ptr())
+            its.append(st.NumIterationsRequired)
+            rel.append(st.RelativeResidual)
+            assert st.HasConverged, st
+        e1.record(stream)
+        e1.synchronize()
+        clocks = sampler.stop()
+        launches = ctx.launch_count() - l0
+        ms = e0.elapsed_time(e1) / steps
+        barrier(ws)
+        return max_over_ranks(ms, ws), its, rel, launches, clocks
+
+    t = time.time()
+    mixed = make("mixed", "duvi")
+    t_setup = time.time() - t
+    ms_mixed, its_mixed, rel_mixed, launches, clocks = timed(mixed, args.steps, args.warmup)
+    x_mixed = dx.cpu().numpy()
+    true_rel = float(np.linalg.norm(b - A[0] @ x_mixed) / np.linalg.norm(b))
+
+    # e2e through the host API: pinned host b -> device, solve, device x -> pinned host
+    hb = torch.from_numpy(b).pin_memory()
+    hx = torch.empty_like(hb).pin_memory()
+    bp, xp = hb.numpy(), hx.numpy()
+    for _ in range(1):
+        mixed.Solve(bp)
+    barrier(ws)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        import ctypes as C
+        st = cb._native.Stats()
+        cb._native.check(cb._native.lib().dv_mgpcg_solve(mixed.h, C.c_void_p(hb.data_ptr()), C.c_void_p(hx.data_ptr()),
+                                                         C.byref(st)))
+        assert st.converged
+    e1.record(stream)
+    e1.synchronize()
+    ms_e2e = max_over_ranks(e0.elapsed_time(e1) / args.steps, ws)
+    mixed.release()
+
+    fp64 = {}
+    if not args.no_fp64:
+        for fmt in ("csr", "duvi"):
+            s = make("f64", fmt)
+            ms, its, rel, _, _ = timed(s, max(2, args.steps // 2), 1)
+            fp64[fmt] = {"ms": round(ms, 2), "iterations": its[-1], "rel_residual": rel[-1],
+                         "mixed_speedup": round(ms / ms_mixed, 2)}
+            s.release()
+
+    spmv, dom = ({}, None) if args.no_spmv else spmv_table(cb, ctx, A[0], 20, peak)
+    roof = None
+    if dom is not None:
+        ms_dom, alg = dom
+        achieved = alg / ms_dom / 1e6
+        roof = {"kernel": "k_duvi<u8,float> (DuVi FP32 row-bundle SpMV; fine-level Jacobi sweep body)",
+                "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 3), "traffic": ncu_traffic(), "peak_kind": peak_kind,
+                "algorithmic_bytes_per_launch": int(alg), "avg_launch_ms": round(ms_dom, 4)}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        try:
+            sys.path.insert(0, os.path.join(ROOT, "oracle"))
+            per_iter, _ = cpu_baseline_sample(A, P, b, its_mixed[-1], 1)
+            v = per_iter * its_mixed[-1] * 1e3
+            cpu = {"value": round(v, 1), "unit": "ms", "cores": 1, "kind": "port",
+                   "sample": f"one outer FP64 FCG iteration of the oracle (single thread) at {n}^3, "
+                             f"x {its_mixed[-1]} iterations"}
+        except Exception as e:  # the baseline must not hide the GPU result
+            cpu = {"value": None, "unit": "ms", "cores": 1, "kind": "port", "sample": f"failed: {e}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(ms_mixed, 3), "unit": "ms", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms_mixed, 3), "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+            "config": {"workload": f"mg-pcg hex elasticity {n}^3 (unit traction, x=0 clamped), V(2,2) Jacobi, "
+                                   "FP32 DuVi V-cycle in FP64 flexible CG, 5 levels to 8^3",
+                       "n_dofs": int(nf), "nnz": int(A[0].nnz), "tol": args.tol, "levels": len(A),
+                       "l2_flush": "inputs larger than L2 (DuVi operator 1.35 GB)", "parallelism": f"replicas x{ws}"},
+            "iterations": its_mixed[-1], "relative_residual_fp64": true_rel,
+            "e2e": {"value": round(ms_e2e, 3), "unit": "ms", "h2d_bytes_per_step": int(8 * nf),
+                    "d2h_bytes_per_step": int(8 * nf)},
+            "gpu_launches": int(launches), "fp64": fp64, "spmv": spmv, "roofline": roof, "cpu_baseline": cpu,
+            "clocks": clocks, "setup_s": {"hierarchy": round(t_build, 1), "solver": round(t_setup, 1)},
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def run_spmv_only(args):
+    import torch
+    import compressiontests_b200 as cb
+    fmt, prec = args.spmv_only.split("_")
+    n = args.size
+    A0 = cb.hex_stiffness((n, n, n))
+    ctx = cb.CudaContext(0)
+    M = cb.SparseMatrix(ctx, A0, fmt, prec)
+    info = M.info()
+    dt = torch.float32 if prec == "f32" else torch.float64
+    g = torch.Generator(device="cuda").manual_seed(20261203)
+    x = torch.randn(A0.shape[0], dtype=dt, device="cuda", generator=g)
+    y = torch.zeros_like(x)
+    torch.cuda.synchronize()
+    fn = lambda: M.multiply_device(x.data_ptr(), y.data_ptr(), prec)
+    for _ in range(args.warmup):
+        fn()
+    ctx.synchronize()
+    ms = time_events(torch.cuda.ExternalStream(ctx.stream), fn, args.steps)
+    alg = info["device_bytes"] + 2 * (4 if prec == "f32" else 8) * A0.shape[0]
+    print(json.dumps({"spmv": args.spmv_only, "size": n, "ms": ms, "algorithmic_bytes": int(alg),
+                      "GBps": alg / ms / 1e6, "launch_shape": info["kernel_variant"]}), flush=True)
+    M.release()
+    ctx.close()
+
+
+if __name__ == "__main__":
+    a = parse()
+    if a.spmv_only:
+        run_spmv_only(a)
+    elif a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)

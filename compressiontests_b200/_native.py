@@ -113,6 +113,7 @@ _SIGNATURES = {
     "dv_mgpcg_create": (C.c_int, [_vp, C.c_int32, _P(CsrHost), _P(CsrHost), _P(MgpcgConfig), _P(_vp)]),
     "dv_mgpcg_solve": (C.c_int, [_vp, _vp, _vp, _P(Stats)]),
     "dv_mgpcg_solve_device": (C.c_int, [_vp, _vp, _vp, _P(Stats)]),
+    "dv_mgpcg_omega": (C.c_int, [_vp, C.c_int32, _P(C.c_double)]),
     "dv_mgpcg_destroy": (C.c_int, [_vp]),
     "dv_hex_csr_size": (C.c_int, [_vp, _P(C.c_int32), _P(C.c_int64)]),
     "dv_hex_assemble": (C.c_int, [_vp, _vp, C.c_double, C.c_double, C.c_double, _vp, _vp, _vp]),

@@ -72,8 +72,13 @@ struct DevMem {
     void alloc(size_t b) {
         release();
         // 64 bytes of tail padding: staged loads round ranges up to 16-byte units.
-        if (b) DV_CUDA(cudaMalloc(&p, b + 64));
-        if (b) DV_CUDA(cudaMemset(p, 0, b + 64));
+        // The zero fill runs on the legacy stream, which does not order against the
+        // non-blocking context streams: finish it before anyone writes the buffer.
+        if (b) {
+            DV_CUDA(cudaMalloc(&p, b + 64));
+            DV_CUDA(cudaMemsetAsync(p, 0, b + 64, 0));
+            DV_CUDA(cudaStreamSynchronize(0));
+        }
         bytes = b;
     }
     void release() {
@@ -100,6 +105,7 @@ struct dv_context {
     int max_smem_optin = 0;
     int64_t launches = 0;
     DevMem status;       // int[4]: device error word, bounded-wait sentinel
+    DevMem red;          // default grid-reduction workspace (ticket + partials)
     void count(int64_t n = 1) { launches += n; }
 };
 
@@ -130,6 +136,7 @@ struct dv_matrix {
     DevMem row_to_col, row_to_dist, col_idx, dist, vidx, values;
     DevMem bundles;            // int32 row starts of row bundles (+ sentinel)
     int32_t nbundles = 0;
+    int duvi_batch = 4;        // entries per gather batch in the decode loop (9 when most blocks hold 9)
     DuviHost host;             // kept for export
     // shared
     DevMem diag;               // FP64 diagonal (0 where absent)

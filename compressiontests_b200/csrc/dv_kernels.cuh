@@ -277,6 +277,7 @@ __global__ void __launch_bounds__(kThreads) k_csr(const int32_t *__restrict__ rp
                                                   const MT *__restrict__ va, int32_t n, Gather g, Op op,
                                                   const int *__restrict__ done, double *partials, unsigned *ticket) {
     if (done && *(volatile const int *)done) return;
+    constexpr int U = 4;   // entries per lane per step: all index/value loads, then all gathers, then the FMAs
     double red[Op::NRED > 0 ? Op::NRED : 1];
 #pragma unroll
     for (int i = 0; i < (Op::NRED > 0 ? Op::NRED : 1); ++i) red[i] = 0.0;
@@ -285,8 +286,21 @@ __global__ void __launch_bounds__(kThreads) k_csr(const int32_t *__restrict__ rp
     for (int32_t row = blockIdx.x * gpb + threadIdx.x / TPR; row < n; row += gridDim.x * gpb) {
         const int32_t s0 = __ldg(rp + row), s1 = __ldg(rp + row + 1);
         AT s = (TPR == 1) ? op.init(row) : AT(0);
-#pragma unroll 4
-        for (int32_t k = s0 + sub; k < s1; k += TPR) s = madd<AT>(s, (AT)__ldg(va + k), g((uint32_t)__ldg(ci + k)));
+        for (int32_t base = s0 + sub; base < s1; base += TPR * U) {
+            int32_t c[U];
+            AT v[U], xv[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int32_t k = base + u * TPR;
+                c[u] = k < s1 ? __ldcs(ci + k) : 0;
+                v[u] = k < s1 ? (AT)__ldcs(va + k) : AT(0);
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) xv[u] = (base + u * TPR < s1) ? g((uint32_t)c[u]) : AT(0);
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+                if (base + u * TPR < s1) s = madd<AT>(s, v[u], xv[u]);
+        }
         s = group_sum<TPR>(s);
         if (TPR > 1) s = op.init(row) + s;
         if (sub == 0) op.row(row, s, red);
@@ -326,8 +340,8 @@ __device__ __forceinline__ void copy16(void *dst, const void *src, int nbytes16,
     for (int i = lane; i < nbytes16; i += 32) d[i] = __ldg(s + i);
 }
 
-template <class VI, class AT, class Gather, class Op, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32) k_duvi(DuviArgs A, Gather g, Op op, const int *__restrict__ done,
+template <class VI, class AT, class Gather, class Op, int WARPS, int BATCH>
+__global__ void __launch_bounds__(WARPS * 32, 2) k_duvi(DuviArgs A, Gather g, Op op, const int *__restrict__ done,
                                                      double *partials, unsigned *ticket) {
     if (done && *(volatile const int *)done) return;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -373,19 +387,33 @@ __global__ void __launch_bounds__(WARPS * 32) k_duvi(DuviArgs A, Gather g, Op op
                 const uint32_t b_end = __ldg(A.row_to_col + row + 1) - ca0;
                 AT s = op.init(row);
                 for (uint32_t b = rc_l - ca0; b < b_end; ++b) {
-                    uint32_t c = scol[b];
-                    int cnt = sdist[di];
-                    AT v = kSmemTable ? tab[svi[dv]] : __ldg(gtab + svi[dv]);
-                    s = madd<AT>(s, v, g(c));
-                    for (int k = 0; k < cnt; ++k) {
-                        ++di;
-                        ++dv;
-                        c += sdist[di] + 1u;
-                        v = kSmemTable ? tab[svi[dv]] : __ldg(gtab + svi[dv]);
-                        s = madd<AT>(s, v, g(c));
+                    const uint32_t n = sdist[di] + 1u;   // entries of the block
+                    uint32_t cc = scol[b];
+                    uint32_t k = 0;
+                    // batches of BATCH entries: column prefix from the gap bytes, then
+                    // BATCH independent gathers, then the FMAs in entry order
+                    for (; k + BATCH <= n; k += BATCH) {
+                        uint32_t cols[BATCH];
+                        AT vals[BATCH], xs[BATCH];
+#pragma unroll
+                        for (int u = 0; u < BATCH; ++u) {
+                            cols[u] = cc;
+                            cc += sdist[di + k + u + 1] + 1u;   // gap to the next entry (the last read is unused)
+                            vals[u] = kSmemTable ? tab[svi[dv + k + u]] : __ldg(gtab + svi[dv + k + u]);
+                        }
+#pragma unroll
+                        for (int u = 0; u < BATCH; ++u) xs[u] = g(cols[u]);
+#pragma unroll
+                        for (int u = 0; u < BATCH; ++u) s = madd<AT>(s, vals[u], xs[u]);
                     }
-                    ++di;
-                    ++dv;
+                    for (; k < n; ++k) {
+                        const AT v = kSmemTable ? tab[svi[dv + k]] : __ldg(gtab + svi[dv + k]);
+                        const AT xv = g(cc);
+                        cc += sdist[di + k + 1] + 1u;
+                        s = madd<AT>(s, v, xv);
+                    }
+                    di += n;
+                    dv += n;
                 }
                 op.row(row, s, red);
             }
@@ -434,11 +462,11 @@ struct LaunchEnv {
     int max_blocks;
 };
 
-template <class VI, class AT, class Gather, class Op>
+template <class VI, class AT, class Gather, class Op, int BATCH>
 void launch_duvi_vi(const LaunchEnv &e, const dv_matrix *m, Gather g, Op op) {
     constexpr int W = sizeof(VI) == 4 ? kDuviWarps32 : kDuviWarps;
     const size_t smem = duvi_smem_bytes<VI, AT>(W);
-    auto kern = k_duvi<VI, AT, Gather, Op, W>;
+    auto kern = k_duvi<VI, AT, Gather, Op, W, BATCH>;
     static bool attr_set = false;   // per instantiation
     if (!attr_set) {
         DV_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -479,9 +507,16 @@ void launch_csr_tpr(const LaunchEnv &e, const dv_matrix *m, Gather g, Op op) {
 template <class AT, class Gather, class Op>
 void launch_rows(const LaunchEnv &e, const dv_matrix *m, Gather g, Op op) {
     if (m->format == DV_FORMAT_DUVI) {
-        if (m->vi_bits == 8) launch_duvi_vi<uint8_t, AT>(e, m, g, op);
-        else if (m->vi_bits == 16) launch_duvi_vi<uint16_t, AT>(e, m, g, op);
-        else launch_duvi_vi<uint32_t, AT>(e, m, g, op);
+        // batch width matched to the dominant block length (chosen at upload)
+        if (m->duvi_batch == 9) {
+            if (m->vi_bits == 8) launch_duvi_vi<uint8_t, AT, Gather, Op, 9>(e, m, g, op);
+            else if (m->vi_bits == 16) launch_duvi_vi<uint16_t, AT, Gather, Op, 9>(e, m, g, op);
+            else launch_duvi_vi<uint32_t, AT, Gather, Op, 9>(e, m, g, op);
+        } else {
+            if (m->vi_bits == 8) launch_duvi_vi<uint8_t, AT, Gather, Op, 4>(e, m, g, op);
+            else if (m->vi_bits == 16) launch_duvi_vi<uint16_t, AT, Gather, Op, 4>(e, m, g, op);
+            else launch_duvi_vi<uint32_t, AT, Gather, Op, 4>(e, m, g, op);
+        }
         return;
     }
     switch (m->csr_tpr) {

@@ -3,7 +3,7 @@
 
 #include <algorithm>
 #include <cstdio>
-#include <mutex>
+#include <cstdlib>
 
 static thread_local std::string g_last_error;
 void dv_set_last_error(const std::string &m) { g_last_error = m; }
@@ -50,6 +50,7 @@ extern "C" DV_API int dv_context_create(int device, dv_context **out) {
         ctx->max_smem_optin = (int)prop.sharedMemPerBlockOptin;
         DV_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
         ctx->status.alloc(64);
+        ctx->red.alloc(sizeof(double) * dvk::kMaxRed * ctx->num_sms * 16 + 64);
         *out = ctx.release();
     });
 }
@@ -60,6 +61,7 @@ extern "C" DV_API int dv_context_destroy(dv_context *ctx) {
         cudaSetDevice(ctx->device);
         cudaStreamSynchronize(ctx->stream);
         ctx->status.release();
+        ctx->red.release();
         cudaStreamDestroy(ctx->stream);
         delete ctx;
     });
@@ -136,6 +138,19 @@ static void finish_duvi_upload(dv_matrix *m, cudaStream_t s) {
         upload(m->values, f.data(), 4 * f.size(), s);
         DV_CUDA(cudaStreamSynchronize(s));
     }
+    // most frequent block length picks the batch width of the decode loop
+    {
+        std::vector<int64_t> hist(257, 0);
+        for (size_t r = 0; r + 1 < h.row_to_col.size(); ++r) {
+            uint32_t di = h.row_to_dist[r];
+            for (uint32_t bl = h.row_to_col[r]; bl < h.row_to_col[r + 1]; ++bl) {
+                hist[h.dist[di] + 1]++;
+                di += h.dist[di] + 1u;
+            }
+        }
+        int mode = (int)(std::max_element(hist.begin(), hist.end()) - hist.begin());
+        m->duvi_batch = (mode >= 9 && mode % 9 == 0) ? 9 : 4;
+    }
     std::vector<int32_t> b;
     dv_make_bundles(h, m->n_rows, m->vi_bits, b);
     m->nbundles = (int32_t)b.size() - 1;
@@ -144,6 +159,67 @@ static void finish_duvi_upload(dv_matrix *m, cudaStream_t s) {
     const size_t vs = m->precision == DV_F64 ? 8 : 4;
     m->device_bytes = (int64_t)(m->nnz * (1 + m->vi_bits / 8) + 4 * m->nblocks + 8 * ((int64_t)m->n_rows + 1) +
                                 vs * m->nuniq);
+}
+
+static dvk::LaunchEnv env_for(dv_context *ctx, const int *done = nullptr) {
+    dvk::LaunchEnv e;
+    e.ctx = ctx;
+    e.stream = ctx->stream;
+    e.done = done;
+    e.ticket = reinterpret_cast<unsigned *>(ctx->red.as<char>());
+    e.partials = reinterpret_cast<double *>(ctx->red.as<char>() + 64);
+    e.max_blocks = ctx->num_sms * 16;
+    return e;
+}
+
+// Project autotuner: time every launch shape of the SpMV on this matrix with
+// CUDA events (FP32 or FP64 vectors as stored) and keep the fastest.  Runs once
+// per matrix at upload; small matrices keep the heuristic choice.
+static void autotune(dv_matrix *m) {
+    const char *env = getenv("DV_AUTOTUNE");
+    if (env && env[0] == '0') return;
+    if (m->n_rows < 100000 || m->n_rows != m->n_cols) return;
+    dv_context *ctx = m->ctx;
+    cudaStream_t s = ctx->stream;
+    const size_t vs = m->precision == DV_F64 ? 8 : 4;
+    DevMem x(vs * (size_t)m->n_cols), y(vs * (size_t)m->n_rows);
+    auto e = env_for(ctx);
+    auto run = [&] {
+        if (m->precision == DV_F64) {
+            dvk::OpSpmv<double, double> op;
+            op.y = y.as<double>();
+            op.clear = 1;
+            dvk::launch_rows<double>(e, m, dvk::GatherVec<double, double>{x.as<double>()}, op);
+        } else {
+            dvk::OpSpmv<float, float> op;
+            op.y = y.as<float>();
+            op.clear = 1;
+            dvk::launch_rows<float>(e, m, dvk::GatherVec<float, float>{x.as<float>()}, op);
+        }
+    };
+    std::vector<int> cand = m->format == DV_FORMAT_CSR ? std::vector<int>{8, 16, 32} : std::vector<int>{4, 9};
+    cudaEvent_t e0, e1;
+    DV_CUDA(cudaEventCreate(&e0));
+    DV_CUDA(cudaEventCreate(&e1));
+    float best = 1e30f;
+    int best_v = m->format == DV_FORMAT_CSR ? m->csr_tpr : m->duvi_batch;
+    for (int v : cand) {
+        if (m->format == DV_FORMAT_CSR) m->csr_tpr = v;
+        else m->duvi_batch = v;
+        run();
+        DV_CUDA(cudaEventRecord(e0, s));
+        for (int k = 0; k < 3; ++k) run();
+        DV_CUDA(cudaEventRecord(e1, s));
+        DV_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best) { best = ms; best_v = v; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (m->format == DV_FORMAT_CSR) m->csr_tpr = best_v;
+    else m->duvi_batch = best_v;
+    ctx->launches -= (int64_t)cand.size() * 4;   // tuning launches are not part of any solve
 }
 
 dv_matrix *dv_matrix_build(dv_context *ctx, const dv_csr_host &a, int format, int precision, int vi_bits, double tol) {
@@ -182,6 +258,7 @@ dv_matrix *dv_matrix_build(dv_context *ctx, const dv_csr_host &a, int format, in
         upload(m->diag, m->host_diag.data(), 8 * m->host_diag.size(), s);
         DV_CUDA(cudaStreamSynchronize(s));
     }
+    autotune(m.get());
     return m.release();
 }
 
@@ -312,34 +389,6 @@ extern "C" DV_API int dv_matrix_destroy(dv_matrix *m) {
 // ---------------------------------------------------------------------------
 // products
 // ---------------------------------------------------------------------------
-namespace {
-struct CtxReduce {   // per-context default reduction workspace (lazily created)
-    DevMem mem;
-};
-std::mutex g_ws_mutex;
-std::vector<std::pair<dv_context *, std::unique_ptr<CtxReduce>>> g_ws;
-
-dvk::LaunchEnv env_for(dv_context *ctx, const int *done = nullptr) {
-    std::lock_guard<std::mutex> lk(g_ws_mutex);
-    CtxReduce *w = nullptr;
-    for (auto &p : g_ws) if (p.first == ctx) w = p.second.get();
-    if (!w) {
-        auto n = std::make_unique<CtxReduce>();
-        n->mem.alloc(sizeof(double) * dvk::kMaxRed * ctx->num_sms * 16 + 64);
-        w = n.get();
-        g_ws.emplace_back(ctx, std::move(n));
-    }
-    dvk::LaunchEnv e;
-    e.ctx = ctx;
-    e.stream = ctx->stream;
-    e.done = done;
-    e.ticket = reinterpret_cast<unsigned *>(w->mem.as<char>());
-    e.partials = reinterpret_cast<double *>(w->mem.as<char>() + 64);
-    e.max_blocks = ctx->num_sms * 16;
-    return e;
-}
-}  // namespace
-
 dvk::LaunchEnv dv_default_env(dv_context *ctx) { return env_for(ctx); }
 
 static void spmv_device(dv_matrix *m, const void *x, void *y, int vprec, int clear) {

@@ -214,12 +214,12 @@ template <class T>
 struct OpPower {
     static constexpr int NRED = 1;
     static constexpr unsigned MAXMASK = 0;
-    const double *__restrict__ dinv;
+    const double *__restrict__ diag;
     T *__restrict__ y;
     SolverScalars *sc;
     __device__ __forceinline__ T init(int32_t) const { return T(0); }
     __device__ __forceinline__ void row(int32_t i, T s, double *red) const {
-        T v = (T)(dinv[i] * (double)s);
+        T v = (T)((double)s / diag[i]);
         y[i] = v;
         red[0] += (double)v * (double)v;
     }
@@ -721,6 +721,14 @@ extern "C" DV_API int dv_mgpcg_solve(dv_mgpcg *s, const double *b, double *x, dv
         else mgpcg_solve_impl<double>(s, *s->v64, stats);
         DV_CUDA(cudaMemcpyAsync(x, s->x.p, nb, cudaMemcpyDeviceToHost, st));
         DV_CUDA(cudaStreamSynchronize(st));
+    });
+}
+
+extern "C" DV_API int dv_mgpcg_omega(const dv_mgpcg *s, int32_t level, double *omega) {
+    return dv_guard([&] {
+        DV_REQUIRE(s && omega, DV_ERR_ARG, "null argument");
+        DV_REQUIRE(level >= 0 && level < (int32_t)s->omega_eff.size(), DV_ERR_ARG, "level out of range");
+        *omega = s->omega_eff[level];
     });
 }
 

@@ -143,6 +143,7 @@ class _GeometricMultigridBase:
         N.check(N.lib().dv_gmg_create(self.context.h, len(A), ah, rh, ph, C.byref(cfg), C.byref(h)))
         del ka, kr, kp
         self.h = h
+        self.context.register(self)
         self.LevelDoFs = [a.shape[0] for a in A]
 
     def omega(self, level):
@@ -166,6 +167,7 @@ class _GeometricMultigridBase:
             self.h = None
 
     ReleaseOpenCLResources = ReleaseCudaResources
+    release = ReleaseCudaResources
 
     def __del__(self):
         try:
@@ -204,6 +206,7 @@ class CudaCsrPcgSolver:
                                       C.byref(h)))
         del keep
         self.h = h
+        self.context.register(self)
         self.b = None if b is None else np.asarray(b, np.float64)
         self.DoFs = A.shape[0]
         return self
@@ -224,6 +227,7 @@ class CudaCsrPcgSolver:
             self.h = None
 
     ReleaseOpenCLResources = ReleaseCudaResources
+    release = ReleaseCudaResources
 
     def __del__(self):
         try:
@@ -254,7 +258,13 @@ class MultigridPcgSolver:
         N.check(N.lib().dv_mgpcg_create(context.h, len(A_levels), ah, ph, C.byref(cfg), C.byref(h)))
         del ka, kp
         self.h = h
+        context.register(self)
         self.n = A_levels[0].shape[0]
+
+    def omega(self, level):
+        w = C.c_double()
+        N.check(N.lib().dv_mgpcg_omega(self.h, level, C.byref(w)))
+        return w.value
 
     def Solve(self, b):
         b = np.ascontiguousarray(b, np.float64)

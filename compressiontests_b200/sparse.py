@@ -9,6 +9,7 @@ SoA of OpenCLDuViGeometricMultigridSolver (OpenCLDuViGeometricMultigridSolver.cs
 from __future__ import annotations
 
 import ctypes as C
+import weakref
 
 import numpy as np
 
@@ -23,6 +24,11 @@ class CudaContext:
         N.check(N.lib().dv_context_create(device, C.byref(h)))
         self.h = h
         self.device = device
+        self._dependents = weakref.WeakSet()
+
+    def register(self, obj):
+        """Track an object holding native resources of this context (released first on close)."""
+        self._dependents.add(obj)
 
     @property
     def stream(self):
@@ -36,6 +42,11 @@ class CudaContext:
 
     def close(self):
         if getattr(self, "h", None):
+            for d in list(getattr(self, "_dependents", ())):
+                try:
+                    d.release()
+                except Exception:
+                    pass
             N.lib().dv_context_destroy(self.h)
             self.h = None
 
@@ -72,6 +83,7 @@ class SparseMatrix:
         del keep
         self.ctx = ctx
         self.h = h
+        ctx.register(self)
         self.shape = (int(shape[0]), int(shape[1]))
         self.format = fmt
         self.precision = precision
@@ -92,6 +104,7 @@ class SparseMatrix:
                                                   N.ptr(di), len(di), N.ptr(vi), bits, N.ptr(vals), len(vals),
                                                   {"f64": N.F64, "f32": N.F32}[precision], C.byref(h)))
         self.ctx, self.h, self.shape, self.format, self.precision = ctx, h, (n_rows, n_cols), "duvi", precision
+        ctx.register(self)
         return self
 
     def info(self):

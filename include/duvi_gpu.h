@@ -211,6 +211,8 @@ DV_API int dv_mgpcg_create(dv_context *ctx, int32_t n_levels, const dv_csr_host 
 DV_API int dv_mgpcg_solve(dv_mgpcg *s, const double *b, double *x, dv_stats *stats);
 /* Device-resident right-hand side and solution (FP64), context stream. */
 DV_API int dv_mgpcg_solve_device(dv_mgpcg *s, const double *d_b, double *d_x, dv_stats *stats);
+/* Effective Jacobi weight omega_eff applied to D^-1 on V-cycle level l. */
+DV_API int dv_mgpcg_omega(const dv_mgpcg *s, int32_t level, double *omega_eff);
 DV_API int dv_mgpcg_destroy(dv_mgpcg *s);
 
 /* ---- structured hex workload generator (FemCantilever3D on unit cubes) ----

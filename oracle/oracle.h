@@ -137,6 +137,8 @@ or_csr *or_galerkin(const or_csr *a, const or_csr *p);
 int32_t or_mg_fcg(int32_t n_levels, or_csr *const *A, or_csr *const *P, double omega_eff,
                   int32_t nu, const double *b, double *x, int32_t max_iter, double tol,
                   double *relres);
+/* Wall time of the iteration phase (after the coarse factorisation) of the last or_mg_fcg. */
+double or_last_solve_seconds(void);
 /* Adjoint gradient dJ/drho_e = -3 rho_e^2 lambda_e^T Ke u_e over free dofs
  * (E_e = rho_e^3), given u and lambda on free dofs. */
 void or_adjoint_element_gradient(const int32_t *ne, double E, double nu, const double *rho,
@@ -145,6 +147,9 @@ void or_adjoint_element_gradient(const int32_t *ne, double E, double nu, const d
 void or_rho_to_modulus(int64_t n, const double *rho, double *E);
 
 /* ---- parallel baseline (restatement, parallelised with OpenMP) ----------- */
+/* Threads for the row loops (SpMV, structured assembly, element-wise vector
+ * updates); default 1.  Row sums keep their order, so results do not change. */
+void or_set_threads(int n);
 void or_csr_spmv_omp(const or_csr *a, const double *x, double *y);
 int or_omp_threads(void);
 

@@ -66,6 +66,7 @@ struct DoubleIndexMap {
 };
 
 int32_t dotnet_double_hash(double x);
+extern int g_or_threads;
 
 // Element stiffness (FemCantilever3D.cs:225-313, FemCantilever2D.cs:29-49),
 // row-major, (nodes*dofs)^2 entries.

@@ -29,9 +29,15 @@ extern "C" void or_csr_copy(const or_csr *a, int32_t *rowptr, int32_t *col, doub
     if (col) std::memcpy(col, a->col.data(), sizeof(int32_t) * a->col.size());
     if (val) std::memcpy(val, a->val.data(), sizeof(double) * a->val.size());
 }
+// Threads used by the row loops of the oracle (1 = the faithful single-threaded
+// reference; more threads only split the row range, each row still sums in order).
+int g_or_threads = 1;
+extern "C" void or_set_threads(int n) { g_or_threads = n < 1 ? 1 : n; }
+
 // CsrMatrix.Multiply (external MSolve; managed provider, GeometricMultigridSolver.cs:355,367):
 // each row summed from 0.0 in stored order.
 extern "C" void or_csr_spmv(const or_csr *a, const double *x, double *y) {
+#pragma omp parallel for schedule(static) num_threads(g_or_threads) if (g_or_threads > 1)
     for (int32_t i = 0; i < a->n_rows; ++i) {
         double s = 0.0;
         for (int32_t k = a->rowptr[i]; k < a->rowptr[i + 1]; ++k) s += a->val[k] * x[a->col[k]];
@@ -419,6 +425,7 @@ extern "C" or_csr *or_hex_stiffness(const int32_t *ne, const double *elem_E, dou
     for (int32_t r = 0; r < nf; ++r) A->rowptr[r + 1] += A->rowptr[r];
     A->col.resize(A->rowptr[nf]);
     A->val.resize(A->rowptr[nf]);
+#pragma omp parallel for collapse(2) schedule(static) num_threads(g_or_threads) if (g_or_threads > 1)
     for (int32_t k = 0; k < nz; ++k)
         for (int32_t j = 0; j < ny; ++j)
             for (int32_t i = 1; i < nx; ++i) {

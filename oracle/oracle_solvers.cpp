@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <chrono>
 #include <memory>
 
 #ifdef _OPENMP
@@ -303,6 +304,9 @@ extern "C" int32_t or_pcg_jacobi(const or_csr *A, const double *b, double *x, in
 // ---------------------------------------------------------------------------
 // Build-defined FP64 checkers
 // ---------------------------------------------------------------------------
+static double g_last_iter_seconds = 0.0;
+extern "C" double or_last_solve_seconds(void) { return g_last_iter_seconds; }
+
 struct McLevel {
     const or_csr *A, *P;
     std::vector<double> w;   // omega_eff / a_ii
@@ -315,12 +319,15 @@ static void vcycle(std::vector<McLevel> &lv, const std::vector<double> &cf, int3
     int32_t n = A->n_rows;
     const std::vector<double> &w = lv[l].w;
     std::vector<double> t(n);
+#pragma omp parallel for num_threads(g_or_threads) if (g_or_threads > 1)
     for (int32_t i = 0; i < n; ++i) x[i] = w[i] * b[i];
     for (int s = 1; s < nu; ++s) {
         or_csr_spmv(A, x, t.data());
+#pragma omp parallel for num_threads(g_or_threads) if (g_or_threads > 1)
         for (int32_t i = 0; i < n; ++i) x[i] = x[i] + w[i] * (b[i] - t[i]);
     }
     or_csr_spmv(A, x, t.data());
+#pragma omp parallel for num_threads(g_or_threads) if (g_or_threads > 1)
     for (int32_t i = 0; i < n; ++i) t[i] = b[i] - t[i];
     const or_csr *P = lv[l].P;
     int32_t m = P->n_cols;
@@ -329,9 +336,11 @@ static void vcycle(std::vector<McLevel> &lv, const std::vector<double> &cf, int3
         for (int32_t k = P->rowptr[i]; k < P->rowptr[i + 1]; ++k) bc[P->col[k]] += P->val[k] * t[i];
     vcycle(lv, cf, nc, l + 1, nu, bc.data(), xc.data());
     or_csr_spmv(P, xc.data(), t.data());
+#pragma omp parallel for num_threads(g_or_threads) if (g_or_threads > 1)
     for (int32_t i = 0; i < n; ++i) x[i] = x[i] + t[i];
     for (int s = 0; s < nu; ++s) {
         or_csr_spmv(A, x, t.data());
+#pragma omp parallel for num_threads(g_or_threads) if (g_or_threads > 1)
         for (int32_t i = 0; i < n; ++i) x[i] = x[i] + w[i] * (b[i] - t[i]);
     }
 }
@@ -362,6 +371,11 @@ extern "C" int32_t or_mg_fcg(int32_t L, or_csr *const *A, or_csr *const *P, doub
         for (int32_t k = A[L - 1]->rowptr[r]; k < A[L - 1]->rowptr[r + 1]; ++k) cf[(size_t)r * nc + A[L - 1]->col[k]] = A[L - 1]->val[k];
     if (or_ldl_factor(nc, cf.data(), 1e-300) != 0) return -2;
     int32_t n = A[0]->n_rows;
+    auto t_start = std::chrono::steady_clock::now();
+    struct Stamp {   // records the time of the iteration phase on every return path
+        std::chrono::steady_clock::time_point t0;
+        ~Stamp() { g_last_iter_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); }
+    } stamp{t_start};
     std::vector<double> xv(n, 0.0), r(b, b + n), z(n), p(n, 0.0), q(n, 0.0), w(n);
     double nb = norm2(r);
     double pq = 1.0;

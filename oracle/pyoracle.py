@@ -89,6 +89,8 @@ def lib():
                                       C.c_int32, C.c_double, C.POINTER(C.c_double)]),
             "or_adjoint_element_gradient": (None, [_i32p, C.c_double, C.c_double, _f64p, _f64p, _f64p, _f64p]),
             "or_omp_threads": (C.c_int, []),
+            "or_set_threads": (None, [C.c_int]),
+            "or_last_solve_seconds": (C.c_double, []),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)

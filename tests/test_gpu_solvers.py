@@ -177,3 +177,23 @@ def test_mgpcg_device_api_and_repeat(ctx, native):
     assert its[0] == its[1] == its[2]
     x = dx.cpu().numpy()
     assert np.linalg.norm(b - A[0] @ x) / np.linalg.norm(b) <= 1e-8
+
+
+def test_mgpcg_deterministic_across_solver_lifetimes(ctx, native):
+    # Buffers of new solvers reuse memory of destroyed ones; every solve must see
+    # fully initialised data (no zero-fill racing the uploads).
+    ne = (16, 16, 16)
+    A, P = native.hex_hierarchy(ne, coarse_ne=4)
+    b = native.traction_rhs(ne)
+    seen = {}
+    for rep in range(3):
+        for nu in (1, 2, 3, 4):
+            for fmt, prec in (("duvi", "mixed"), ("csr", "f64")):
+                s = native.MultigridPcgSolver(ctx, A, P, precision=prec, fmt=fmt, nu=nu, tol=1e-8, max_iterations=100)
+                x, st = s.Solve(b)
+                assert st.HasConverged
+                key = (nu, fmt, prec)
+                seen.setdefault(key, st.NumIterationsRequired)
+                assert seen[key] == st.NumIterationsRequired, key
+                s.release()
+    assert seen[(4, "csr", "f64")] <= 12 and seen[(3, "duvi", "mixed")] <= 13
