@@ -183,6 +183,22 @@ DV_API int dv_pcg_create(dv_context *ctx, const dv_csr_host *A, int32_t format, 
 DV_API int dv_pcg_solve(dv_pcg *p, const double *b, const double *x0, double *x, dv_stats *stats);
 DV_API int dv_pcg_destroy(dv_pcg *p);
 
+/* Jacobi PCG that allocates nothing.  No counterpart in the reference: it is for
+ * callers that cannot allocate device memory when they solve -- code recording
+ * its own work into a CUDA graph (cudaMalloc/cudaFree are not allowed during
+ * stream capture, and cudaFree synchronises the device) and hosts that reserve
+ * all device memory up front.  Same algorithm and stop test as dv_pcg_solve; the
+ * work vectors live in one fixed device array of this library (4,325,632 bytes
+ * per device, held until the process exits), which limits A to 131,072 rows
+ * (larger: DV_ERR_ARG).  A must be an FP64 square matrix created beforehand;
+ * d_b and d_x are device pointers (x: initial guess if use_x0, else zeroed; the
+ * solution on return).  All calls on a device share the array: calls that
+ * overlap on the GPU race and must be serialised by the caller.  The first call
+ * on a device looks up the array's device address; make it before any stream
+ * capture. */
+DV_API int dv_pcg_solve_noalloc(dv_matrix *A, const double *d_b, double *d_x, int32_t use_x0,
+                                int32_t max_iterations, double tol, dv_stats *stats);
+
 /* ---- multigrid-preconditioned flexible PCG (FP64 or mixed precision) ------
  * Build-defined extension of the reference pieces: an FP64 flexible CG
  * (FCG(1)) outer loop with true-residual refinement restarts, preconditioned
