@@ -146,6 +146,99 @@ void dv_make_bundles(const DuviHost &h, int32_t n_rows, int vi_bits, std::vector
     bundles.push_back(n_rows);
 }
 
+// Group size: g consecutive rows with identical block structure (same block
+// count, same block columns, same gap bytes), e.g. the dofs of one node.
+static int detect_group(const DuviHost &h, int32_t n) {
+    for (int g : {3, 2}) {
+        if (n % g != 0 || n == 0) continue;
+        int ok = 1;
+#pragma omp parallel for schedule(static) reduction(min : ok)
+        for (int32_t gi = 0; gi < n / g; ++gi) {
+            const int32_t r0 = gi * g;
+            const uint32_t nb = h.row_to_col[r0 + 1] - h.row_to_col[r0], ne = h.row_to_dist[r0 + 1] - h.row_to_dist[r0];
+            for (int d = 1; d < g && ok; ++d) {
+                const int32_t r = r0 + d;
+                if (h.row_to_col[r + 1] - h.row_to_col[r] != nb || h.row_to_dist[r + 1] - h.row_to_dist[r] != ne) { ok = 0; break; }
+                if (std::memcmp(&h.col_idx[h.row_to_col[r]], &h.col_idx[h.row_to_col[r0]], 4 * (size_t)nb) != 0 ||
+                    std::memcmp(&h.dist[h.row_to_dist[r]], &h.dist[h.row_to_dist[r0]], ne) != 0) ok = 0;
+            }
+        }
+        if (ok) return g;
+    }
+    return 1;
+}
+
+void dv_build_duvi_lanes(const DuviHost &h, int32_t n, DuviLanesHost &L) {
+    const int g = detect_group(h, n);
+    const int vib = h.vi_bits / 8;            // bytes per value index
+    const size_t chunk = 4 * (size_t)vib;     // bytes per chunk of 4 indices
+    L.group = g;
+    L.ngroups = n / g;
+    L.nbundles = (L.ngroups + 31) / 32;
+    L.meta.assign(5 * L.nbundles, 0);
+    L.nent.assign(L.ngroups, 0);
+    // sizes per bundle
+    std::vector<uint64_t> dwords(L.nbundles + 1, 0), vchunks(L.nbundles + 1, 0), cwords(L.nbundles + 1, 0);
+#pragma omp parallel for schedule(static)
+    for (int64_t bi = 0; bi < L.nbundles; ++bi) {
+        uint32_t le = 0, lb = 0;
+        for (int t = 0; t < 32; ++t) {
+            int64_t gi = bi * 32 + t;
+            if (gi >= L.ngroups) break;
+            int32_t r0 = (int32_t)(gi * g);
+            uint32_t ne = h.row_to_dist[r0 + 1] - h.row_to_dist[r0], nb = h.row_to_col[r0 + 1] - h.row_to_col[r0];
+            L.nent[gi] = ne;
+            le = std::max(le, ne);
+            lb = std::max(lb, nb);
+        }
+        const uint32_t words = (le + 3) / 4;
+        dwords[bi + 1] = (uint64_t)words * 32;
+        vchunks[bi + 1] = (uint64_t)words * g * 32;
+        cwords[bi + 1] = (uint64_t)lb * 32;
+        L.meta[5 * bi + 3] = words;
+        L.meta[5 * bi + 4] = lb;
+    }
+    for (int64_t bi = 0; bi < L.nbundles; ++bi) {
+        dwords[bi + 1] += dwords[bi];
+        vchunks[bi + 1] += vchunks[bi];
+        cwords[bi + 1] += cwords[bi];
+    }
+    DV_REQUIRE(dwords[L.nbundles] < 0xFFFFFFFFull && vchunks[L.nbundles] < 0xFFFFFFFFull && cwords[L.nbundles] < 0xFFFFFFFFull,
+               DV_ERR_FORMAT, "lane layout exceeds 32-bit offsets");
+    L.dist.assign(dwords[L.nbundles], 0);
+    L.vi.assign(vchunks[L.nbundles] * chunk, 0);
+    L.cols.assign(cwords[L.nbundles], 0);
+#pragma omp parallel for schedule(static)
+    for (int64_t bi = 0; bi < L.nbundles; ++bi) {
+        L.meta[5 * bi + 0] = (uint32_t)dwords[bi];
+        L.meta[5 * bi + 1] = (uint32_t)vchunks[bi];
+        L.meta[5 * bi + 2] = (uint32_t)cwords[bi];
+        const uint32_t words = L.meta[5 * bi + 3];
+        for (int t = 0; t < 32; ++t) {
+            int64_t gi = bi * 32 + t;
+            if (gi >= L.ngroups) break;
+            const int32_t r0 = (int32_t)(gi * g);
+            const uint32_t d0 = h.row_to_dist[r0], ne = h.row_to_dist[r0 + 1] - d0;
+            for (uint32_t e = 0; e < ne; ++e) {
+                uint32_t w = e / 4, k = e % 4;
+                L.dist[dwords[bi] + (uint64_t)w * 32 + t] |= (uint32_t)h.dist[d0 + e] << (8 * k);
+            }
+            for (int d = 0; d < g; ++d) {
+                const uint32_t rd = h.row_to_dist[r0 + d];
+                for (uint32_t e = 0; e < ne; ++e) {
+                    uint32_t w = e / 4, k = e % 4;
+                    uint64_t c = vchunks[bi] + ((uint64_t)w * g + d) * 32 + t;
+                    uint32_t v = h.vidx[rd + e];
+                    std::memcpy(&L.vi[c * chunk + k * vib], &v, vib);   // little-endian low bytes
+                }
+            }
+            const uint32_t c0 = h.row_to_col[r0], nb = h.row_to_col[r0 + 1] - c0;
+            for (uint32_t b = 0; b < nb; ++b) L.cols[cwords[bi] + (uint64_t)b * 32 + t] = h.col_idx[c0 + b];
+            (void)words;
+        }
+    }
+}
+
 void dv_extract_diag(const dv_csr_host &a, std::vector<double> &d) {
     d.assign(a.n_rows, 0.0);
 #pragma omp parallel for schedule(static)

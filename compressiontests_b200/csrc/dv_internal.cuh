@@ -121,6 +121,25 @@ struct DuviHost {   // host copy of the SoA encoding (export / parity)
     int vi_bits = 8;
 };
 
+// Lane-interleaved derived layout of a DuVi matrix for the "lanes" kernel.
+// Rows are grouped `group` at a time when consecutive rows share their column
+// structure (the dofs of one mesh node); one lane owns one group, 32 groups
+// form a bundle, and each bundle stores its streams word-interleaved by lane so
+// that every warp load is one coalesced 128-byte transaction:
+//   dist word w of lane t     at dist[d_base + w*32 + t]      (leader row, 4 entries per word)
+//   value-index chunk (w, d)  at vi[v_base + (w*group + d)*32 + t]  (row d of the group, 4 entries)
+//   block start b of lane t   at cols[c_base + b*32 + t]      (leader row)
+// The canonical SoA stays on the device (export, Gauss-Seidel, SpMM).
+struct DuviLanesHost {
+    int group = 1;
+    int64_t ngroups = 0, nbundles = 0;
+    std::vector<uint32_t> meta;    // per bundle: d_base, v_base, c_base, words, blocks
+    std::vector<uint32_t> dist;    // leader gap/count bytes, 4 per word
+    std::vector<uint8_t> vi;       // chunks of 4 value indices (4 * vi_bits / 8 bytes each)
+    std::vector<uint32_t> cols;    // leader block column starts
+    std::vector<uint32_t> nent;    // entries per leader row
+};
+
 struct dv_matrix {
     dv_context *ctx = nullptr;
     int32_t n_rows = 0, n_cols = 0;
@@ -137,6 +156,11 @@ struct dv_matrix {
     DevMem bundles;            // int32 row starts of row bundles (+ sentinel)
     int32_t nbundles = 0;
     int duvi_batch = 4;        // entries per gather batch in the decode loop (9 when most blocks hold 9)
+    int duvi_variant = 0;      // 0: shared-memory staged rows, 1: lane-interleaved groups (autotuned)
+    int lanes_group = 1;
+    int64_t lanes_bundles = 0, lanes_groups = 0;
+    DevMem lanes_meta, lanes_dist, lanes_vi, lanes_cols, lanes_nent;
+    int64_t lanes_bytes = 0;   // bytes one product reads from the lane layout
     DuviHost host;             // kept for export
     // shared
     DevMem diag;               // FP64 diagonal (0 where absent)
@@ -153,6 +177,7 @@ constexpr int kBundleBlocks = 480;    // block column starts (+ alignment slack)
 // Host helpers (dv_host.cpp)
 void dv_encode_duvi(const dv_csr_host &a, double tol, int force_bits, DuviHost &out);
 void dv_make_bundles(const DuviHost &h, int32_t n_rows, int vi_bits, std::vector<int32_t> &bundles);
+void dv_build_duvi_lanes(const DuviHost &h, int32_t n_rows, DuviLanesHost &out);
 void dv_extract_diag(const dv_csr_host &a, std::vector<double> &diag);
 // Row-ratio bound max_i sum_j |a_ij| / max_j |a_ij| (GeometricMultigridSolver.cs:144-151).
 double dv_row_ratio_bound(const dv_csr_host &a);

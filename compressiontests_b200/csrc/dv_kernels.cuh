@@ -462,6 +462,144 @@ struct LaunchEnv {
     int max_blocks;
 };
 
+// ---------------------------------------------------------------------------
+// DuVi lane kernel (lane-interleaved derived layout, see DuviLanesHost)
+//
+// One warp per bundle of 32 row groups, one lane per group.  The loop over the
+// bundle's 4-entry words is warp-uniform; each lane decodes its leader row's
+// columns once (count byte at a block start, gap bytes inside a block) and
+// applies every gathered x value to the G rows of its group, which share the
+// column structure.  No shared-memory staging: every stream load is a
+// coalesced 128-byte warp transaction.  Each row still sums its entries in
+// order, so FP64 results equal the reference walk bit for bit.
+// ---------------------------------------------------------------------------
+template <class VI> struct ViChunk;
+template <> struct ViChunk<uint8_t> { using T = uint32_t; };
+template <> struct ViChunk<uint16_t> { using T = uint2; };
+template <> struct ViChunk<uint32_t> { using T = uint4; };
+
+__device__ __forceinline__ uint32_t vi_get(uint32_t c, int k) { return (c >> (8 * k)) & 0xFFu; }
+__device__ __forceinline__ uint32_t vi_get(uint2 c, int k) { return ((k < 2 ? c.x : c.y) >> (16 * (k & 1))) & 0xFFFFu; }
+__device__ __forceinline__ uint32_t vi_get(uint4 c, int k) { return k == 0 ? c.x : k == 1 ? c.y : k == 2 ? c.z : c.w; }
+
+struct DuviLanesArgs {
+    const uint32_t *__restrict__ meta;
+    const uint32_t *__restrict__ dist;
+    const void *__restrict__ vi;
+    const uint32_t *__restrict__ cols;
+    const uint32_t *__restrict__ nent;
+    const void *__restrict__ values;
+    int64_t ngroups;
+    int32_t nbundles;
+    int32_t nuniq;
+};
+
+template <class VI, class AT, class Gather, class Op, int G>
+__global__ void __launch_bounds__(256) k_duvi_lanes(DuviLanesArgs A, Gather g, Op op, const int *__restrict__ done,
+                                                    double *partials, unsigned *ticket) {
+    if (done && *(volatile const int *)done) return;
+    using Chunk = typename ViChunk<VI>::T;
+    constexpr bool kSmemTable = sizeof(VI) == 1;
+    __shared__ AT tab[kSmemTable ? 256 : 1];
+    const AT *gtab = static_cast<const AT *>(A.values);
+    if (kSmemTable) {
+        for (int i = threadIdx.x; i < A.nuniq; i += blockDim.x) tab[i] = gtab[i];
+        __syncthreads();
+    }
+    double red[Op::NRED > 0 ? Op::NRED : 1];
+#pragma unroll
+    for (int i = 0; i < (Op::NRED > 0 ? Op::NRED : 1); ++i) red[i] = 0.0;
+    const int lane = threadIdx.x & 31;
+    const int wpb = blockDim.x >> 5;
+    const Chunk *vbase = static_cast<const Chunk *>(A.vi);
+    for (int32_t bi = blockIdx.x * wpb + (threadIdx.x >> 5); bi < A.nbundles; bi += gridDim.x * wpb) {
+        const uint32_t d_base = __ldg(A.meta + 5 * bi), v_base = __ldg(A.meta + 5 * bi + 1);
+        const uint32_t c_base = __ldg(A.meta + 5 * bi + 2), words = __ldg(A.meta + 5 * bi + 3);
+        const int64_t grp = (int64_t)bi * 32 + lane;
+        const bool valid = grp < A.ngroups;
+        const uint32_t ne = valid ? __ldg(A.nent + grp) : 0u;
+        const int32_t r0 = (int32_t)(grp * G);
+        AT s[G];
+#pragma unroll
+        for (int d = 0; d < G; ++d) s[d] = valid ? op.init(r0 + d) : AT(0);
+        const uint32_t *dp = A.dist + d_base + lane;
+        const Chunk *vp = vbase + v_base + lane;
+        const uint32_t *cp = A.cols + c_base + lane;
+        uint32_t c = 0, rem = 0, b = 0;
+        for (uint32_t w = 0; w < words; ++w) {
+            const uint32_t dw = __ldg(dp + (size_t)w * 32);
+            Chunk vw[G];
+#pragma unroll
+            for (int d = 0; d < G; ++d) vw[d] = __ldg(vp + ((size_t)w * G + d) * 32);
+            uint32_t cols[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const uint32_t byte = (dw >> (8 * k)) & 0xFFu;
+                if (w * 4 + k < ne) {
+                    if (rem == 0) {
+                        c = __ldg(cp + (size_t)b * 32);
+                        ++b;
+                        rem = byte + 1u;
+                    } else {
+                        c += byte + 1u;
+                    }
+                    --rem;
+                }
+                cols[k] = c;
+            }
+            AT xv[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) xv[k] = (w * 4 + k < ne) ? g(cols[k]) : AT(0);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                if (w * 4 + k < ne) {
+#pragma unroll
+                    for (int d = 0; d < G; ++d) {
+                        const uint32_t idx = vi_get(vw[d], k);
+                        const AT v = kSmemTable ? tab[idx] : __ldg(gtab + idx);
+                        s[d] = madd<AT>(s[d], v, xv[k]);
+                    }
+                }
+            }
+        }
+        if (valid) {
+#pragma unroll
+            for (int d = 0; d < G; ++d) op.row(r0 + d, s[d], red);
+        }
+    }
+    if constexpr (Op::NRED > 0) {
+        double tot[Op::NRED];
+        if (grid_reduce<Op::NRED, Op::MAXMASK>(red, partials, ticket, tot)) op.finish(tot);
+    }
+}
+
+template <class VI, class AT, class Gather, class Op, int G>
+void launch_duvi_lanes_g(const LaunchEnv &e, const dv_matrix *m, Gather g, Op op) {
+    DuviLanesArgs a;
+    a.meta = m->lanes_meta.as<uint32_t>();
+    a.dist = m->lanes_dist.as<uint32_t>();
+    a.vi = m->lanes_vi.p;
+    a.cols = m->lanes_cols.as<uint32_t>();
+    a.nent = m->lanes_nent.as<uint32_t>();
+    a.values = m->values.p;
+    a.ngroups = m->lanes_groups;
+    a.nbundles = (int32_t)m->lanes_bundles;
+    a.nuniq = (int32_t)m->nuniq;
+    int blocks = (int)((m->lanes_bundles + 7) / 8);
+    if (blocks > e.max_blocks) blocks = e.max_blocks;
+    if (blocks < 1) blocks = 1;
+    k_duvi_lanes<VI, AT, Gather, Op, G><<<blocks, 256, 0, e.stream>>>(a, g, op, e.done, e.partials, e.ticket);
+    DV_CUDA(cudaGetLastError());
+    e.ctx->count();
+}
+
+template <class VI, class AT, class Gather, class Op>
+void launch_duvi_lanes(const LaunchEnv &e, const dv_matrix *m, Gather g, Op op) {
+    if (m->lanes_group == 3) launch_duvi_lanes_g<VI, AT, Gather, Op, 3>(e, m, g, op);
+    else launch_duvi_lanes_g<VI, AT, Gather, Op, 1>(e, m, g, op);
+}
+
+
 template <class VI, class AT, class Gather, class Op, int BATCH>
 void launch_duvi_vi(const LaunchEnv &e, const dv_matrix *m, Gather g, Op op) {
     constexpr int W = sizeof(VI) == 4 ? kDuviWarps32 : kDuviWarps;
@@ -506,6 +644,12 @@ void launch_csr_tpr(const LaunchEnv &e, const dv_matrix *m, Gather g, Op op) {
 // Runs op over every row of m with the accumulator type AT (= value precision).
 template <class AT, class Gather, class Op>
 void launch_rows(const LaunchEnv &e, const dv_matrix *m, Gather g, Op op) {
+    if (m->format == DV_FORMAT_DUVI && m->duvi_variant == 1) {
+        if (m->vi_bits == 8) launch_duvi_lanes<uint8_t, AT>(e, m, g, op);
+        else if (m->vi_bits == 16) launch_duvi_lanes<uint16_t, AT>(e, m, g, op);
+        else launch_duvi_lanes<uint32_t, AT>(e, m, g, op);
+        return;
+    }
     if (m->format == DV_FORMAT_DUVI) {
         // batch width matched to the dominant block length (chosen at upload)
         if (m->duvi_batch == 9) {

@@ -151,6 +151,24 @@ static void finish_duvi_upload(dv_matrix *m, cudaStream_t s) {
         int mode = (int)(std::max_element(hist.begin(), hist.end()) - hist.begin());
         m->duvi_batch = (mode >= 9 && mode % 9 == 0) ? 9 : 4;
     }
+    {   // lane-interleaved derived layout
+        DuviLanesHost L;
+        dv_build_duvi_lanes(h, m->n_rows, L);
+        m->lanes_group = L.group;
+        m->lanes_groups = L.ngroups;
+        m->lanes_bundles = L.nbundles;
+        upload(m->lanes_meta, L.meta.data(), 4 * L.meta.size(), s);
+        upload(m->lanes_dist, L.dist.data(), 4 * L.dist.size(), s);
+        upload(m->lanes_vi, L.vi.data(), L.vi.size(), s);
+        upload(m->lanes_cols, L.cols.data(), 4 * L.cols.size(), s);
+        upload(m->lanes_nent, L.nent.data(), 4 * L.nent.size(), s);
+        DV_CUDA(cudaStreamSynchronize(s));
+        const size_t vs = m->precision == DV_F64 ? 8 : 4;
+        m->lanes_bytes = (int64_t)(4 * L.meta.size() + 4 * L.dist.size() + L.vi.size() + 4 * L.cols.size() +
+                                   4 * L.nent.size() + vs * h.values.size());
+        // the lane kernel is the default when rows come in node groups
+        m->duvi_variant = L.group > 1 ? 1 : 0;
+    }
     std::vector<int32_t> b;
     dv_make_bundles(h, m->n_rows, m->vi_bits, b);
     m->nbundles = (int32_t)b.size() - 1;
@@ -197,15 +215,21 @@ static void autotune(dv_matrix *m) {
             dvk::launch_rows<float>(e, m, dvk::GatherVec<float, float>{x.as<float>()}, op);
         }
     };
-    std::vector<int> cand = m->format == DV_FORMAT_CSR ? std::vector<int>{8, 16, 32} : std::vector<int>{4, 9};
+    // CSR: threads per row; DuVi: 4 / 9 = staged kernel with that batch width, 100 = lane kernel
+    std::vector<int> cand = m->format == DV_FORMAT_CSR ? std::vector<int>{8, 16, 32} : std::vector<int>{4, 9, 100};
     cudaEvent_t e0, e1;
     DV_CUDA(cudaEventCreate(&e0));
     DV_CUDA(cudaEventCreate(&e1));
     float best = 1e30f;
-    int best_v = m->format == DV_FORMAT_CSR ? m->csr_tpr : m->duvi_batch;
-    for (int v : cand) {
+    auto current = [&] { return m->format == DV_FORMAT_CSR ? m->csr_tpr : (m->duvi_variant == 1 ? 100 : m->duvi_batch); };
+    auto apply = [&](int v) {
         if (m->format == DV_FORMAT_CSR) m->csr_tpr = v;
-        else m->duvi_batch = v;
+        else if (v == 100) m->duvi_variant = 1;
+        else { m->duvi_variant = 0; m->duvi_batch = v; }
+    };
+    int best_v = current();
+    for (int v : cand) {
+        apply(v);
         run();
         DV_CUDA(cudaEventRecord(e0, s));
         for (int k = 0; k < 3; ++k) run();
@@ -213,12 +237,15 @@ static void autotune(dv_matrix *m) {
         DV_CUDA(cudaEventSynchronize(e1));
         float ms = 0;
         cudaEventElapsedTime(&ms, e0, e1);
+        const char *vb = getenv("DV_AUTOTUNE_VERBOSE");
+        if (vb && vb[0] == '1')
+            fprintf(stderr, "autotune %s n=%d variant=%d: %.4f ms\n", m->format == DV_FORMAT_CSR ? "csr" : "duvi",
+                    m->n_rows, v, ms / 3);
         if (ms < best) { best = ms; best_v = v; }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    if (m->format == DV_FORMAT_CSR) m->csr_tpr = best_v;
-    else m->duvi_batch = best_v;
+    apply(best_v);
     ctx->launches -= (int64_t)cand.size() * 4;   // tuning launches are not part of any solve
 }
 
@@ -343,7 +370,8 @@ extern "C" DV_API int dv_matrix_get_info(const dv_matrix *m, dv_matrix_info *inf
         info->format = m->format;
         info->precision = m->precision;
         info->value_index_bits = m->format == DV_FORMAT_DUVI ? m->vi_bits : 0;
-        info->kernel_variant = m->format == DV_FORMAT_CSR ? m->csr_tpr : m->nbundles;
+        info->kernel_variant = m->format == DV_FORMAT_CSR ? m->csr_tpr
+                               : (m->duvi_variant == 1 ? 100 + m->lanes_group : m->duvi_batch);
         info->device_bytes = m->device_bytes;
     });
 }
