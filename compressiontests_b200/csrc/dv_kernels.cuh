@@ -526,18 +526,31 @@ __global__ void __launch_bounds__(256) k_duvi_lanes(DuviLanesArgs A, Gather g, O
         const Chunk *vp = vbase + v_base + lane;
         const uint32_t *cp = A.cols + c_base + lane;
         uint32_t c = 0, rem = 0, b = 0;
+        // register double buffer: the streams of word w+1 are in flight while word w is decoded
+        uint32_t dw_next = 0;
+        Chunk vw_next[G];
+        if (words > 0) {
+            dw_next = __ldcs(dp);
+#pragma unroll
+            for (int d = 0; d < G; ++d) vw_next[d] = __ldcs(vp + (size_t)d * 32);
+        }
         for (uint32_t w = 0; w < words; ++w) {
-            const uint32_t dw = __ldg(dp + (size_t)w * 32);
+            const uint32_t dw = dw_next;
             Chunk vw[G];
 #pragma unroll
-            for (int d = 0; d < G; ++d) vw[d] = __ldg(vp + ((size_t)w * G + d) * 32);
+            for (int d = 0; d < G; ++d) vw[d] = vw_next[d];
+            if (w + 1 < words) {
+                dw_next = __ldcs(dp + (size_t)(w + 1) * 32);
+#pragma unroll
+                for (int d = 0; d < G; ++d) vw_next[d] = __ldcs(vp + ((size_t)(w + 1) * G + d) * 32);
+            }
             uint32_t cols[4];
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
                 const uint32_t byte = (dw >> (8 * k)) & 0xFFu;
                 if (w * 4 + k < ne) {
                     if (rem == 0) {
-                        c = __ldg(cp + (size_t)b * 32);
+                        c = __ldcs(cp + (size_t)b * 32);
                         ++b;
                         rem = byte + 1u;
                     } else {
