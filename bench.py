@@ -53,6 +53,11 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-fp64", action="store_true")
     p.add_argument("--no-spmv", action="store_true")
+    p.add_argument("--no-batched", action="store_true", help="skip the multi-load-case section")
+    p.add_argument("--batched-only", action="store_true",
+                   help="only the multi-load-case MG-PCG (64 load cases on the 64^3 mesh)")
+    p.add_argument("--batch-size", type=int, default=64, help="mesh edge of the multi-load-case section")
+    p.add_argument("--batch-k", type=int, default=64, help="load cases of the multi-load-case section")
     p.add_argument("--spmv-only", default=None, metavar="FMT_PREC",
                    help="only time the SpMV of the finest operator (duvi_f32, duvi_f64, csr_f32, csr_f64): "
                         "the small case used for ncu captures")
@@ -363,6 +368,10 @@ def run_ours(args):
                 "frac": round(achieved / peak, 3), "traffic": ncu_traffic(), "peak_kind": peak_kind,
                 "algorithmic_bytes_per_launch": int(alg), "avg_launch_ms": round(ms_dom, 4)}
 
+    batched = None
+    if not args.no_batched:
+        batched = batched_multi_rhs(cb, ctx, stream, args.batch_size, args.batch_k, max(1, args.steps // 2), args.tol)
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         try:
@@ -387,7 +396,8 @@ def run_ours(args):
             "iterations": its_mixed[-1], "relative_residual_fp64": true_rel,
             "e2e": {"value": round(ms_e2e, 3), "unit": "ms", "h2d_bytes_per_step": int(8 * nf),
                     "d2h_bytes_per_step": int(8 * nf)},
-            "gpu_launches": int(launches), "fp64": fp64, "spmv": spmv, "roofline": roof, "cpu_baseline": cpu,
+            "gpu_launches": int(launches), "fp64": fp64, "spmv": spmv, "batched": batched, "roofline": roof,
+            "cpu_baseline": cpu,
             "clocks": clocks, "setup_s": {"hierarchy": round(t_build, 1), "solver": round(t_setup, 1)},
         }
         print(json.dumps(line), flush=True)
@@ -395,6 +405,63 @@ def run_ours(args):
     if ws > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def batched_multi_rhs(cb, ctx, stream, size, k, steps, tol):
+    """k load cases (N(0,1) nodal forces on the free face) on the size^3 mesh: one
+    multi-right-hand-side solve against k single solves of the same load cases."""
+    import torch
+    ne = (size, size, size)
+    A, P = cb.hex_hierarchy(ne, coarse_ne=8)
+    B = cb.random_face_loads(ne, k, seed=20261203)
+    s = cb.MultigridPcgSolver(ctx, A, P, precision="mixed", fmt="duvi", nu=2, omega=2 / 3, omega_mode="spectral",
+                              tol=tol, max_iterations=500)
+    dB = torch.from_numpy(np.ascontiguousarray(B)).cuda()
+    dX = torch.zeros_like(dB)
+    torch.cuda.synchronize()
+    st, conv = s.solve_many_device(k, dB.data_ptr(), dX.data_ptr())   # eager warm-up, then graph replays
+    l0 = ctx.launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        st, conv = s.solve_many_device(k, dB.data_ptr(), dX.data_ptr())
+        assert conv.all(), st
+    e1.record(stream)
+    e1.synchronize()
+    ms_multi = e0.elapsed_time(e1) / steps
+    launches = (ctx.launch_count() - l0) // steps
+    X = dX.cpu().numpy()
+    rel = float(np.max(np.linalg.norm(B - A[0] @ X, axis=0) / np.linalg.norm(B, axis=0)))
+    # the same load cases one after another (PcgSolver2.InverseSystemMatrixTimesOtherMatrix order)
+    cols = [torch.from_numpy(np.ascontiguousarray(B[:, j])).cuda() for j in range(k)]
+    dx = torch.zeros_like(cols[0])
+    torch.cuda.synchronize()
+    s.solve_device(cols[0].data_ptr(), dx.data_ptr())
+    its1 = []
+    e0.record(stream)
+    for j in range(k):
+        st1 = s.solve_device(cols[j].data_ptr(), dx.data_ptr())
+        its1.append(st1.NumIterationsRequired)
+    e1.record(stream)
+    e1.synchronize()
+    ms_seq = e0.elapsed_time(e1)
+    s.release()
+    return {"workload": f"{k} load cases, N(0,1) nodal forces on the free face, {size}^3 hex mesh, "
+                        "mixed MG-PCG (FP32 DuVi V(2,2) in FP64 FCG), tol {tol:g} per load case".format(tol=tol),
+            "n_dofs": int(A[0].shape[0]), "k": k, "ms": round(ms_multi, 3), "ms_per_load_case": round(ms_multi / k, 4),
+            "iterations": int(st.NumIterationsRequired), "worst_relative_residual_fp64": rel,
+            "sequential_ms": round(ms_seq, 3), "sequential_iterations_max": int(max(its1)),
+            "speedup_vs_sequential": round(ms_seq / ms_multi, 2), "gpu_launches_per_solve": int(launches)}
+
+
+def run_batched_only(args):
+    import torch
+    import compressiontests_b200 as cb
+    ctx = cb.CudaContext(0)
+    r = batched_multi_rhs(cb, ctx, torch.cuda.ExternalStream(ctx.stream), args.batch_size, args.batch_k,
+                          args.steps, args.tol)
+    print(json.dumps({"batched": r}), flush=True)
+    ctx.close()
 
 
 def run_spmv_only(args):
@@ -427,6 +494,8 @@ if __name__ == "__main__":
     a = parse()
     if a.spmv_only:
         run_spmv_only(a)
+    elif a.batched_only:
+        run_batched_only(a)
     elif a.impl == "reference":
         run_reference(a)
     else:

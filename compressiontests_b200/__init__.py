@@ -10,12 +10,13 @@ from ._native import DuviError, NotImplementedFeatureError, NotInitializedError,
 from .sparse import CudaContext, SparseMatrix
 from .solvers import (CudaCsrGeometricMultigridSolver, CudaCsrPcgSolver, CudaDuViGeometricMultigridSolver,
                       IterativeStatistics, MultigridPcgSolver, make_path)
-from .cantilever import FemCantilever3D, hex_hierarchy, hex_stiffness, hex_trilinear, traction_rhs, cartesian_transfer
+from .cantilever import (FemCantilever3D, cartesian_transfer, hex_hierarchy, hex_stiffness, hex_trilinear,
+                         random_face_loads, traction_rhs)
 
 __all__ = [
     "CudaContext", "SparseMatrix", "CudaCsrGeometricMultigridSolver", "CudaDuViGeometricMultigridSolver",
     "CudaCsrPcgSolver", "MultigridPcgSolver", "IterativeStatistics", "FemCantilever3D", "hex_hierarchy",
-    "hex_stiffness", "hex_trilinear", "traction_rhs", "cartesian_transfer", "make_path", "DuviError",
+    "hex_stiffness", "hex_trilinear", "traction_rhs", "random_face_loads", "cartesian_transfer", "make_path", "DuviError",
     "NotImplementedFeatureError", "NotInitializedError", "NoDeviceError",
 ]
 

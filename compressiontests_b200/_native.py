@@ -65,7 +65,8 @@ class Stats(C.Structure):
 class MatrixInfo(C.Structure):
     _fields_ = [("n_rows", C.c_int32), ("n_cols", C.c_int32), ("nnz", C.c_int64), ("nblocks", C.c_int64),
                 ("nuniq", C.c_int64), ("format", C.c_int32), ("precision", C.c_int32),
-                ("value_index_bits", C.c_int32), ("kernel_variant", C.c_int32), ("device_bytes", C.c_int64)]
+                ("value_index_bits", C.c_int32), ("kernel_variant", C.c_int32), ("device_bytes", C.c_int64),
+                ("row_group", C.c_int32), ("reserved", C.c_int32)]
 
 
 class GmgConfig(C.Structure):
@@ -115,6 +116,8 @@ _SIGNATURES = {
     "dv_mgpcg_solve": (C.c_int, [_vp, _vp, _vp, _P(Stats)]),
     "dv_mgpcg_solve_device": (C.c_int, [_vp, _vp, _vp, _P(Stats)]),
     "dv_mgpcg_omega": (C.c_int, [_vp, C.c_int32, _P(C.c_double)]),
+    "dv_mgpcg_solve_multi": (C.c_int, [_vp, C.c_int32, _vp, _vp, _vp, _P(Stats)]),
+    "dv_mgpcg_solve_multi_device": (C.c_int, [_vp, C.c_int32, _vp, _vp, _vp, _P(Stats)]),
     "dv_mgpcg_destroy": (C.c_int, [_vp]),
     "dv_hex_csr_size": (C.c_int, [_vp, _P(C.c_int32), _P(C.c_int64)]),
     "dv_hex_assemble": (C.c_int, [_vp, _vp, C.c_double, C.c_double, C.c_double, _vp, _vp, _vp]),

@@ -141,6 +141,18 @@ def traction_rhs(ne, t=(0.0, 0.0, -1.0)):
     return b.ravel()
 
 
+def random_face_loads(ne, k, seed=0):
+    """k load cases with i.i.d. N(0, 1) nodal forces (all 3 components) on the free face x = ne[0].
+
+    Returns an n_free x k array (column j = load case j), dofs ordered as traction_rhs.
+    """
+    nx, ny, nz = ne[0] + 1, ne[1] + 1, ne[2] + 1
+    rng = np.random.default_rng(seed)
+    B = np.zeros((nz, ny, nx - 1, 3, k))
+    B[:, :, -1, :, :] = rng.standard_normal((nz, ny, 3, k))
+    return B.reshape(-1, k)
+
+
 def coarsen_moduli(ne, elem_E):
     """Average of the 8 children of every coarse element (factor-2 grids)."""
     e = np.asarray(elem_E, np.float64).reshape(ne[2], ne[1], ne[0])

@@ -168,6 +168,27 @@ static int detect_group(const DuviHost &h, int32_t n) {
     return 1;
 }
 
+int dv_csr_row_group(const dv_csr_host &a) {
+    const int32_t n = a.n_rows;
+    for (int g : {3, 2}) {
+        if (n % g != 0 || n == 0) continue;
+        int ok = 1;
+#pragma omp parallel for schedule(static) reduction(min : ok)
+        for (int32_t gi = 0; gi < n / g; ++gi) {
+            const int32_t r0 = gi * g;
+            const int32_t len = a.rowptr[r0 + 1] - a.rowptr[r0];
+            for (int d = 1; d < g && ok; ++d) {
+                const int32_t r = r0 + d;
+                if (a.rowptr[r + 1] - a.rowptr[r] != len ||
+                    std::memcmp(a.col + a.rowptr[r], a.col + a.rowptr[r0], 4 * (size_t)len) != 0)
+                    ok = 0;
+            }
+        }
+        if (ok) return g;
+    }
+    return 1;
+}
+
 void dv_build_duvi_lanes(const DuviHost &h, int32_t n, DuviLanesHost &L) {
     const int g = detect_group(h, n);
     const int vib = h.vi_bits / 8;            // bytes per value index

@@ -163,6 +163,7 @@ struct dv_matrix {
     int64_t lanes_bytes = 0;   // bytes one product reads from the lane layout
     DuviHost host;             // kept for export
     // shared
+    int row_group = 1;         // g consecutive rows share one column list (node dofs); 1 otherwise
     DevMem diag;               // FP64 diagonal (0 where absent)
     std::vector<double> host_diag;
     int64_t device_bytes = 0;
@@ -179,6 +180,8 @@ void dv_encode_duvi(const dv_csr_host &a, double tol, int force_bits, DuviHost &
 void dv_make_bundles(const DuviHost &h, int32_t n_rows, int vi_bits, std::vector<int32_t> &bundles);
 void dv_build_duvi_lanes(const DuviHost &h, int32_t n_rows, DuviLanesHost &out);
 void dv_extract_diag(const dv_csr_host &a, std::vector<double> &diag);
+// 3 or 2 when every run of that many consecutive rows has one column list, else 1.
+int dv_csr_row_group(const dv_csr_host &a);
 // Row-ratio bound max_i sum_j |a_ij| / max_j |a_ij| (GeometricMultigridSolver.cs:144-151).
 double dv_row_ratio_bound(const dv_csr_host &a);
 // Dense inverse of an SPD matrix via LDL^T (no pivoting); returns false on a tiny pivot.

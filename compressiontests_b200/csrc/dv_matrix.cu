@@ -155,6 +155,7 @@ static void finish_duvi_upload(dv_matrix *m, cudaStream_t s) {
         DuviLanesHost L;
         dv_build_duvi_lanes(h, m->n_rows, L);
         m->lanes_group = L.group;
+        m->row_group = L.group;
         m->lanes_groups = L.ngroups;
         m->lanes_bundles = L.nbundles;
         upload(m->lanes_meta, L.meta.data(), 4 * L.meta.size(), s);
@@ -275,6 +276,7 @@ dv_matrix *dv_matrix_build(dv_context *ctx, const dv_csr_host &a, int format, in
             DV_CUDA(cudaStreamSynchronize(s));
         }
         m->csr_tpr = pick_tpr(a.n_rows ? (double)m->nnz / a.n_rows : 1.0);
+        m->row_group = dv_csr_row_group(a);
         m->device_bytes = m->nnz * (4 + (precision == DV_F64 ? 8 : 4)) + 4 * ((int64_t)a.n_rows + 1);
     } else {
         dv_encode_duvi(a, tol, vi_bits, m->host);
@@ -373,6 +375,8 @@ extern "C" DV_API int dv_matrix_get_info(const dv_matrix *m, dv_matrix_info *inf
         info->kernel_variant = m->format == DV_FORMAT_CSR ? m->csr_tpr
                                : (m->duvi_variant == 1 ? 100 + m->lanes_group : m->duvi_batch);
         info->device_bytes = m->device_bytes;
+        info->row_group = m->row_group;
+        info->reserved = 0;
     });
 }
 

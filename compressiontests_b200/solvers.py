@@ -278,6 +278,30 @@ class MultigridPcgSolver:
         N.check(N.lib().dv_mgpcg_solve_device(self.h, b_ptr, x_ptr, C.byref(st)))
         return _stats(st, "relative residual")
 
+    def solve_many(self, B):
+        """Solve k load cases at once: B is n x k (column j = load case j), k <= 128.
+
+        Returns (X, stats, converged) with X n x k and converged a length-k bool array.
+        Replaces PcgSolver2.InverseSystemMatrixTimesOtherMatrix (PcgSolver2.cs:92-136),
+        which solves the columns one after another.
+        """
+        B = np.ascontiguousarray(B, np.float64)
+        if B.ndim != 2 or B.shape[0] != self.n:
+            raise ValueError(f"B must be {self.n} x k")
+        k = B.shape[1]
+        X = np.empty_like(B)
+        conv = np.zeros(k, np.int32)
+        st = N.Stats()
+        N.check(N.lib().dv_mgpcg_solve_multi(self.h, k, N.ptr(B), N.ptr(X), N.ptr(conv), C.byref(st)))
+        return X, _stats(st, "worst relative residual"), conv.astype(bool)
+
+    def solve_many_device(self, k, B_ptr, X_ptr):
+        """Device-resident n x k FP64 blocks (row-interleaved); returns (stats, converged)."""
+        conv = np.zeros(k, np.int32)
+        st = N.Stats()
+        N.check(N.lib().dv_mgpcg_solve_multi_device(self.h, k, B_ptr, X_ptr, N.ptr(conv), C.byref(st)))
+        return _stats(st, "worst relative residual"), conv.astype(bool)
+
     def release(self):
         if getattr(self, "h", None) is not None:
             N.lib().dv_mgpcg_destroy(self.h)

@@ -110,6 +110,8 @@ typedef struct {
     int32_t value_index_bits;  /* 8, 16, 32 (DuVi) */
     int32_t kernel_variant;    /* autotuned launch shape */
     int64_t device_bytes;      /* bytes one product reads from the matrix arrays */
+    int32_t row_group;         /* 3 (or 2) when consecutive rows share one column list (node dofs), else 1 */
+    int32_t reserved;
 } dv_matrix_info;
 
 /* CSR upload (uint row offsets / column indices / double values of
@@ -229,6 +231,19 @@ DV_API int dv_mgpcg_solve(dv_mgpcg *s, const double *b, double *x, dv_stats *sta
 DV_API int dv_mgpcg_solve_device(dv_mgpcg *s, const double *d_b, double *d_x, dv_stats *stats);
 /* Effective Jacobi weight omega_eff applied to D^-1 on V-cycle level l. */
 DV_API int dv_mgpcg_omega(const dv_mgpcg *s, int32_t level, double *omega_eff);
+/* k load cases (1 <= k <= 128) in one solve on the same hierarchy.  B and X are
+ * n x k row-interleaved (B[i*k + j] = load case j at dof i).  Every operator
+ * application reads the matrix once for all k vectors; each load case has its
+ * own FCG scalars and stops at ||r_j|| <= tol ||b_j|| (FP64-verified).
+ * converged_per_rhs (optional, k entries) receives 1 per converged load case;
+ * stats->relative_residual is the worst case.  Replaces calling
+ * PcgSolver2.InverseSystemMatrixTimesOtherMatrix (PcgSolver2.cs:92-136), which
+ * solves the columns one after another. */
+DV_API int dv_mgpcg_solve_multi(dv_mgpcg *s, int32_t k, const double *B, double *X, int32_t *converged_per_rhs,
+                                dv_stats *stats);
+/* Same with device-resident B and X (FP64, n x k), context stream. */
+DV_API int dv_mgpcg_solve_multi_device(dv_mgpcg *s, int32_t k, const double *d_B, double *d_X,
+                                       int32_t *converged_per_rhs, dv_stats *stats);
 DV_API int dv_mgpcg_destroy(dv_mgpcg *s);
 
 /* ---- structured hex workload generator (FemCantilever3D on unit cubes) ----

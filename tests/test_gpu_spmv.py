@@ -139,21 +139,56 @@ def test_duvi_long_rows_fallback(ctx, native, oracle, rng):
     np.testing.assert_array_equal(y, oracle.DuVi(oracle.Csr.from_scipy(A), 0.0).spmv(x))
 
 
-@pytest.mark.parametrize("fmt", ["csr", "duvi"])
-@pytest.mark.parametrize("k", [1, 7, 64, 130])
-def test_spmm(ctx, native, cantilever, rng, fmt, k):
+def _spmm(native, M, X, dtype):
     import torch
+    dX = torch.from_numpy(np.ascontiguousarray(X, dtype)).cuda()
+    dY = torch.zeros((M.shape[0], X.shape[1]), dtype=dX.dtype, device="cuda")
+    torch.cuda.synchronize()
+    M.multiply_many_device(X.shape[1], dX.data_ptr(), dY.data_ptr(), "f64" if dtype == np.float64 else "f32")
+    M.ctx.synchronize()
+    return dY.cpu().numpy()
+
+
+@pytest.mark.parametrize("fmt", ["csr", "duvi"])
+@pytest.mark.parametrize("k", [1, 7, 33, 64, 130])
+def test_spmm_bit_exact(ctx, native, oracle, cantilever, rng, fmt, k):
+    # One warp per node group, lanes over right-hand sides, each row summed in
+    # storage order: every column equals the oracle's sequential product bit for bit.
     m, A = cantilever
     X = rng.standard_normal((A.shape[1], k))
     M = native.SparseMatrix(ctx, A, fmt)
-    dX = torch.from_numpy(np.ascontiguousarray(X)).cuda()
-    dY = torch.zeros((A.shape[0], k), dtype=torch.float64, device="cuda")
-    torch.cuda.synchronize()
-    M.multiply_many_device(k, dX.data_ptr(), dY.data_ptr())
-    ctx.synchronize()
-    Y = dY.cpu().numpy()
-    ref = A @ X
-    assert np.max(np.abs(Y - ref)) <= REL64 * np.max(np.abs(A) @ np.abs(X))
+    assert M.info()["row_group"] == 3
+    Y = _spmm(native, M, X, np.float64)
+    ref_op = oracle.DuVi(m.kff) if fmt == "duvi" else m.kff
+    for j in range(k):
+        np.testing.assert_array_equal(Y[:, j], ref_op.spmv(X[:, j]))
+
+
+@pytest.mark.parametrize("fmt", ["csr", "duvi"])
+def test_spmm_ungrouped_rows_bit_exact(ctx, native, oracle, rng, fmt):
+    A = random_csr(rng, 700, 900, 0.02, empty_rows=(0, 5, 699))
+    X = rng.standard_normal((900, 40))
+    M = native.SparseMatrix(ctx, A, fmt, dedup_tol=0.0)
+    assert M.info()["row_group"] == 1
+    Y = _spmm(native, M, X, np.float64)
+    ref = oracle.Csr.from_scipy(A)
+    ref_op = oracle.DuVi(ref, 0.0) if fmt == "duvi" else ref
+    for j in range(40):
+        np.testing.assert_array_equal(Y[:, j], ref_op.spmv(X[:, j]))
+    assert not Y[[0, 5, 699]].any()
+
+
+def test_spmm_f32_duvi_equals_single_products(ctx, native, cantilever, rng):
+    # FP32 DuVi: the block product and the single-vector kernel both sum each row
+    # in storage order with fused multiply-adds, so the results are identical.
+    m, A = cantilever
+    X = rng.standard_normal((A.shape[1], 33)).astype(np.float32)
+    M = native.SparseMatrix(ctx, A, "duvi", "f32")
+    Y = _spmm(native, M, X, np.float32)
+    for j in (0, 17, 32):
+        np.testing.assert_array_equal(Y[:, j], M.Multiply(X[:, j].astype(np.float64)).astype(np.float32))
+    X64 = X.astype(np.float64)
+    assert np.max(np.abs(Y - A @ X64) / (abs(A) @ np.abs(X64) + 1e-300)) <= REL32
 
 
 def test_residual_device(ctx, native, cantilever, rng):
