@@ -27,6 +27,7 @@ using dvk::madd;
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int kMaxCols = 128;   // columns of one launch (lanes x U)
+constexpr int kReduceBlocksPerSm = 8;   // grid cap of products and vector kernels that reduce per column
 
 // ---------------------------------------------------------------------------
 // per-column deterministic grid reduction
@@ -34,7 +35,7 @@ constexpr int kMaxCols = 128;   // columns of one launch (lanes x U)
 // acc[u][c]: this lane's sums for column j = lane + 32 u.  Partials hold
 // gridDim.x * kc * NC doubles.  The last block calls fin(j, totals) for each column.
 template <int NC, int U, class Fin>
-__device__ void col_reduce(double (&acc)[U][NC], int kc, double *partials, unsigned *ticket, Fin fin) {
+__device__ __forceinline__ void col_reduce(double (&acc)[U][NC], int kc, double *partials, unsigned *ticket, Fin fin) {
     __shared__ double sh[kWarps][32 * U * NC];
     __shared__ int is_last;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -144,20 +145,67 @@ struct BEpiJacobiFromZero {   // two sweeps from zero: Y = wB + w (B - A (wB))
 
 // ---------------------------------------------------------------------------
 // block product kernels
+//
+// A warp walks its group's entries in chunks of 32: the lanes decode one
+// entry each (coalesced loads of columns, gaps and value indices; for DuVi a
+// segmented warp scan turns block starts and gaps into columns) into a
+// shared-memory record {column, G values}, then every lane runs over the
+// chunk's records (one broadcast shared load per entry) and gathers its
+// columns of X.  Per entry the warp issues one shared load and U gathers.
 // ---------------------------------------------------------------------------
-template <class AT, int G, int U, class Gather, class Epi>
+template <class AT, int G>
+struct alignas(16) Rec {
+    uint32_t c;
+    AT a[G];
+};
+
+// EXACT: product rounded, then added (the oracle's order, bit-exact for FP64);
+// otherwise one fused multiply-add per term.
+template <class AT, int G, int U, bool EXACT, class Gather>
+__device__ __forceinline__ void chunk_fma(const Rec<AT, G> *rec, int n, int kc, int lane, const Gather &g,
+                                          AT (&acc)[G][U]) {
+#pragma unroll 4
+    for (int e = 0; e < n; ++e) {
+        const Rec<AT, G> r = rec[e];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int j = lane + 32 * u;
+            if (j < kc) {
+                const AT x = g(r.c, j);
+#pragma unroll
+                for (int t = 0; t < G; ++t) acc[t][u] = EXACT ? madd<AT>(acc[t][u], r.a[t], x) : fma(r.a[t], x, acc[t][u]);
+            }
+        }
+    }
+}
+
+template <class AT, int G, int U, class Epi>
+__device__ __forceinline__ void group_epilogue(int32_t r0, int kc, int lane, const Epi &ep, AT (&acc)[G][U],
+                                               double (&red)[U][Epi::NC > 0 ? Epi::NC : 1]) {
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        const int j = lane + 32 * u;
+        if (j < kc)
+#pragma unroll
+            for (int t = 0; t < G; ++t) ep.apply(r0 + t, j, acc[t][u], red[u]);
+    }
+}
+
+template <class AT, int G, int U, bool EXACT, class Gather, class Epi>
 __global__ void __launch_bounds__(kThreads) k_bprod_csr(const int32_t *__restrict__ rp, const int32_t *__restrict__ ci,
                                                         const AT *__restrict__ va, int32_t ngroups, int kc, Gather g,
                                                         Epi ep, const int *__restrict__ done, double *partials,
                                                         unsigned *ticket) {
     if (done && *(volatile const int *)done) return;
+    __shared__ Rec<AT, G> srec[kWarps][32];
     constexpr int NC = Epi::NC > 0 ? Epi::NC : 1;
     double red[U][NC];
 #pragma unroll
     for (int u = 0; u < U; ++u)
 #pragma unroll
         for (int c = 0; c < NC; ++c) red[u][c] = 0.0;
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    Rec<AT, G> *rec = srec[warp];
     const int32_t nw = (gridDim.x * blockDim.x) >> 5;
     for (int32_t grp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; grp < ngroups; grp += nw) {
         const int32_t r0 = grp * G;
@@ -170,29 +218,20 @@ __global__ void __launch_bounds__(kThreads) k_bprod_csr(const int32_t *__restric
         for (int t = 0; t < G; ++t)
 #pragma unroll
             for (int u = 0; u < U; ++u) acc[t][u] = AT(0);
-#pragma unroll 2
-        for (int32_t e = 0; e < len; ++e) {
-            const uint32_t c = (uint32_t)__ldg(ci + s[0] + e);
-            AT a[G];
+        for (int32_t off = 0; off < len; off += 32) {
+            const int n = min(32, len - off);
+            if (lane < n) {
+                Rec<AT, G> r;
+                r.c = (uint32_t)__ldg(ci + s[0] + off + lane);
 #pragma unroll
-            for (int t = 0; t < G; ++t) a[t] = __ldg(va + s[t] + e);
-#pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const int j = lane + 32 * u;
-                if (j < kc) {
-                    const AT x = g(c, j);
-#pragma unroll
-                    for (int t = 0; t < G; ++t) acc[t][u] = madd<AT>(acc[t][u], a[t], x);
-                }
+                for (int t = 0; t < G; ++t) r.a[t] = __ldg(va + s[t] + off + lane);
+                rec[lane] = r;
             }
+            __syncwarp();
+            chunk_fma<AT, G, U, EXACT>(rec, n, kc, lane, g, acc);
+            __syncwarp();
         }
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const int j = lane + 32 * u;
-            if (j < kc)
-#pragma unroll
-                for (int t = 0; t < G; ++t) ep.apply(r0 + t, j, acc[t][u], red[u]);
-        }
+        group_epilogue<AT, G, U>(r0, kc, lane, ep, acc, red);
     }
     if constexpr (Epi::NC > 0) col_reduce<Epi::NC, U>(red, kc, partials, ticket, ep.fin);
 }
@@ -205,6 +244,7 @@ struct BDuviArgs {
     const void *__restrict__ vidx;
     const void *__restrict__ values;
     int vi_bits;
+    int nuniq;
 };
 
 __device__ __forceinline__ uint32_t load_vi(const void *v, int bits, uint32_t i) {
@@ -213,64 +253,100 @@ __device__ __forceinline__ uint32_t load_vi(const void *v, int bits, uint32_t i)
     return __ldg(static_cast<const uint32_t *>(v) + i);
 }
 
-// Walks the leader row's blocks (count byte at a block start, gap bytes
-// inside: DuViGeometricMultigrid.cl:84-98); the G rows of a group have equal
-// block structure, so their value indices sit at the same offsets of their
-// own entry ranges.
-template <class AT, int G, int U, class Gather, class Epi>
+// DuVi rows (DuViGeometricMultigrid.cl:84-98): a row is a run of blocks; the
+// first entry byte of a block holds the count of its following entries, the
+// others hold gap - 1; block start columns are in col_idx.  The G rows of a
+// group share their block structure, so their value indices sit at the same
+// offsets of their own entry ranges.  Chunk decode: block starts inside the
+// chunk are found by hopping count bytes (one shuffle per block), then a
+// segmented inclusive scan over the lanes gives every entry its column.
+template <class AT, int G, int U, bool EXACT, class Gather, class Epi>
 __global__ void __launch_bounds__(kThreads) k_bprod_duvi(BDuviArgs A, int32_t ngroups, int kc, Gather g, Epi ep,
                                                          const int *__restrict__ done, double *partials,
                                                          unsigned *ticket) {
     if (done && *(volatile const int *)done) return;
+    __shared__ Rec<AT, G> srec[kWarps][32];
+    __shared__ AT stab[256];
     constexpr int NC = Epi::NC > 0 ? Epi::NC : 1;
+    const AT *gtab = static_cast<const AT *>(A.values);
+    const bool smem_tab = A.vi_bits == 8;
+    if (smem_tab) {
+        for (int i = threadIdx.x; i < A.nuniq; i += blockDim.x) stab[i] = gtab[i];
+        __syncthreads();
+    }
     double red[U][NC];
 #pragma unroll
     for (int u = 0; u < U; ++u)
 #pragma unroll
         for (int c = 0; c < NC; ++c) red[u][c] = 0.0;
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned below = (1u << lane) - 1u;
+    Rec<AT, G> *rec = srec[warp];
     const int32_t nw = (gridDim.x * blockDim.x) >> 5;
-    const AT *tab = static_cast<const AT *>(A.values);
     for (int32_t grp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; grp < ngroups; grp += nw) {
         const int32_t r0 = grp * G;
-        const uint32_t b0 = __ldg(A.row_to_col + r0), b1 = __ldg(A.row_to_col + r0 + 1);
         uint32_t d[G];
 #pragma unroll
         for (int t = 0; t < G; ++t) d[t] = __ldg(A.row_to_dist + r0 + t);
+        const uint32_t len = __ldg(A.row_to_dist + r0 + 1) - d[0];
+        uint32_t bl = __ldg(A.row_to_col + r0);   // next block to start
+        uint32_t rem = 0;                           // entries of the open block not yet decoded
+        uint32_t ccur = 0;                          // column of the last decoded entry
         AT acc[G][U];
 #pragma unroll
         for (int t = 0; t < G; ++t)
 #pragma unroll
             for (int u = 0; u < U; ++u) acc[t][u] = AT(0);
-        uint32_t off = 0;   // entry offset inside the rows
-        for (uint32_t bl = b0; bl < b1; ++bl) {
-            uint32_t c = __ldg(A.col_idx + bl);
-            const uint32_t cnt = __ldg(A.dist + d[0] + off);
-            for (uint32_t q = 0;; ++q) {
-                AT a[G];
-#pragma unroll
-                for (int t = 0; t < G; ++t) a[t] = __ldg(tab + load_vi(A.vidx, A.vi_bits, d[t] + off));
-#pragma unroll
-                for (int u = 0; u < U; ++u) {
-                    const int j = lane + 32 * u;
-                    if (j < kc) {
-                        const AT x = g(c, j);
-#pragma unroll
-                        for (int t = 0; t < G; ++t) acc[t][u] = madd<AT>(acc[t][u], a[t], x);
-                    }
-                }
-                ++off;
-                if (q == cnt) break;
-                c += __ldg(A.dist + d[0] + off) + 1u;
+        for (uint32_t off = 0; off < len; off += 32) {
+            const int n = (int)min(32u, len - off);
+            const bool act = lane < n;
+            const uint32_t db = act ? (uint32_t)__ldg(A.dist + d[0] + off + lane) : 0u;
+            // block starts of this chunk
+            unsigned mask = 0;
+            uint32_t p = rem;
+            while (p < (uint32_t)n) {
+                mask |= 1u << p;
+                p += __shfl_sync(0xffffffffu, db, (int)p) + 1u;
             }
-        }
+            rem = p - (uint32_t)n;
+            const bool start = (mask >> lane) & 1u;
+            const int nstart_le = __popc(mask & (below | (1u << lane)));   // starts at or before this lane
+            // segmented scan: heads are block starts (their col_idx) and lane 0 (continuing the open block)
+            uint32_t v;
+            bool head;
+            if (start) {
+                v = __ldg(A.col_idx + bl + nstart_le - 1);
+                head = true;
+            } else {
+                v = db + 1u + (lane == 0 ? ccur : 0u);
+                head = lane == 0;
+            }
 #pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const int j = lane + 32 * u;
-            if (j < kc)
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, v, o);
+                const bool hy = __shfl_up_sync(0xffffffffu, head, o);
+                if (lane >= o && !head) {
+                    v += y;
+                    head = hy;
+                }
+            }
+            bl += __popc(mask);
+            ccur = __shfl_sync(0xffffffffu, v, n - 1);
+            if (act) {
+                Rec<AT, G> r;
+                r.c = v;
 #pragma unroll
-                for (int t = 0; t < G; ++t) ep.apply(r0 + t, j, acc[t][u], red[u]);
+                for (int t = 0; t < G; ++t) {
+                    const uint32_t idx = load_vi(A.vidx, A.vi_bits, d[t] + off + lane);
+                    r.a[t] = smem_tab ? stab[idx] : __ldg(gtab + idx);
+                }
+                rec[lane] = r;
+            }
+            __syncwarp();
+            chunk_fma<AT, G, U, EXACT>(rec, n, kc, lane, g, acc);
+            __syncwarp();
         }
+        group_epilogue<AT, G, U>(r0, kc, lane, ep, acc, red);
     }
     if constexpr (Epi::NC > 0) col_reduce<Epi::NC, U>(red, kc, partials, ticket, ep.fin);
 }
@@ -279,42 +355,42 @@ __global__ void __launch_bounds__(kThreads) k_bprod_duvi(BDuviArgs A, int32_t ng
 // (products that reduce use fewer blocks so the last block's sum stays short).
 inline int bprod_blocks(const LaunchEnv &e, int64_t ngroups, bool reduces) {
     const int64_t want = (ngroups * 32 + kThreads - 1) / kThreads;
-    const int64_t cap = reduces ? (int64_t)e.ctx->num_sms * 4 : (int64_t)e.max_blocks;
+    const int64_t cap = reduces ? (int64_t)e.ctx->num_sms * kReduceBlocksPerSm : (int64_t)e.max_blocks;
     return (int)std::max<int64_t>(1, std::min<int64_t>(want, cap));
 }
 
-template <class AT, int G, int U, class Gather, class Epi>
+template <class AT, int G, int U, bool EXACT, class Gather, class Epi>
 void launch_bprod_gu(const LaunchEnv &e, const dv_matrix *m, int kc, Gather g, Epi ep) {
     const int32_t ngroups = m->n_rows / G;
     const int blocks = bprod_blocks(e, ngroups, Epi::NC > 0);
     if (m->format == DV_FORMAT_CSR) {
-        k_bprod_csr<AT, G, U, Gather, Epi><<<blocks, kThreads, 0, e.stream>>>(
+        k_bprod_csr<AT, G, U, EXACT, Gather, Epi><<<blocks, kThreads, 0, e.stream>>>(
             m->rowptr.as<int32_t>(), m->col.as<int32_t>(), static_cast<const AT *>(m->val.p), ngroups, kc, g, ep,
             e.done, e.partials, e.ticket);
     } else {
         BDuviArgs a{m->row_to_col.as<uint32_t>(), m->row_to_dist.as<uint32_t>(), m->col_idx.as<uint32_t>(),
-                    m->dist.as<uint8_t>(), m->vidx.p, m->values.p, m->vi_bits};
-        k_bprod_duvi<AT, G, U, Gather, Epi><<<blocks, kThreads, 0, e.stream>>>(a, ngroups, kc, g, ep, e.done,
-                                                                               e.partials, e.ticket);
+                    m->dist.as<uint8_t>(), m->vidx.p, m->values.p, m->vi_bits, (int)m->nuniq};
+        k_bprod_duvi<AT, G, U, EXACT, Gather, Epi><<<blocks, kThreads, 0, e.stream>>>(a, ngroups, kc, g, ep, e.done,
+                                                                                      e.partials, e.ticket);
     }
     DV_CUDA(cudaGetLastError());
     e.ctx->count();
 }
 
 // Y-epilogue product over kc <= kMaxCols columns; the matrix's values have type AT.
-template <class AT, class Gather, class Epi>
+template <class AT, bool EXACT = true, class Gather, class Epi>
 void launch_bprod(const LaunchEnv &e, const dv_matrix *m, int kc, Gather g, Epi ep) {
     DV_REQUIRE(kc >= 1 && kc <= kMaxCols, DV_ERR_ARG, "block product of more than 128 columns");
     const bool g3 = m->row_group == 3;
     if (kc <= 32) {
-        if (g3) launch_bprod_gu<AT, 3, 1>(e, m, kc, g, ep);
-        else launch_bprod_gu<AT, 1, 1>(e, m, kc, g, ep);
+        if (g3) launch_bprod_gu<AT, 3, 1, EXACT>(e, m, kc, g, ep);
+        else launch_bprod_gu<AT, 1, 1, EXACT>(e, m, kc, g, ep);
     } else if (kc <= 64) {
-        if (g3) launch_bprod_gu<AT, 3, 2>(e, m, kc, g, ep);
-        else launch_bprod_gu<AT, 1, 2>(e, m, kc, g, ep);
+        if (g3) launch_bprod_gu<AT, 3, 2, EXACT>(e, m, kc, g, ep);
+        else launch_bprod_gu<AT, 1, 2, EXACT>(e, m, kc, g, ep);
     } else {
-        if (g3) launch_bprod_gu<AT, 3, 4>(e, m, kc, g, ep);
-        else launch_bprod_gu<AT, 1, 4>(e, m, kc, g, ep);
+        if (g3) launch_bprod_gu<AT, 3, 4, EXACT>(e, m, kc, g, ep);
+        else launch_bprod_gu<AT, 1, 4, EXACT>(e, m, kc, g, ep);
     }
 }
 

@@ -151,29 +151,37 @@ __global__ void k_bfcg_stop(const ColScalars *cs, int k, dvk::SolverScalars *sc)
     }
 }
 
-// ||v_j||^2 per column, one block per column, fixed order: into bb (slot 0) or rr (slot 1)
-__global__ void k_bnorm_cols(const double *__restrict__ v, int32_t n, int k, ColScalars *cs, int slot) {
-    __shared__ double sh[dvb::kThreads];
-    const int j = blockIdx.x;
-    double t = 0.0;
-    for (int32_t i = threadIdx.x; i < n; i += blockDim.x) {
-        const double a = v[(size_t)i * k + j];
-        t += a * a;
-    }
-    sh[threadIdx.x] = t;
-    __syncthreads();
-    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-        if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) {
+// ||v_j||^2 per column into bb (slot 0; a zero load case is converged at once) or rr (slot 1)
+struct FinNorm {
+    ColScalars *cs;
+    int slot;
+    __device__ void operator()(int j, const double *t) const {
         if (slot == 0) {
-            cs[j].bb = sh[0];
-            if (sh[0] == 0.0) cs[j].converged = 1;   // zero load case: x_j = 0 is exact
+            cs[j].bb = t[0];
+            if (t[0] == 0.0) cs[j].converged = 1;   // x_j = 0 is exact
         } else {
-            cs[j].rr = sh[0];
+            cs[j].rr = t[0];
         }
     }
+};
+template <int U>
+__global__ void __launch_bounds__(dvb::kThreads) k_bnorm(const double *__restrict__ v, int32_t n, int k, ColScalars *cs,
+                                                         int slot, double *partials, unsigned *ticket) {
+    double red[U][1];
+#pragma unroll
+    for (int u = 0; u < U; ++u) red[u][0] = 0.0;
+    const int lane = threadIdx.x & 31;
+    const int32_t nw = (gridDim.x * blockDim.x) >> 5;
+    for (int32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nw)
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int j = lane + 32 * u;
+            if (j < k) {
+                const double a = v[(size_t)i * k + j];
+                red[u][0] += a * a;
+            }
+        }
+    dvb::col_reduce<1, U>(red, k, partials, ticket, FinNorm{cs, slot});
 }
 
 template <class T>
@@ -185,20 +193,28 @@ __global__ void k_bscale(const T *__restrict__ w, const T *__restrict__ b, T *__
         x[q] = w[q / k] * b[q];
 }
 
-// Y = Ainv B on the coarsest level (dense inverse, nc x nc, times nc x k);
-// one thread per output, the Ainv row read in order.
+// Y = Ainv B on the coarsest level (dense inverse, nc x nc row-major, times
+// nc x k): a block computes 8 rows x 32 columns, one output per thread, over
+// 32-wide tiles of Ainv and B staged in shared memory.
 template <class T>
-__global__ void k_bcoarse(const T *__restrict__ a, const T *__restrict__ b, T *__restrict__ y, int32_t nc, int k,
-                          const int *__restrict__ done) {
+__global__ void __launch_bounds__(256) k_bcoarse(const T *__restrict__ a, const T *__restrict__ b, T *__restrict__ y,
+                                                 int32_t nc, int k, const int *__restrict__ done) {
     if (done && *(volatile const int *)done) return;
-    const size_t tot = (size_t)nc * k;
-    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < tot; q += (size_t)gridDim.x * blockDim.x) {
-        const size_t r = q / k, j = q % k;
-        const T *ar = a + r * nc;
-        T s = 0;
-        for (int32_t c = 0; c < nc; ++c) s += ar[c] * b[(size_t)c * k + j];
-        y[q] = s;
+    __shared__ T As[8][33];
+    __shared__ T Bs[32][33];
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const int32_t row = blockIdx.x * 8 + ty;
+    const int col = blockIdx.y * 32 + tx;
+    T s = 0;
+    for (int32_t c0 = 0; c0 < nc; c0 += 32) {
+        As[ty][tx] = (row < nc && c0 + tx < nc) ? a[(size_t)row * nc + c0 + tx] : T(0);
+        for (int q = ty; q < 32; q += 8) Bs[q][tx] = (c0 + q < nc && col < k) ? b[(size_t)(c0 + q) * k + col] : T(0);
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < 32; ++q) s += As[ty][q] * Bs[q][tx];
+        __syncthreads();
     }
+    if (row < nc && col < k) y[(size_t)row * k + col] = s;
 }
 
 // ---------------------------------------------------------------------------
@@ -220,8 +236,8 @@ T *block_vcycle(const LaunchEnv &e, VCycle<T> &vc, BlockLevels<T> &W, size_t l, 
     cudaStream_t s = e.stream;
     dv_context *ctx = vc.ctx;
     if (l == vc.lv.size()) {
-        k_bcoarse<T><<<vec_grid(ctx, (size_t)vc.nc * k), 256, 0, s>>>(vc.ainv.template as<T>(), b,
-                                                                      W.xc.template as<T>(), vc.nc, k, e.done);
+        k_bcoarse<T><<<dim3((vc.nc + 7) / 8, (k + 31) / 32), 256, 0, s>>>(vc.ainv.template as<T>(), b,
+                                                                          W.xc.template as<T>(), vc.nc, k, e.done);
         DV_CUDA(cudaGetLastError());
         ctx->count();
         return W.xc.template as<T>();
@@ -293,7 +309,7 @@ void multi_solve(dv_mgpcg *s, VCycle<T> &vc, MultiState<T> &M, int k, const doub
         M.Q.alloc(8 * nk);
         if (kMixed) M.Rlow.alloc(4 * nk);
         M.cols.alloc(sizeof(ColScalars) * (size_t)k);
-        M.red.alloc(64 + sizeof(double) * 2 * (size_t)kMaxK * ctx->num_sms * 4);
+        M.red.alloc(64 + sizeof(double) * 2 * (size_t)kMaxK * ctx->num_sms * dvb::kReduceBlocksPerSm);
         M.ws = std::make_unique<SolverWs>(ctx);
     }
     SolverWs &ws = *M.ws;
@@ -310,6 +326,15 @@ void multi_solve(dv_mgpcg *s, VCycle<T> &vc, MultiState<T> &M, int k, const doub
     LaunchEnv ed = e0;
     ed.done = &ws.sc()->done;
     ColScalars *cs = M.cols.template as<ColScalars>();
+    const int gw = (int)std::max<int64_t>(1, std::min<int64_t>(((int64_t)n * 32 + 255) / 256,
+                                                                (int64_t)ctx->num_sms * dvb::kReduceBlocksPerSm));
+    auto norms = [&](const double *v, int slot) {
+        if (k <= 32) k_bnorm<1><<<gw, dvb::kThreads, 0, st>>>(v, n, k, cs, slot, e0.partials, e0.ticket);
+        else if (k <= 64) k_bnorm<2><<<gw, dvb::kThreads, 0, st>>>(v, n, k, cs, slot, e0.partials, e0.ticket);
+        else k_bnorm<4><<<gw, dvb::kThreads, 0, st>>>(v, n, k, cs, slot, e0.partials, e0.ticket);
+        DV_CUDA(cudaGetLastError());
+        ctx->count();
+    };
     std::vector<ColScalars> hc(k);
     for (auto &c : hc) {
         std::memset(&c, 0, sizeof(c));
@@ -318,9 +343,7 @@ void multi_solve(dv_mgpcg *s, VCycle<T> &vc, MultiState<T> &M, int k, const doub
     }
     DV_CUDA(cudaMemcpyAsync(cs, hc.data(), sizeof(ColScalars) * k, cudaMemcpyHostToDevice, st));
     DV_CUDA(cudaMemcpyAsync(M.B.p, dB, 8 * nk, cudaMemcpyDeviceToDevice, st));
-    k_bnorm_cols<<<k, dvb::kThreads, 0, st>>>(M.B.template as<double>(), n, k, cs, 0);
-    DV_CUDA(cudaGetLastError());
-    ctx->count();
+    norms(M.B.template as<double>(), 0);
     DV_CUDA(cudaMemsetAsync(M.X.p, 0, 8 * nk, st));
     DV_CUDA(cudaMemcpyAsync(M.R.p, M.B.p, 8 * nk, cudaMemcpyDeviceToDevice, st));
     DV_CUDA(cudaMemsetAsync(M.Pv.p, 0, 8 * nk, st));
@@ -336,7 +359,6 @@ void multi_solve(dv_mgpcg *s, VCycle<T> &vc, MultiState<T> &M, int k, const doub
     };
     to_low();
     const T *z = block_vcycle<T>(ed, vc, M.W, 0, rin, k);
-    const int gw = (int)std::max<int64_t>(1, std::min<int64_t>(((int64_t)n * 32 + 255) / 256, ctx->num_sms * 4));
     const int per = s->cfg.iterations_per_sync > 0 ? s->cfg.iterations_per_sync : 4;
     const double tol2 = h.tol2;
     const T *zfinal = z;
@@ -363,7 +385,7 @@ void multi_solve(dv_mgpcg *s, VCycle<T> &vc, MultiState<T> &M, int k, const doub
         const T *zz = z;
         for (int it = 0; it < per; ++it) {
             launch_red(zz);
-            launch_bprod<double>(ed, s->Aout.get(), k, BGatherVec<T, double>{zz, k},
+            launch_bprod<double, false>(ed, s->Aout.get(), k, BGatherVec<T, double>{zz, k},
                                  BEpiFcg<T>{zz, Pd, Qd, cs, k, FinFcg{cs}});
             launch_update();
             zz = block_vcycle<T>(ed, vc, M.W, 0, rin, k);
@@ -373,9 +395,7 @@ void multi_solve(dv_mgpcg *s, VCycle<T> &vc, MultiState<T> &M, int k, const doub
     auto true_residual = [&] {   // into Pd (free once the recurrence stopped)
         launch_bprod<double>(e0, s->Aout.get(), k, BGatherVec<double, double>{Xd, k},
                              BEpiResid<double>{M.B.template as<double>(), Pd, k, {}});
-        k_bnorm_cols<<<k, dvb::kThreads, 0, st>>>(Pd, n, k, cs, 1);
-        DV_CUDA(cudaGetLastError());
-        ctx->count();
+        norms(Pd, 1);
         DV_CUDA(cudaMemcpyAsync(hc.data(), cs, sizeof(ColScalars) * k, cudaMemcpyDeviceToHost, st));
         DV_CUDA(cudaStreamSynchronize(st));
     };
