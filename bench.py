@@ -58,6 +58,7 @@ def parse():
                    help="only the multi-load-case MG-PCG (64 load cases on the 64^3 mesh)")
     p.add_argument("--batch-size", type=int, default=64, help="mesh edge of the multi-load-case section")
     p.add_argument("--batch-k", type=int, default=64, help="load cases of the multi-load-case section")
+    p.add_argument("--batch-meshes", type=int, default=32, help="meshes of the batched-mesh section")
     p.add_argument("--spmv-only", default=None, metavar="FMT_PREC",
                    help="only time the SpMV of the finest operator (duvi_f32, duvi_f64, csr_f32, csr_f64): "
                         "the small case used for ncu captures")
@@ -370,7 +371,9 @@ def run_ours(args):
 
     batched = None
     if not args.no_batched:
-        batched = batched_multi_rhs(cb, ctx, stream, args.batch_size, args.batch_k, max(1, args.steps // 2), args.tol)
+        batched = {"load_cases": batched_multi_rhs(cb, ctx, stream, args.batch_size, args.batch_k,
+                                                   max(1, args.steps // 2), args.tol),
+                   "meshes": batched_meshes(cb, ctx, stream, args.batch_meshes, max(1, args.steps // 2), args.tol)}
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -454,12 +457,70 @@ def batched_multi_rhs(cb, ctx, stream, size, k, steps, tol):
             "speedup_vs_sequential": round(ms_seq / ms_multi, 2), "gpu_launches_per_solve": int(launches)}
 
 
+def batched_meshes(cb, ctx, stream, n_meshes, steps, tol):
+    """n_meshes cantilevers with edge lengths U{8..48} (seeded), Galerkin hierarchies, unit
+    traction on each free face: one batched solve (block-diagonal levels, graph-captured)
+    against the same meshes solved one after another with one solver each."""
+    import torch
+    t = time.time()
+    dims, meshes, rhs = cb.cantilever_batch(n_meshes, 8, 48, seed=20261203)
+    t_build = time.time() - t
+    t = time.time()
+    s = cb.BatchedMultigridSolver(ctx, meshes, precision="mixed", fmt="duvi", nu=2, omega=2 / 3,
+                                  omega_mode="spectral", tol=tol, max_iterations=500)
+    t_setup = time.time() - t
+    b = torch.from_numpy(np.concatenate(rhs)).cuda()
+    x = torch.zeros_like(b)
+    torch.cuda.synchronize()
+    st, conv, its = s.solve_device(b.data_ptr(), x.data_ptr())
+    l0 = ctx.launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        st, conv, its = s.solve_device(b.data_ptr(), x.data_ptr())
+        assert conv.all(), st
+    e1.record(stream)
+    e1.synchronize()
+    ms_batch = e0.elapsed_time(e1) / steps
+    launches = (ctx.launch_count() - l0) // steps
+    xs = np.split(x.cpu().numpy(), s.offsets[1:-1])
+    worst = max(float(np.linalg.norm(r - A[0] @ xm) / np.linalg.norm(r)) for (A, _), r, xm in zip(meshes, rhs, xs))
+    info = s.info()
+    s.release()
+    # the same meshes one after another, one solver per mesh (the reference's one-model-per-solver shape)
+    ms_seq, its_seq = 0.0, []
+    for (A, P), r in zip(meshes, rhs):
+        one = cb.MultigridPcgSolver(ctx, A, P, precision="mixed", fmt="duvi", nu=2, omega=2 / 3,
+                                    omega_mode="spectral", tol=tol, max_iterations=500)
+        db = torch.from_numpy(r).cuda()
+        dx = torch.zeros_like(db)
+        torch.cuda.synchronize()
+        one.solve_device(db.data_ptr(), dx.data_ptr())
+        e0.record(stream)
+        st1 = one.solve_device(db.data_ptr(), dx.data_ptr())
+        e1.record(stream)
+        e1.synchronize()
+        ms_seq += e0.elapsed_time(e1)
+        its_seq.append(st1.NumIterationsRequired)
+        one.release()
+    return {"workload": f"{n_meshes} cantilevers, edge lengths U{{8..48}} per axis (seeded), unit traction, "
+                        "Galerkin hierarchies to <= 1000 coarse dofs, mixed MG-PCG per mesh to "
+                        f"{tol:g}, one batched graph-captured solve",
+            "n_dofs": int(s.n), "levels_max": info["n_levels_max"], "ms": round(ms_batch, 3),
+            "iterations_max": int(its.max()), "worst_relative_residual_fp64": worst,
+            "sequential_ms": round(ms_seq, 3), "sequential_iterations_max": int(max(its_seq)),
+            "speedup_vs_sequential": round(ms_seq / ms_batch, 2), "gpu_launches_per_solve": int(launches),
+            "launches_per_graph_chunk": info["launches_per_chunk"],
+            "setup_s": {"hierarchies": round(t_build, 1), "solver": round(t_setup, 1)}}
+
+
 def run_batched_only(args):
     import torch
     import compressiontests_b200 as cb
     ctx = cb.CudaContext(0)
-    r = batched_multi_rhs(cb, ctx, torch.cuda.ExternalStream(ctx.stream), args.batch_size, args.batch_k,
-                          args.steps, args.tol)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    r = {"load_cases": batched_multi_rhs(cb, ctx, stream, args.batch_size, args.batch_k, args.steps, args.tol),
+         "meshes": batched_meshes(cb, ctx, stream, args.batch_meshes, args.steps, args.tol)}
     print(json.dumps({"batched": r}), flush=True)
     ctx.close()
 

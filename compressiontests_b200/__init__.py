@@ -9,14 +9,14 @@ from . import _native
 from ._native import DuviError, NotImplementedFeatureError, NotInitializedError, NoDeviceError
 from .sparse import CudaContext, SparseMatrix
 from .solvers import (CudaCsrGeometricMultigridSolver, CudaCsrPcgSolver, CudaDuViGeometricMultigridSolver,
-                      IterativeStatistics, MultigridPcgSolver, make_path)
-from .cantilever import (FemCantilever3D, cartesian_transfer, hex_hierarchy, hex_stiffness, hex_trilinear,
-                         random_face_loads, traction_rhs)
+                      BatchedMultigridSolver, IterativeStatistics, MultigridPcgSolver, make_path)
+from .cantilever import (FemCantilever3D, cantilever_batch, cartesian_transfer, galerkin, galerkin_hierarchy,
+                         hex_hierarchy, hex_stiffness, hex_trilinear, random_face_loads, traction_rhs)
 
 __all__ = [
     "CudaContext", "SparseMatrix", "CudaCsrGeometricMultigridSolver", "CudaDuViGeometricMultigridSolver",
-    "CudaCsrPcgSolver", "MultigridPcgSolver", "IterativeStatistics", "FemCantilever3D", "hex_hierarchy",
-    "hex_stiffness", "hex_trilinear", "traction_rhs", "random_face_loads", "cartesian_transfer", "make_path", "DuviError",
+    "CudaCsrPcgSolver", "MultigridPcgSolver", "BatchedMultigridSolver", "cantilever_batch", "IterativeStatistics", "FemCantilever3D", "hex_hierarchy",
+    "hex_stiffness", "hex_trilinear", "galerkin", "galerkin_hierarchy", "traction_rhs", "random_face_loads", "cartesian_transfer", "make_path", "DuviError",
     "NotImplementedFeatureError", "NotInitializedError", "NoDeviceError",
 ]
 

@@ -119,10 +119,18 @@ _SIGNATURES = {
     "dv_mgpcg_solve_multi": (C.c_int, [_vp, C.c_int32, _vp, _vp, _vp, _P(Stats)]),
     "dv_mgpcg_solve_multi_device": (C.c_int, [_vp, C.c_int32, _vp, _vp, _vp, _P(Stats)]),
     "dv_mgpcg_destroy": (C.c_int, [_vp]),
+    "dv_batch_create": (C.c_int, [_vp, C.c_int32, _vp, _vp, _vp, _P(MgpcgConfig), _P(_vp)]),
+    "dv_batch_info": (C.c_int, [_vp, _P(C.c_int32), _P(C.c_int32), _P(C.c_int32)]),
+    "dv_batch_omega": (C.c_int, [_vp, C.c_int32, _P(C.c_double)]),
+    "dv_batch_solve": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _P(Stats)]),
+    "dv_batch_solve_device": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _P(Stats)]),
+    "dv_batch_destroy": (C.c_int, [_vp]),
     "dv_hex_csr_size": (C.c_int, [_vp, _P(C.c_int32), _P(C.c_int64)]),
     "dv_hex_assemble": (C.c_int, [_vp, _vp, C.c_double, C.c_double, C.c_double, _vp, _vp, _vp]),
     "dv_hex_trilinear_size": (C.c_int, [_vp, _P(C.c_int32), _P(C.c_int32), _P(C.c_int64)]),
     "dv_hex_trilinear": (C.c_int, [_vp, _vp, _vp, _vp]),
+    "dv_galerkin_size": (C.c_int, [_P(CsrHost), _P(CsrHost), _P(C.c_int32), _P(C.c_int64)]),
+    "dv_galerkin": (C.c_int, [_P(CsrHost), _P(CsrHost), _vp, _vp, _vp]),
     "dv_cartesian_transfer_size": (C.c_int, [C.c_int32, _vp, _vp, C.c_int32, C.c_int32, _vp, C.c_int32, _vp,
                                              _P(C.c_int64), _P(C.c_int64)]),
     "dv_cartesian_transfer": (C.c_int, [C.c_int32, _vp, _vp, C.c_int32, C.c_int32, _vp, C.c_int32, _vp, _vp, _vp, _vp,

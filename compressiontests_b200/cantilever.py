@@ -34,6 +34,8 @@ def hex_stiffness(ne, elem_E=None, scale=1.0, E=1.0, nu=0.3):
 
 
 def hex_trilinear(ne_fine):
+    """Trilinear prolongation of the factor-2 vertex coarsening (coarse nodes at the even
+    fine nodes and the last one, so odd element counts coarsen to ceil(n/2))."""
     ne = np.ascontiguousarray(ne_fine, np.int32)
     nr, nc, nnz = C.c_int32(), C.c_int32(), C.c_int64()
     N.check(N.lib().dv_hex_trilinear_size(N.ptr(ne), C.byref(nr), C.byref(nc), C.byref(nnz)))
@@ -42,6 +44,40 @@ def hex_trilinear(ne_fine):
     va = np.empty(nnz.value, np.float64)
     N.check(N.lib().dv_hex_trilinear(N.ptr(ne), N.ptr(rp), N.ptr(ci), N.ptr(va)))
     return sp.csr_matrix((va, ci, rp), shape=(nr.value, nc.value))
+
+
+def galerkin(A, P):
+    """Galerkin coarse operator P^T A P (native, sorted rows)."""
+    ah, ka = _host(A)
+    ph, kp = _host(P)
+    n, nnz = C.c_int32(), C.c_int64()
+    N.check(N.lib().dv_galerkin_size(C.byref(ah), C.byref(ph), C.byref(n), C.byref(nnz)))
+    rp = np.empty(n.value + 1, np.int32)
+    ci = np.empty(nnz.value, np.int32)
+    va = np.empty(nnz.value, np.float64)
+    N.check(N.lib().dv_galerkin(C.byref(ah), C.byref(ph), N.ptr(rp), N.ptr(ci), N.ptr(va)))
+    del ka, kp
+    return sp.csr_matrix((va, ci, rp), shape=(n.value, n.value))
+
+
+def _host(a):
+    from .sparse import _csr_arrays
+    rp, ci, va, shape = _csr_arrays(a)
+    return N.csr_host(rp, ci, va, shape)
+
+
+def galerkin_hierarchy(ne, max_coarse_dofs=1000, elem_E=None, E=1.0, nu=0.3):
+    """Hierarchy of an arbitrary ne[0] x ne[1] x ne[2] cantilever: vertex-based factor-2
+    coarsening (odd counts coarsen to ceil(n/2)), trilinear P, Galerkin A_{l+1} = P^T A_l P,
+    until the coarsest level has at most max_coarse_dofs dofs.  Returns (A_levels, P_levels)."""
+    ne = [int(n) for n in ne]
+    A = [hex_stiffness(ne, elem_E, 1.0, E, nu)]
+    P = []
+    while A[-1].shape[0] > max_coarse_dofs and max(ne) > 1:
+        P.append(hex_trilinear(ne))
+        A.append(galerkin(A[-1], P[-1]))
+        ne = [(n + 1) // 2 for n in ne]
+    return A, P
 
 
 def cartesian_transfer(dim, ne_fine, ne_coarse, dofs_per_node, fine_free, coarse_free):
@@ -181,3 +217,14 @@ def hex_hierarchy(ne, coarse_ne=8, elem_E=None, E=1.0, nu=0.3):
         ne = [n // 2 for n in ne]
         scale *= 2.0
     return A, P
+
+
+def cantilever_batch(n_meshes=32, lo=8, hi=48, seed=0, max_coarse_dofs=1000):
+    """n_meshes independent cantilevers whose three edge lengths are drawn uniformly from
+    lo..hi elements (seeded), each with its Galerkin hierarchy and the unit traction load
+    on its free face.  Returns (dims, meshes, rhs) with meshes = [(A_levels, P_levels)]."""
+    rng = np.random.default_rng(seed)
+    dims = [tuple(int(v) for v in rng.integers(lo, hi + 1, size=3)) for _ in range(n_meshes)]
+    meshes = [galerkin_hierarchy(ne, max_coarse_dofs) for ne in dims]
+    rhs = [traction_rhs(ne) for ne in dims]
+    return dims, meshes, rhs

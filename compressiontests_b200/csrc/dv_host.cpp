@@ -497,16 +497,36 @@ extern "C" DV_API int dv_hex_assemble(const int32_t *ne, const double *elem_E, d
     });
 }
 
+// Vertex-based factor-2 coarsening of one axis with n elements: coarse nodes
+// sit at the even fine nodes and at the last fine node (for odd n the last
+// coarse element has length 1).  Fine node i takes 1 or 2 coarse nodes with
+// the linear-interpolation weights; for even n this is standard trilinear.
+static int coarse_1d(int32_t i, int32_t n, int32_t idx[2], double w[2]) {
+    if ((i & 1) && i != n) {
+        idx[0] = i / 2;
+        idx[1] = i / 2 + 1;
+        w[0] = w[1] = 0.5;
+        return 2;
+    }
+    idx[0] = i == n ? (n + 1) / 2 : i / 2;
+    w[0] = 1.0;
+    return 1;
+}
+
 extern "C" DV_API int dv_hex_trilinear_size(const int32_t *nef, int32_t *n_rows, int32_t *n_cols, int64_t *nnz) {
     return dv_guard([&] {
-        DV_REQUIRE(nef && nef[0] >= 2 && nef[1] >= 2 && nef[2] >= 2 && nef[0] % 2 == 0 && nef[1] % 2 == 0 &&
-                       nef[2] % 2 == 0, DV_ERR_ARG, "trilinear transfer needs even element counts");
+        DV_REQUIRE(nef && nef[0] >= 1 && nef[1] >= 1 && nef[2] >= 1, DV_ERR_ARG, "element counts must be >= 1");
         int64_t nx = nef[0] + 1, ny = nef[1] + 1, nz = nef[2] + 1;
-        int64_t cx = nef[0] / 2 + 1, cy = nef[1] / 2 + 1, cz = nef[2] / 2 + 1;
+        int64_t cx = (nef[0] + 1) / 2 + 1, cy = (nef[1] + 1) / 2 + 1, cz = (nef[2] + 1) / 2 + 1;
         int64_t sx = 0, sy = 0, sz = 0;
-        for (int64_t i = 1; i < nx; ++i) sx += (i & 1) ? ((i / 2 == 0) ? 1 : 2) : 1;   // coarse x=0 is clamped
-        for (int64_t j = 0; j < ny; ++j) sy += (j & 1) ? 2 : 1;
-        for (int64_t k = 0; k < nz; ++k) sz += (k & 1) ? 2 : 1;
+        int32_t idx[2];
+        double w[2];
+        for (int32_t i = 1; i < nx; ++i) {   // coarse x = 0 is clamped
+            const int m = coarse_1d(i, nef[0], idx, w);
+            for (int a = 0; a < m; ++a) sx += idx[a] != 0;
+        }
+        for (int32_t j = 0; j < ny; ++j) sy += coarse_1d(j, nef[1], idx, w);
+        for (int32_t k = 0; k < nz; ++k) sz += coarse_1d(k, nef[2], idx, w);
         *n_rows = (int32_t)(3 * (nx - 1) * ny * nz);
         *n_cols = (int32_t)(3 * (cx - 1) * cy * cz);
         *nnz = 3 * sx * sy * sz;
@@ -520,7 +540,7 @@ extern "C" DV_API int dv_hex_trilinear(const int32_t *nef, int32_t *rowptr, int3
         int st = dv_hex_trilinear_size(nef, &nr, &nc, &nnz);
         DV_REQUIRE(st == DV_OK, st, "bad mesh");
         int32_t nx = nef[0] + 1, ny = nef[1] + 1, nz = nef[2] + 1;
-        int32_t cx = nef[0] / 2 + 1, cy = nef[1] / 2 + 1;
+        int32_t cx = (nef[0] + 1) / 2 + 1, cy = (nef[1] + 1) / 2 + 1;
         int64_t p = 0;
         int32_t r = 0;
         rowptr[0] = 0;
@@ -528,10 +548,10 @@ extern "C" DV_API int dv_hex_trilinear(const int32_t *nef, int32_t *rowptr, int3
             for (int32_t j = 0; j < ny; ++j)
                 for (int32_t i = 1; i < nx; ++i)
                     for (int d = 0; d < 3; ++d) {
-                        int ni = (i & 1) ? 2 : 1, nj = (j & 1) ? 2 : 1, nk = (k & 1) ? 2 : 1;
-                        int32_t ci[2] = {i / 2, i / 2 + 1}, cj[2] = {j / 2, j / 2 + 1}, ck[2] = {k / 2, k / 2 + 1};
-                        double wi[2] = {ni == 2 ? 0.5 : 1.0, 0.5}, wj[2] = {nj == 2 ? 0.5 : 1.0, 0.5},
-                               wk[2] = {nk == 2 ? 0.5 : 1.0, 0.5};
+                        int32_t ci[2], cj[2], ck[2];
+                        double wi[2], wj[2], wk[2];
+                        const int ni = coarse_1d(i, nef[0], ci, wi), nj = coarse_1d(j, nef[1], cj, wj),
+                                  nk = coarse_1d(k, nef[2], ck, wk);
                         for (int c = 0; c < nk; ++c)
                             for (int b = 0; b < nj; ++b)
                                 for (int a = 0; a < ni; ++a) {
@@ -543,6 +563,111 @@ extern "C" DV_API int dv_hex_trilinear(const int32_t *nef, int32_t *rowptr, int3
                         rowptr[++r] = (int32_t)p;
                     }
         DV_REQUIRE(p == nnz && r == nr, DV_ERR_ARG, "internal size mismatch");
+    });
+}
+
+// ---------------------------------------------------------------------------
+// Galerkin coarse operator P^T A P (sorted rows).  Row I of the result sums,
+// in order, over the entries (r, I) of P, the entries (r, j) of A and the
+// entries (j, J) of P, each term ((P_rI A_rj) P_jJ).
+// ---------------------------------------------------------------------------
+void dv_csr_transpose(const dv_csr_host &a, std::vector<int32_t> &rp, std::vector<int32_t> &ci, std::vector<double> &va) {
+    const int64_t nnz = a.rowptr[a.n_rows];
+    rp.assign((size_t)a.n_cols + 1, 0);
+    ci.resize(nnz);
+    va.resize(nnz);
+    for (int64_t k = 0; k < nnz; ++k) rp[a.col[k] + 1]++;
+    for (int32_t i = 0; i < a.n_cols; ++i) rp[i + 1] += rp[i];
+    std::vector<int32_t> fill(rp.begin(), rp.end() - 1);
+    for (int32_t r = 0; r < a.n_rows; ++r)
+        for (int32_t k = a.rowptr[r]; k < a.rowptr[r + 1]; ++k) {
+            const int32_t c = a.col[k];
+            ci[fill[c]] = r;
+            va[fill[c]] = a.val[k];
+            fill[c]++;
+        }
+}
+
+static void galerkin_rows(const dv_csr_host &A, const dv_csr_host &P, const std::vector<int32_t> &tp,
+                          const std::vector<int32_t> &tc, const std::vector<double> &tv, int32_t *count,
+                          const int32_t *rowptr, int32_t *col, double *val) {
+    const int32_t nc = P.n_cols;
+#pragma omp parallel
+    {
+        std::vector<double> acc(nc, 0.0);
+        std::vector<char> mark(nc, 0);
+        std::vector<int32_t> cols;
+#pragma omp for schedule(dynamic, 64)
+        for (int32_t I = 0; I < nc; ++I) {
+            cols.clear();
+            for (int32_t k = tp[I]; k < tp[I + 1]; ++k) {
+                const int32_t r = tc[k];
+                const double pr = tv[k];
+                for (int32_t q = A.rowptr[r]; q < A.rowptr[r + 1]; ++q) {
+                    const int32_t j = A.col[q];
+                    const double ar = pr * A.val[q];
+                    for (int32_t s = P.rowptr[j]; s < P.rowptr[j + 1]; ++s) {
+                        const int32_t J = P.col[s];
+                        if (!mark[J]) {
+                            mark[J] = 1;
+                            acc[J] = 0.0;
+                            cols.push_back(J);
+                        }
+                        acc[J] += ar * P.val[s];
+                    }
+                }
+            }
+            std::sort(cols.begin(), cols.end());
+            if (count) count[I] = (int32_t)cols.size();
+            int64_t p = rowptr ? rowptr[I] : 0;
+            for (int32_t J : cols) {
+                if (col) {
+                    col[p] = J;
+                    val[p] = acc[J];
+                    ++p;
+                }
+                mark[J] = 0;
+            }
+        }
+    }
+}
+
+static void check_galerkin_args(const dv_csr_host *A, const dv_csr_host *P) {
+    DV_REQUIRE(A && P && A->rowptr && A->col && A->val && P->rowptr && P->col && P->val, DV_ERR_ARG, "null argument");
+    DV_REQUIRE(A->n_rows == A->n_cols && P->n_rows == A->n_rows && P->n_cols >= 1, DV_ERR_ARG,
+               "need square A and P with as many rows as A");
+}
+
+extern "C" DV_API int dv_galerkin_size(const dv_csr_host *A, const dv_csr_host *P, int32_t *n, int64_t *nnz) {
+    return dv_guard([&] {
+        check_galerkin_args(A, P);
+        DV_REQUIRE(n && nnz, DV_ERR_ARG, "null output");
+        std::vector<int32_t> tp, tc;
+        std::vector<double> tv;
+        dv_csr_transpose(*P, tp, tc, tv);
+        std::vector<int32_t> cnt(P->n_cols);
+        galerkin_rows(*A, *P, tp, tc, tv, cnt.data(), nullptr, nullptr, nullptr);
+        int64_t t = 0;
+        for (int32_t c : cnt) t += c;
+        DV_REQUIRE(t < INT32_MAX, DV_ERR_ARG, "coarse operator too large for int32 offsets");
+        *n = P->n_cols;
+        *nnz = t;
+    });
+}
+
+extern "C" DV_API int dv_galerkin(const dv_csr_host *A, const dv_csr_host *P, int32_t *rowptr, int32_t *col,
+                                  double *val) {
+    return dv_guard([&] {
+        check_galerkin_args(A, P);
+        DV_REQUIRE(rowptr && col && val, DV_ERR_ARG, "null output array");
+        std::vector<int32_t> tp, tc;
+        std::vector<double> tv;
+        dv_csr_transpose(*P, tp, tc, tv);
+        std::vector<int32_t> cnt(P->n_cols);
+        galerkin_rows(*A, *P, tp, tc, tv, cnt.data(), nullptr, nullptr, nullptr);
+        rowptr[0] = 0;
+        for (int32_t i = 0; i < P->n_cols; ++i) rowptr[i + 1] = rowptr[i] + cnt[i];
+        galerkin_rows(*A, *P, tp, tc, tv, nullptr, rowptr, col, val);
     });
 }
 

@@ -180,6 +180,8 @@ void dv_encode_duvi(const dv_csr_host &a, double tol, int force_bits, DuviHost &
 void dv_make_bundles(const DuviHost &h, int32_t n_rows, int vi_bits, std::vector<int32_t> &bundles);
 void dv_build_duvi_lanes(const DuviHost &h, int32_t n_rows, DuviLanesHost &out);
 void dv_extract_diag(const dv_csr_host &a, std::vector<double> &diag);
+// CSR transpose (rows sorted by column of the input).
+void dv_csr_transpose(const dv_csr_host &a, std::vector<int32_t> &rp, std::vector<int32_t> &ci, std::vector<double> &va);
 // 3 or 2 when every run of that many consecutive rows has one column list, else 1.
 int dv_csr_row_group(const dv_csr_host &a);
 // Row-ratio bound max_i sum_j |a_ij| / max_j |a_ij| (GeometricMultigridSolver.cs:144-151).

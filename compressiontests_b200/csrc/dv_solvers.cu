@@ -398,24 +398,6 @@ extern "C" DV_API int dv_pcg_destroy(dv_pcg *s) {
 // ---------------------------------------------------------------------------
 // multigrid-preconditioned flexible CG
 // ---------------------------------------------------------------------------
-// CSR transpose on the host (restriction = P^T).
-static void csr_transpose(const dv_csr_host &a, std::vector<int32_t> &rp, std::vector<int32_t> &ci, std::vector<double> &va) {
-    int64_t nnz = a.rowptr[a.n_rows];
-    rp.assign(a.n_cols + 1, 0);
-    ci.resize(nnz);
-    va.resize(nnz);
-    for (int64_t k = 0; k < nnz; ++k) rp[a.col[k] + 1]++;
-    for (int32_t i = 0; i < a.n_cols; ++i) rp[i + 1] += rp[i];
-    std::vector<int32_t> fill(rp.begin(), rp.end() - 1);
-    for (int32_t r = 0; r < a.n_rows; ++r)
-        for (int32_t k = a.rowptr[r]; k < a.rowptr[r + 1]; ++k) {
-            int32_t c = a.col[k];
-            ci[fill[c]] = r;
-            va[fill[c]] = a.val[k];
-            fill[c]++;
-        }
-}
-
 template <class T>
 static std::unique_ptr<VCycle<T>> build_vcycle(dv_context *ctx, SolverWs &ws, int32_t L, const dv_csr_host *A,
                                                const dv_csr_host *P, const dv_mgpcg_config &cfg,
@@ -436,7 +418,7 @@ static std::unique_ptr<VCycle<T>> build_vcycle(dv_context *ctx, SolverWs &ws, in
         lv.P.reset(dv_matrix_build(ctx, P[l], cfg.format, prec, 0, 1e-10));
         std::vector<int32_t> rp, ci;
         std::vector<double> va;
-        csr_transpose(P[l], rp, ci, va);
+        dv_csr_transpose(P[l], rp, ci, va);
         dv_csr_host rt{P[l].n_cols, P[l].n_rows, rp.data(), ci.data(), va.data()};
         lv.R.reset(dv_matrix_build(ctx, rt, cfg.format, prec, 0, 1e-10));
         for (double d : lv.A->host_diag) DV_REQUIRE(d != 0.0, DV_ERR_SINGULAR, "zero diagonal entry");

@@ -312,3 +312,83 @@ class MultigridPcgSolver:
             self.release()
         except Exception:
             pass
+
+
+class BatchedMultigridSolver:
+    """Many independent meshes solved together (block-diagonal levels, one launch per
+    operation for all meshes, CUDA-graph-captured iterations).
+
+    meshes: list of (A_levels, P_levels), each as accepted by MultigridPcgSolver; the
+    meshes may have different sizes and depths.  Every mesh's coarsest level is solved
+    with a dense inverse.  Solve takes and returns one vector per mesh.
+    """
+
+    def __init__(self, context: CudaContext, meshes, precision="mixed", fmt="duvi", outer_fmt=None, nu=2,
+                 omega=2.0 / 3.0, omega_mode="spectral", tol=1e-8, max_iterations=500, iterations_per_sync=4,
+                 use_graphs=True):
+        self.context = context
+        f = {"csr": N.FORMAT_CSR, "duvi": N.FORMAT_DUVI}
+        cfg = N.MgpcgConfig({"mixed": N.MIXED, "f64": N.F64}[precision], f[fmt], f[outer_fmt or fmt], nu, omega,
+                            {"absolute": N.OMEGA_ABSOLUTE, "spectral": N.OMEGA_SPECTRAL}[omega_mode], max_iterations,
+                            tol, iterations_per_sync, 1 if use_graphs else 0)
+        nm = len(meshes)
+        nlev = np.array([len(a) for a, _ in meshes], np.int32)
+        keep, a_arrs, p_arrs = [], (C.c_void_p * nm)(), (C.c_void_p * nm)()
+        for m, (A, P) in enumerate(meshes):
+            if len(P) != len(A) - 1:
+                raise ValueError(f"mesh {m}: need len(P) == len(A) - 1")
+            ah, ka = _hosts(A)
+            ph, kp = _hosts(P)
+            keep += [ah, ka, ph, kp]
+            a_arrs[m] = C.cast(ah, C.c_void_p)
+            p_arrs[m] = C.cast(ph, C.c_void_p)
+        h = C.c_void_p()
+        N.check(N.lib().dv_batch_create(context.h, nm, N.ptr(nlev), a_arrs, p_arrs, C.byref(cfg), C.byref(h)))
+        del keep
+        self.h = h
+        context.register(self)
+        self.sizes = [A[0].shape[0] for A, _ in meshes]
+        self.offsets = np.concatenate([[0], np.cumsum(self.sizes)]).astype(np.int64)
+        self.n = int(self.offsets[-1])
+
+    def info(self):
+        n, L, k = C.c_int32(), C.c_int32(), C.c_int32()
+        N.check(N.lib().dv_batch_info(self.h, C.byref(n), C.byref(L), C.byref(k)))
+        return {"n_rows": n.value, "n_levels_max": L.value, "launches_per_chunk": k.value}
+
+    def omega(self, level):
+        w = C.c_double()
+        N.check(N.lib().dv_batch_omega(self.h, level, C.byref(w)))
+        return w.value
+
+    def Solve(self, rhs):
+        """rhs: list of per-mesh vectors (or one concatenated vector).  Returns
+        (list of solutions, stats, converged per mesh, iterations per mesh)."""
+        b = np.ascontiguousarray(np.concatenate(rhs) if isinstance(rhs, (list, tuple)) else rhs, np.float64)
+        if b.shape != (self.n,):
+            raise ValueError(f"rhs must hold {self.n} values")
+        x = np.empty_like(b)
+        nm = len(self.sizes)
+        conv, its = np.zeros(nm, np.int32), np.zeros(nm, np.int32)
+        st = N.Stats()
+        N.check(N.lib().dv_batch_solve(self.h, N.ptr(b), N.ptr(x), N.ptr(conv), N.ptr(its), C.byref(st)))
+        xs = [x[self.offsets[m]:self.offsets[m + 1]] for m in range(nm)]
+        return xs, _stats(st, "worst relative residual"), conv.astype(bool), its
+
+    def solve_device(self, b_ptr, x_ptr):
+        nm = len(self.sizes)
+        conv, its = np.zeros(nm, np.int32), np.zeros(nm, np.int32)
+        st = N.Stats()
+        N.check(N.lib().dv_batch_solve_device(self.h, b_ptr, x_ptr, N.ptr(conv), N.ptr(its), C.byref(st)))
+        return _stats(st, "worst relative residual"), conv.astype(bool), its
+
+    def release(self):
+        if getattr(self, "h", None) is not None:
+            N.lib().dv_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass

@@ -64,6 +64,7 @@ typedef struct dv_matrix dv_matrix;
 typedef struct dv_gmg dv_gmg;
 typedef struct dv_pcg dv_pcg;
 typedef struct dv_mgpcg dv_mgpcg;
+typedef struct dv_batch dv_batch;
 
 /* Host CSR view (int32 indices, float64 values; columns sorted per row). */
 typedef struct {
@@ -246,6 +247,32 @@ DV_API int dv_mgpcg_solve_multi_device(dv_mgpcg *s, int32_t k, const double *d_B
                                        int32_t *converged_per_rhs, dv_stats *stats);
 DV_API int dv_mgpcg_destroy(dv_mgpcg *s);
 
+/* ---- batched MG-PCG over many independent meshes ------------------------
+ * n_meshes systems, mesh m with n_levels[m] levels: A[m][0..n_levels[m]-1]
+ * (square, finest first) and P[m][0..n_levels[m]-2] (prolongation from level
+ * l+1 to l; restriction is its transpose).  Every mesh's coarsest level is
+ * solved with a dense inverse (at most 16384 dofs).  Per level the operators
+ * of all meshes are concatenated block-diagonally, so each smoothing sweep,
+ * transfer and outer product is one launch for all meshes, and the iteration
+ * sequence is captured in one CUDA graph.  cfg as for dv_mgpcg (mixed: FP32
+ * V-cycles inside the FP64 flexible CG).  Each mesh stops at its own
+ * ||r_m|| <= tol ||b_m|| (FP64-verified).  The reference builds one solver per
+ * model (GeometricMultigridSolver.Initialize, GeometricMultigridSolver.cs:57-77). */
+DV_API int dv_batch_create(dv_context *ctx, int32_t n_meshes, const int32_t *n_levels, const dv_csr_host *const *A,
+                           const dv_csr_host *const *P, const dv_mgpcg_config *cfg, dv_batch **out);
+/* Total fine rows, levels of the deepest mesh, kernel launches per captured chunk (0 before the first solve). */
+DV_API int dv_batch_info(const dv_batch *b, int32_t *n_rows, int32_t *n_levels_max, int32_t *n_launches_per_chunk);
+/* Effective Jacobi weight of batch level l (one weight for all meshes smoothing on that level). */
+DV_API int dv_batch_omega(const dv_batch *b, int32_t level, double *omega_eff);
+/* rhs and x: the meshes' fine-level vectors concatenated in mesh order (host
+ * arrays, FP64).  converged_per_mesh / iterations_per_mesh: optional, n_meshes entries. */
+DV_API int dv_batch_solve(dv_batch *b, const double *rhs, double *x, int32_t *converged_per_mesh,
+                          int32_t *iterations_per_mesh, dv_stats *stats);
+/* Same with device-resident rhs and x, context stream. */
+DV_API int dv_batch_solve_device(dv_batch *b, const double *d_rhs, double *d_x, int32_t *converged_per_mesh,
+                                 int32_t *iterations_per_mesh, dv_stats *stats);
+DV_API int dv_batch_destroy(dv_batch *b);
+
 /* ---- structured hex workload generator (FemCantilever3D on unit cubes) ----
  * Free dofs: all nodes with x index > 0 (FemCantileverBase.cs:137-158), node
  * ids x-fastest, VTK hexa corner order.  Entry (i,j) = sum over elements in
@@ -254,9 +281,17 @@ DV_API int dv_mgpcg_destroy(dv_mgpcg *s);
 DV_API int dv_hex_csr_size(const int32_t *ne, int32_t *n_rows, int64_t *nnz);
 DV_API int dv_hex_assemble(const int32_t *ne, const double *elem_E, double scale, double E, double nu,
                            int32_t *rowptr, int32_t *col, double *val);
-/* Trilinear prolongation between factor-2 grids (fine free x coarse free). */
+/* Trilinear prolongation of the factor-2 vertex coarsening (fine free x coarse
+ * free).  Per axis with n elements the coarse nodes are the even fine nodes
+ * and the last one, so odd n coarsens to (n+1)/2 elements (the last of length
+ * 1); for even n this is the standard trilinear interpolation. */
 DV_API int dv_hex_trilinear_size(const int32_t *ne_fine, int32_t *n_rows, int32_t *n_cols, int64_t *nnz);
 DV_API int dv_hex_trilinear(const int32_t *ne_fine, int32_t *rowptr, int32_t *col, double *val);
+/* Galerkin coarse operator P^T A P (square A, P with as many rows as A),
+ * sorted rows; row I sums over the entries (r, I) of P, then (r, j) of A,
+ * then (j, J) of P in storage order.  Size query, then fill. */
+DV_API int dv_galerkin_size(const dv_csr_host *A, const dv_csr_host *P, int32_t *n, int64_t *nnz);
+DV_API int dv_galerkin(const dv_csr_host *A, const dv_csr_host *P, int32_t *rowptr, int32_t *col, double *val);
 
 /* Restriction and interpolation between two structured Cartesian meshes
  * (IGeometricMultigridModel.CreateRestrictionAndInterpolationMatrix,

@@ -465,9 +465,27 @@ extern "C" or_csr *or_hex_stiffness(const int32_t *ne, const double *elem_E, dou
 }
 
 // Trilinear interpolation (fine free dofs x coarse free dofs) for factor-2 grids.
+// Trilinear prolongation of a factor-2 vertex coarsening (free dofs of the
+// clamped cantilever, x-fastest nodes, 3 dofs per node).  Per axis with n
+// elements the coarse nodes are the even fine nodes plus the last fine node;
+// an odd fine node between two coarse nodes takes 1/2 of each, every other
+// fine node coincides with one coarse node.  Even n: the standard trilinear P.
+static int or_coarse_axis(int32_t i, int32_t n, int32_t c[2], double w[2]) {
+    if ((i % 2 == 1) && i != n) {
+        c[0] = (i - 1) / 2;
+        c[1] = (i + 1) / 2;
+        w[0] = 0.5;
+        w[1] = 0.5;
+        return 2;
+    }
+    c[0] = (i == n) ? (n + 1) / 2 : i / 2;
+    w[0] = 1.0;
+    return 1;
+}
+
 extern "C" or_csr *or_hex_trilinear(const int32_t *nef) {
     int32_t nx = nef[0] + 1, ny = nef[1] + 1, nz = nef[2] + 1;
-    int32_t cx = nef[0] / 2 + 1, cy = nef[1] / 2 + 1, cz = nef[2] / 2 + 1;
+    int32_t cx = (nef[0] + 1) / 2 + 1, cy = (nef[1] + 1) / 2 + 1, cz = (nef[2] + 1) / 2 + 1;
     int32_t nf = 3 * (nx - 1) * ny * nz, nc = 3 * (cx - 1) * cy * cz;
     or_csr *P = new or_csr;
     P->n_rows = nf; P->n_cols = nc;
@@ -478,10 +496,9 @@ extern "C" or_csr *or_hex_trilinear(const int32_t *nef) {
                 for (int d = 0; d < 3; ++d) {
                     int32_t ci[2], cj[2], ck[2];
                     double wi[2], wj[2], wk[2];
-                    int ni = (i & 1) ? 2 : 1, nj = (j & 1) ? 2 : 1, nk = (k & 1) ? 2 : 1;
-                    ci[0] = i / 2; ci[1] = i / 2 + 1; wi[0] = ni == 2 ? 0.5 : 1.0; wi[1] = 0.5;
-                    cj[0] = j / 2; cj[1] = j / 2 + 1; wj[0] = nj == 2 ? 0.5 : 1.0; wj[1] = 0.5;
-                    ck[0] = k / 2; ck[1] = k / 2 + 1; wk[0] = nk == 2 ? 0.5 : 1.0; wk[1] = 0.5;
+                    int ni = or_coarse_axis(i, nef[0], ci, wi);
+                    int nj = or_coarse_axis(j, nef[1], cj, wj);
+                    int nk = or_coarse_axis(k, nef[2], ck, wk);
                     // columns sorted: k outer, j, i inner
                     for (int c = 0; c < nk; ++c)
                         for (int b = 0; b < nj; ++b)

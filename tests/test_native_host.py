@@ -65,7 +65,7 @@ def test_hex_assembly_with_moduli_bit_exact(native, oracle, rng):
     np.testing.assert_array_equal(A.data, M[2])
 
 
-@pytest.mark.parametrize("ne", [(4, 4, 4), (8, 4, 2)])
+@pytest.mark.parametrize("ne", [(4, 4, 4), (8, 4, 2), (5, 3, 4), (7, 9, 1)])
 def test_trilinear_bit_exact(native, oracle, ne):
     P = native.hex_trilinear(ne)
     Q = oracle.hex_trilinear(ne).arrays()
@@ -112,3 +112,33 @@ def test_hierarchy_shapes(native):
 def test_make_path_matches_oracle(native, oracle):
     for ld in ([1, 1, 0, 0], [1, 1, 0], [1, 0, 1, 0], [1, 1, 1, 0, 0, 0]):
         assert native.make_path(ld) == oracle.make_path(ld)
+
+
+@pytest.mark.parametrize("ne", [(4, 4, 4), (5, 3, 4), (7, 9, 5)])
+def test_galerkin_bit_exact(native, oracle, ne):
+    # P^T A P summed in the oracle's order (entries of P^T, then A, then P)
+    A = native.hex_stiffness(ne)
+    P = native.hex_trilinear(ne)
+    G = native.galerkin(A, P)
+    H = oracle.galerkin(oracle.Csr.from_scipy(A), oracle.hex_trilinear(ne)).arrays()
+    np.testing.assert_array_equal(G.indptr, H[0])
+    np.testing.assert_array_equal(G.indices, H[1])
+    np.testing.assert_array_equal(G.data, H[2])
+
+
+def test_galerkin_hierarchy_odd_sizes(native):
+    A, P = native.galerkin_hierarchy((37, 11, 23), max_coarse_dofs=1000)
+    assert [a.shape[0] for a in A] == [31968, 5187, 840]
+    for l, p in enumerate(P):
+        assert p.shape == (A[l].shape[0], A[l + 1].shape[0])
+        d = A[l + 1] - (p.T @ A[l] @ p)
+        assert abs(d).max() <= 1e-12 * abs(A[l + 1]).max()
+        assert abs(A[l + 1] - A[l + 1].T).max() <= 1e-12 * abs(A[l + 1]).max()
+
+
+def test_cantilever_batch_is_seeded(native):
+    d1, m1, r1 = native.cantilever_batch(4, seed=7)
+    d2, m2, r2 = native.cantilever_batch(4, seed=7)
+    assert d1 == d2 and all(8 <= v <= 48 for d in d1 for v in d)
+    assert all(np.array_equal(a, b) for a, b in zip(r1, r2))
+    assert [m[0][0].shape[0] for m in m1] == [3 * d[0] * (d[1] + 1) * (d[2] + 1) for d in d1]

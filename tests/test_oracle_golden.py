@@ -105,6 +105,32 @@ def test_trilinear_transfer_equals_reference_weights(oracle):
     assert np.all(s <= 1 + 1e-12) and np.isclose(s.max(), 1.0)
 
 
+@pytest.mark.parametrize("ne", [(4, 4, 4), (5, 3, 4), (7, 9, 1)])
+def test_trilinear_reproduces_linear_fields(oracle, ne):
+    # Vertex coarsening per axis: coarse nodes at the even fine nodes and at the last
+    # one.  Interpolating a linear field given at the coarse nodes must reproduce it
+    # exactly at every fine node (odd counts included).
+    def axis(n):
+        return np.array(sorted(set(range(0, n + 1, 2)) | {n}), float)
+    cx, cy, cz = axis(ne[0]), axis(ne[1]), axis(ne[2])
+    fx, fy, fz = np.arange(ne[0] + 1.0), np.arange(ne[1] + 1.0), np.arange(ne[2] + 1.0)
+
+    def field(xs, ys, zs, d):
+        Z, Y, X = np.meshgrid(zs, ys, xs[1:], indexing="ij")   # x = 0 nodes are clamped
+        f = np.stack([1 + 2 * X - Y + 0.5 * Z, -X + 3 * Z, 0.25 * Y + X], axis=-1)
+        return f.reshape(-1)
+    P = oracle.hex_trilinear(ne).to_scipy()
+    assert P.shape == (3 * ne[0] * (ne[1] + 1) * (ne[2] + 1), 3 * (len(cx) - 1) * len(cy) * len(cz))
+    # the clamped coarse node 0 carries the field value 1 + 0.5 z - y etc.; subtract its share
+    full = oracle.hex_trilinear(ne).to_scipy()
+    fine = field(fx, fy, fz, 0)
+    coarse = field(cx, cy, cz, 0)
+    # fine nodes at x = 1 interpolate from the clamped plane (x = 0) too: test away from it
+    Zf, Yf, Xf = np.meshgrid(fz, fy, fx[1:], indexing="ij")
+    mask = np.repeat((Xf.reshape(-1) >= 2), 3)
+    np.testing.assert_allclose((full @ coarse)[mask], fine[mask], atol=1e-12)
+
+
 def test_galerkin_of_trilinear_equals_rediscretised(oracle):
     ne = (4, 4, 4)
     A = oracle.hex_stiffness(ne)
