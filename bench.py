@@ -56,6 +56,8 @@ def parse():
     p.add_argument("--no-batched", action="store_true", help="skip the multi-load-case section")
     p.add_argument("--batched-only", action="store_true",
                    help="only the multi-load-case MG-PCG (64 load cases on the 64^3 mesh)")
+    p.add_argument("--adjoint-only", action="store_true", help="only the adjoint section (96x48x48)")
+    p.add_argument("--no-adjoint", action="store_true", help="skip the adjoint section")
     p.add_argument("--batch-size", type=int, default=64, help="mesh edge of the multi-load-case section")
     p.add_argument("--batch-k", type=int, default=64, help="load cases of the multi-load-case section")
     p.add_argument("--batch-meshes", type=int, default=32, help="meshes of the batched-mesh section")
@@ -375,6 +377,10 @@ def run_ours(args):
                                                    max(1, args.steps // 2), args.tol),
                    "meshes": batched_meshes(cb, ctx, stream, args.batch_meshes, max(1, args.steps // 2), args.tol)}
 
+    adjoint = None
+    if not args.no_adjoint:
+        adjoint = adjoint_section(cb, ctx, stream, max(1, args.steps // 2), 1e-10)
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         try:
@@ -399,7 +405,7 @@ def run_ours(args):
             "iterations": its_mixed[-1], "relative_residual_fp64": true_rel,
             "e2e": {"value": round(ms_e2e, 3), "unit": "ms", "h2d_bytes_per_step": int(8 * nf),
                     "d2h_bytes_per_step": int(8 * nf)},
-            "gpu_launches": int(launches), "fp64": fp64, "spmv": spmv, "batched": batched, "roofline": roof,
+            "gpu_launches": int(launches), "fp64": fp64, "spmv": spmv, "batched": batched, "adjoint": adjoint, "roofline": roof,
             "cpu_baseline": cpu,
             "clocks": clocks, "setup_s": {"hierarchy": round(t_build, 1), "solver": round(t_setup, 1)},
         }
@@ -514,6 +520,64 @@ def batched_meshes(cb, ctx, stream, n_meshes, steps, tol):
             "setup_s": {"hierarchies": round(t_build, 1), "solver": round(t_setup, 1)}}
 
 
+def adjoint_section(cb, ctx, stream, steps, tol):
+    """96 x 48 x 48 cantilever, rho ~ U[0.01, 1] (seeded), E = rho^3, unit traction, J = c^T u
+    with c ~ N(0, 1): forward solve, adjoint solve + element gradient kernel, FP64 and mixed."""
+    import torch
+    ne = (96, 48, 48)
+    rng = np.random.default_rng(20261203)
+    rho = rng.uniform(0.01, 1.0, int(np.prod(ne)))
+    f = cb.traction_rhs(ne)
+    c = rng.standard_normal(f.shape[0])
+    out = {"workload": "adjoint dJ/drho, 96x48x48 hex cantilever, rho~U[0.01,1] seeded, E=rho^3, unit traction, "
+                       f"J=c^T u (c~N(0,1)), Galerkin hierarchy to <= 2000 dofs, tol {tol:g}",
+           "n_elements": int(rho.size), "n_dofs": int(f.shape[0])}
+    grads = {}
+    for prec in ("mixed", "f64"):
+        t = time.time()
+        prob = cb.AdjointCantilever(ctx, ne, rho, max_coarse_dofs=2000, precision=prec, tol=tol, max_iterations=2000)
+        t_setup = time.time() - t
+        prob.forward(f)
+        prob.backward(c)
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        fw = bw = 0.0
+        for _ in range(steps):
+            e0.record(stream)
+            u, st_f = prob.forward(f)
+            e1.record(stream)
+            g, st_b = prob.backward(c)
+            e2.record(stream)
+            e2.synchronize()
+            fw += e0.elapsed_time(e1)
+            bw += e1.elapsed_time(e2)
+        grads[prec] = g
+        out[prec] = {"forward_ms": round(fw / steps, 3), "backward_ms": round(bw / steps, 3),
+                     "forward_iterations": int(st_f.NumIterationsRequired),
+                     "adjoint_iterations": int(st_b.NumIterationsRequired),
+                     "forward_rel_residual": float(st_f.RelativeResidual),
+                     "adjoint_rel_residual": float(st_b.RelativeResidual), "setup_s": round(t_setup, 1)}
+        prob.release()
+    out["mixed_vs_f64_gradient_max_rel"] = float(np.max(np.abs(grads["mixed"] - grads["f64"])) /
+                                                 np.max(np.abs(grads["f64"])))
+    # the element kernel alone
+    d = [torch.from_numpy(v).cuda() for v in (rho, u, u)]
+    gd = torch.zeros(rho.size, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    fn = lambda: cb.element_gradient_device(ctx, ne, d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(), gd.data_ptr())
+    fn()
+    out["element_kernel_ms_incl_sync"] = round(time_events(stream, fn, 10), 4)
+    return out
+
+
+def run_adjoint_only(args):
+    import torch
+    import compressiontests_b200 as cb
+    ctx = cb.CudaContext(0)
+    r = adjoint_section(cb, ctx, torch.cuda.ExternalStream(ctx.stream), args.steps, 1e-10)
+    print(json.dumps({"adjoint": r}), flush=True)
+    ctx.close()
+
+
 def run_batched_only(args):
     import torch
     import compressiontests_b200 as cb
@@ -557,6 +621,8 @@ if __name__ == "__main__":
         run_spmv_only(a)
     elif a.batched_only:
         run_batched_only(a)
+    elif a.adjoint_only:
+        run_adjoint_only(a)
     elif a.impl == "reference":
         run_reference(a)
     else:

@@ -125,6 +125,13 @@ _SIGNATURES = {
     "dv_batch_solve": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _P(Stats)]),
     "dv_batch_solve_device": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _P(Stats)]),
     "dv_batch_destroy": (C.c_int, [_vp]),
+    "dv_adjoint_create": (C.c_int, [_vp, _vp, _vp, C.c_double, C.c_double, C.c_double, C.c_int32, _P(MgpcgConfig),
+                                    _P(_vp)]),
+    "dv_adjoint_info": (C.c_int, [_vp, _P(C.c_int32), _P(C.c_int64)]),
+    "dv_adjoint_forward": (C.c_int, [_vp, _vp, _vp, _P(Stats)]),
+    "dv_adjoint_backward": (C.c_int, [_vp, _vp, _vp, _vp, _P(Stats)]),
+    "dv_adjoint_destroy": (C.c_int, [_vp]),
+    "dv_hex_element_gradient": (C.c_int, [_vp, _vp, _vp, C.c_double, C.c_double, C.c_double, _vp, _vp, _vp]),
     "dv_hex_csr_size": (C.c_int, [_vp, _P(C.c_int32), _P(C.c_int64)]),
     "dv_hex_assemble": (C.c_int, [_vp, _vp, C.c_double, C.c_double, C.c_double, _vp, _vp, _vp]),
     "dv_hex_trilinear_size": (C.c_int, [_vp, _P(C.c_int32), _P(C.c_int32), _P(C.c_int64)]),

@@ -401,6 +401,8 @@ static void hex_ke(double E, double v, double *ke) {
                 }
 }
 
+void dv_hex_ke(double E, double nu, double *ke) { hex_ke(E, nu, ke); }
+
 static inline int32_t hex_row_nodes(int32_t i, int32_t j, int32_t k, int32_t nx, int32_t ny, int32_t nz) {
     int ci = (i > 1 ? 1 : 0) + 1 + (i + 1 < nx ? 1 : 0);   // x neighbours among free nodes (x index >= 1)
     int cj = (j > 0 ? 1 : 0) + 1 + (j + 1 < ny ? 1 : 0);

@@ -188,6 +188,8 @@ int dv_csr_row_group(const dv_csr_host &a);
 double dv_row_ratio_bound(const dv_csr_host &a);
 // Dense inverse of an SPD matrix via LDL^T (no pivoting); returns false on a tiny pivot.
 bool dv_dense_inverse(int32_t n, std::vector<double> &a, double pivot_tol);
+// 24 x 24 unit-cube hexahedron stiffness (row-major, local nodes in VTK hexa order, 3 dofs per node).
+void dv_hex_ke(double E, double nu, double *ke);
 // Greedy coloring of node blocks (bs consecutive rows) for multicolor Gauss-Seidel.
 int dv_block_coloring(const dv_csr_host &a, int bs, std::vector<int32_t> &color_of_block);
 // Level sets of the forward Gauss-Seidel dependency graph (row i depends on j < i).

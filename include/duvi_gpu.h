@@ -65,6 +65,7 @@ typedef struct dv_gmg dv_gmg;
 typedef struct dv_pcg dv_pcg;
 typedef struct dv_mgpcg dv_mgpcg;
 typedef struct dv_batch dv_batch;
+typedef struct dv_adjoint dv_adjoint;
 
 /* Host CSR view (int32 indices, float64 values; columns sorted per row). */
 typedef struct {
@@ -272,6 +273,31 @@ DV_API int dv_batch_solve(dv_batch *b, const double *rhs, double *x, int32_t *co
 DV_API int dv_batch_solve_device(dv_batch *b, const double *d_rhs, double *d_x, int32_t *converged_per_mesh,
                                  int32_t *iterations_per_mesh, dv_stats *stats);
 DV_API int dv_batch_destroy(dv_batch *b);
+
+/* ---- adjoint sensitivities of a density-parametrised cantilever -----------
+ * Unit-cube hexahedra on an ne[0] x ne[1] x ne[2] grid (x = 0 face clamped),
+ * element moduli E_e = E0 rho_e^penal.  Forward/Backward pair in the shape of
+ * an autograd function: forward u = K(rho)^-1 f; backward takes dJ/du, solves
+ * K lambda = dJ/du with the forward's solver (K is symmetric; no state of the
+ * forward iterations is kept) and returns dJ/drho_e = -lambda_e^T (dK_e/drho_e) u_e
+ * from an element kernel over the connectivity.  The reference has no adjoint
+ * path; the elements, dof numbering and load follow FemCantilever3D
+ * (FemCantileverBase.cs:87-158).  create builds K(rho) and a Galerkin
+ * hierarchy (vertex factor-2 coarsening, trilinear P) down to at most
+ * max_coarse_dofs dofs, then the MG-PCG solver of cfg. */
+DV_API int dv_adjoint_create(dv_context *ctx, const int32_t *ne, const double *rho, double penal, double E0, double nu,
+                             int32_t max_coarse_dofs, const dv_mgpcg_config *cfg, dv_adjoint **out);
+DV_API int dv_adjoint_info(const dv_adjoint *a, int32_t *n_dofs, int64_t *n_elements);
+/* u = K(rho)^-1 f (host arrays, free dofs); keeps u on the device for backward. */
+DV_API int dv_adjoint_forward(dv_adjoint *a, const double *f, double *u, dv_stats *stats);
+/* dJdrho (n_elements) from dJdu (free dofs); lambda optional (free dofs).
+ * DV_ERR_NOT_INITIALIZED before the first forward. */
+DV_API int dv_adjoint_backward(dv_adjoint *a, const double *dJdu, double *dJdrho, double *lambda, dv_stats *stats);
+DV_API int dv_adjoint_destroy(dv_adjoint *a);
+/* The element kernel alone (device pointers, context stream, synchronous):
+ * grad_e = -penal rho_e^(penal-1) lambda_e^T Ke(E0, nu) u_e. */
+DV_API int dv_hex_element_gradient(dv_context *ctx, const int32_t *ne, const double *d_rho, double penal, double E0,
+                                   double nu, const double *d_u, const double *d_lambda, double *d_grad);
 
 /* ---- structured hex workload generator (FemCantilever3D on unit cubes) ----
  * Free dofs: all nodes with x index > 0 (FemCantileverBase.cs:137-158), node
