@@ -16,8 +16,15 @@ weight 2/3 of the spectrally normalised operator, dense coarse solve.
   fp64        the plain FP64 path (CSR FP64 operators everywhere) for comparison
   spmv        isolated SpMV of the finest operator per format/precision, GB/s of
               the algorithmic bytes and the fraction of the measured HBM peak
-  roofline    the dominant kernel (DuVi FP32 row-bundle decode, the body of every
+  roofline    the dominant kernel (DuVi FP32 lane-kernel decode, the body of every
               fine-level smoothing sweep), timed with CUDA events on its stream
+  gauss_seidel  the same solve with V(2,2) forward Gauss-Seidel (multicolor; the
+              reference's row order), mixed precision
+  batched     64 load cases on 64^3 in one multi-right-hand-side solve, and 32
+              uneven cantilevers in one batched solve, each against the same
+              work done one solve at a time
+  adjoint     96x48x48, E = rho^3: forward solve, adjoint solve + dJ/drho kernel
+The comparison sections (fp64, gauss_seidel, batched, adjoint) run at N = 1 only.
 
 --impl reference times the CPU restatement of the reference's algorithm
 (oracle/, FP64, all host threads) on the same workload; each step is a
@@ -57,6 +64,7 @@ def parse():
     p.add_argument("--batched-only", action="store_true",
                    help="only the multi-load-case MG-PCG (64 load cases on the 64^3 mesh)")
     p.add_argument("--adjoint-only", action="store_true", help="only the adjoint section (96x48x48)")
+    p.add_argument("--no-gs", action="store_true", help="skip the Gauss-Seidel-smoothed MG-PCG lines")
     p.add_argument("--no-adjoint", action="store_true", help="skip the adjoint section")
     p.add_argument("--batch-size", type=int, default=64, help="mesh edge of the multi-load-case section")
     p.add_argument("--batch-k", type=int, default=64, help="load cases of the multi-load-case section")
@@ -180,13 +188,13 @@ def time_events(stream, fn, reps):
     return e0.elapsed_time(e1) / reps
 
 
-def spmv_table(cb, ctx, A0, reps, peak):
+def spmv_table(cb, ctx, A0, reps, peak, cases=(("duvi", "f32"), ("duvi", "f64"), ("csr", "f32"), ("csr", "f64"))):
     import torch
     stream = torch.cuda.ExternalStream(ctx.stream)
     out = {}
     n = A0.shape[0]
     dom = None
-    for fmt, prec in (("duvi", "f32"), ("duvi", "f64"), ("csr", "f32"), ("csr", "f64")):
+    for fmt, prec in cases:
         M = cb.SparseMatrix(ctx, A0, fmt, prec)
         info = M.info()
         dt = torch.float32 if prec == "f32" else torch.float64
@@ -211,6 +219,16 @@ def spmv_table(cb, ctx, A0, reps, peak):
         del x, y
         torch.cuda.empty_cache()
     return out, dom
+
+
+def spmv_log_uniform(cb, ctx, n, reps, peak):
+    """SpMV of the n^3 operator with per-element E = 10^U(-2, 0) (seeded): nearly every stored
+    value is distinct, so DuVi needs 32-bit value indices and a table as long as nnz."""
+    rng = np.random.default_rng(20261203)
+    E = 10.0 ** rng.uniform(-2.0, 0.0, n ** 3)
+    A0 = cb.hex_stiffness((n, n, n), E)
+    out, _ = spmv_table(cb, ctx, A0, reps, peak, (("duvi", "f64"), ("csr", "f64")))
+    return {"size": f"{n}^3", "elem_E": "10^U(-2,0) per element, seed 20261203", **out}
 
 
 def cpu_baseline_sample(A, P, b, iters_needed, threads):
@@ -348,7 +366,8 @@ def run_ours(args):
     mixed.release()
 
     fp64 = {}
-    if not args.no_fp64:
+    extras = ws == 1   # the comparison sections run at N = 1 only (replicas would repeat them per rank)
+    if not args.no_fp64 and extras:
         for fmt in ("csr", "duvi"):
             s = make("f64", fmt)
             ms, its, rel, _, _ = timed(s, max(2, args.steps // 2), 1)
@@ -356,7 +375,21 @@ def run_ours(args):
                          "mixed_speedup": round(ms / ms_mixed, 2)}
             s.release()
 
+    gauss_seidel = {}
+    if not args.no_gs and extras:
+        for smoother, prec in (("gs_color", "mixed"), ("gs_lex", "mixed")):
+            t = time.time()
+            s = cb.MultigridPcgSolver(ctx, A, P, precision=prec, fmt="duvi", outer_fmt="duvi", nu=2, tol=args.tol,
+                                      max_iterations=500, smoother=smoother)
+            t_gs = time.time() - t
+            ms, its, rel, _, _ = timed(s, 1, 1)
+            gauss_seidel[f"{smoother}_{prec}"] = {"ms": round(ms, 2), "iterations": its[-1], "rel_residual": rel[-1],
+                                                  "setup_s": round(t_gs, 1)}
+            s.release()
+
     spmv, dom = ({}, None) if args.no_spmv else spmv_table(cb, ctx, A[0], 20, peak)
+    if not args.no_spmv and extras:
+        spmv["log_uniform_E"] = spmv_log_uniform(cb, ctx, 64, 20, peak)
     roof = None
     if dom is not None:
         ms_dom, alg = dom
@@ -367,13 +400,13 @@ def run_ours(args):
                 "algorithmic_bytes_per_launch": int(alg), "avg_launch_ms": round(ms_dom, 4)}
 
     batched = None
-    if not args.no_batched:
+    if not args.no_batched and extras:
         batched = {"load_cases": batched_multi_rhs(cb, ctx, stream, args.batch_size, args.batch_k,
                                                    max(1, args.steps // 2), args.tol),
                    "meshes": batched_meshes(cb, ctx, stream, args.batch_meshes, max(1, args.steps // 2), args.tol)}
 
     adjoint = None
-    if not args.no_adjoint:
+    if not args.no_adjoint and extras:
         adjoint = adjoint_section(cb, ctx, stream, max(1, args.steps // 2), 1e-10)
 
     cpu = None
@@ -400,7 +433,7 @@ def run_ours(args):
             "iterations": its_mixed[-1], "relative_residual_fp64": true_rel,
             "e2e": {"value": round(ms_e2e, 3), "unit": "ms", "h2d_bytes_per_step": int(8 * nf),
                     "d2h_bytes_per_step": int(8 * nf)},
-            "gpu_launches": int(launches), "fp64": fp64, "spmv": spmv, "batched": batched, "adjoint": adjoint, "roofline": roof,
+            "gpu_launches": int(launches), "fp64": fp64, "spmv": spmv, "gauss_seidel": gauss_seidel, "batched": batched, "adjoint": adjoint, "roofline": roof,
             "cpu_baseline": cpu,
             "clocks": clocks, "setup_s": {"hierarchy": round(t_build, 1), "solver": round(t_setup, 1)},
         }

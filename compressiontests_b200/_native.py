@@ -79,7 +79,8 @@ class GmgConfig(C.Structure):
 class MgpcgConfig(C.Structure):
     _fields_ = [("precision", C.c_int32), ("format", C.c_int32), ("outer_format", C.c_int32), ("nu", C.c_int32),
                 ("omega", C.c_double), ("omega_mode", C.c_int32), ("max_iterations", C.c_int32),
-                ("tol", C.c_double), ("iterations_per_sync", C.c_int32), ("use_graphs", C.c_int32)]
+                ("tol", C.c_double), ("iterations_per_sync", C.c_int32), ("use_graphs", C.c_int32),
+                ("smoother", C.c_int32)]
 
 
 _vp = C.c_void_p

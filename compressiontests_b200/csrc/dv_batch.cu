@@ -605,6 +605,7 @@ extern "C" DV_API int dv_batch_create(dv_context *ctx, int32_t n_meshes, const i
         DV_REQUIRE(ctx && n_levels && A && P && cfg && out && n_meshes >= 1, DV_ERR_ARG, "null argument");
         DV_REQUIRE(cfg->precision == DV_F64 || cfg->precision == DV_MIXED, DV_ERR_ARG, "precision must be DV_F64 or DV_MIXED");
         DV_REQUIRE(cfg->nu >= 1 && cfg->max_iterations >= 1 && cfg->tol > 0, DV_ERR_ARG, "bad smoothing or stop parameters");
+        DV_REQUIRE(cfg->smoother == DV_SMOOTHER_JACOBI, DV_ERR_UNSUPPORTED, "batched meshes smooth with weighted Jacobi only");
         dv_ctx_check(ctx);
         for (int32_t m = 0; m < n_meshes; ++m) {
             DV_REQUIRE(n_levels[m] >= 1 && A[m] && (n_levels[m] == 1 || P[m]), DV_ERR_ARG, "mesh without levels");

@@ -12,6 +12,7 @@
 // "gauss_seidel_iteration" kernel (CsrGeometricMultigrid.cl:207-225) updates x
 // in place while other work-items read it, which is a data race; it is not
 // reproduced.
+#include "dv_gs.cuh"
 #include "dv_kernels.cuh"
 #include "dv_solvers.cuh"
 
@@ -28,79 +29,6 @@ static int grid_n(dv_context *ctx, int64_t n) {
 }
 
 // ---------------------------------------------------------------------------
-// Gauss-Seidel kernels
-// ---------------------------------------------------------------------------
-// Row update x_i = (b_i - sum_{j != i} a_ij x_j) / a_ii, column order, each
-// product and difference rounded separately.
-__device__ __forceinline__ void gs_row_csr(const int32_t *__restrict__ rp, const int32_t *__restrict__ ci,
-                                           const double *__restrict__ va, const double *__restrict__ b, double *x,
-                                           int32_t i) {
-    double s = b[i], d = 0.0;
-    for (int32_t k = rp[i]; k < rp[i + 1]; ++k) {
-        int32_t c = ci[k];
-        double a = va[k];
-        if (c != i) s = __dsub_rn(s, __dmul_rn(a, ((volatile double *)x)[c]));
-        else d = a;
-    }
-    x[i] = __ddiv_rn(s, d);
-}
-
-template <class VI>
-__device__ __forceinline__ void gs_row_duvi(const DuviArgs &A, const double *__restrict__ b, double *x, int32_t i) {
-    const double *tab = static_cast<const double *>(A.values);
-    const VI *vi = static_cast<const VI *>(A.vidx);
-    double s = b[i], d = 0.0;
-    uint32_t di = A.row_to_dist[i];
-    for (uint32_t bl = A.row_to_col[i]; bl < A.row_to_col[i + 1]; ++bl) {
-        uint32_t c = A.col_idx[bl];
-        int cnt = A.dist[di];
-        for (int k = 0;; ++k) {
-            double a = tab[vi[di]];
-            if ((int32_t)c != i) s = __dsub_rn(s, __dmul_rn(a, ((volatile double *)x)[c]));
-            else d = a;
-            ++di;
-            if (k == cnt) break;
-            c += A.dist[di] + 1u;
-        }
-    }
-    x[i] = __ddiv_rn(s, d);
-}
-
-// Rows rows[0..count) (one dependency level, or the rows of one color).
-__global__ void k_gs_csr(const int32_t *__restrict__ rp, const int32_t *__restrict__ ci, const double *__restrict__ va,
-                         const double *__restrict__ b, double *x, const int32_t *__restrict__ rows, int32_t count,
-                         int bs, const int *__restrict__ done) {
-    if (done && *(volatile const int *)done) return;
-    for (int32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < count; t += gridDim.x * blockDim.x) {
-        int32_t r0 = rows[t];
-        for (int q = 0; q < bs; ++q) gs_row_csr(rp, ci, va, b, x, r0 + q);
-    }
-}
-template <class VI>
-__global__ void k_gs_duvi(DuviArgs A, const double *__restrict__ b, double *x, const int32_t *__restrict__ rows,
-                          int32_t count, int bs, const int *__restrict__ done) {
-    if (done && *(volatile const int *)done) return;
-    for (int32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < count; t += gridDim.x * blockDim.x) {
-        int32_t r0 = rows[t];
-        for (int q = 0; q < bs; ++q) gs_row_duvi<VI>(A, b, x, r0 + q);
-    }
-}
-
-static DuviArgs duvi_args(const dv_matrix *m) {
-    DuviArgs a;
-    a.row_to_col = m->row_to_col.as<uint32_t>();
-    a.row_to_dist = m->row_to_dist.as<uint32_t>();
-    a.col_idx = m->col_idx.as<uint32_t>();
-    a.dist = m->dist.as<uint8_t>();
-    a.vidx = m->vidx.p;
-    a.values = m->values.p;
-    a.bundles = m->bundles.as<int32_t>();
-    a.nbundles = m->nbundles;
-    a.nuniq = (int32_t)m->nuniq;
-    return a;
-}
-
-// ---------------------------------------------------------------------------
 // solver object
 // ---------------------------------------------------------------------------
 struct GLevel {
@@ -108,10 +36,7 @@ struct GLevel {
     DevMem D, b, x, t, r;
     int32_t n = 0;
     double omega = 1.0;
-    // ordered row groups for Gauss-Seidel: rows (or block starts) and group offsets
-    DevMem gs_rows;
-    std::vector<int32_t> gs_off;
-    int gs_bs = 1;
+    GsOrder gs;   // Gauss-Seidel row groups (forward-sweep levels or colors)
 };
 
 struct dv_gmg {
@@ -146,28 +71,7 @@ static void smooth(dv_gmg *g, const LaunchEnv &e, GLevel &L, int sweeps) {
         }
         return;
     }
-    const int32_t ngroups = (int32_t)L.gs_off.size() - 1;
-    for (int k = 0; k < sweeps; ++k)
-        for (int32_t q = 0; q < ngroups; ++q) {
-            int32_t cnt = L.gs_off[q + 1] - L.gs_off[q];
-            const int32_t *rows = L.gs_rows.as<int32_t>() + L.gs_off[q];
-            int grid = grid_n(ctx, cnt);
-            if (L.A->format == DV_FORMAT_CSR) {
-                k_gs_csr<<<grid, kThreads, 0, s>>>(L.A->rowptr.as<int32_t>(), L.A->col.as<int32_t>(), L.A->val.as<double>(),
-                                                   L.b.as<double>(), L.x.as<double>(), rows, cnt, L.gs_bs, e.done);
-            } else if (L.A->vi_bits == 8) {
-                k_gs_duvi<uint8_t><<<grid, kThreads, 0, s>>>(duvi_args(L.A.get()), L.b.as<double>(), L.x.as<double>(), rows,
-                                                             cnt, L.gs_bs, e.done);
-            } else if (L.A->vi_bits == 16) {
-                k_gs_duvi<uint16_t><<<grid, kThreads, 0, s>>>(duvi_args(L.A.get()), L.b.as<double>(), L.x.as<double>(), rows,
-                                                              cnt, L.gs_bs, e.done);
-            } else {
-                k_gs_duvi<uint32_t><<<grid, kThreads, 0, s>>>(duvi_args(L.A.get()), L.b.as<double>(), L.x.as<double>(), rows,
-                                                              cnt, L.gs_bs, e.done);
-            }
-            DV_CUDA(cudaGetLastError());
-            ctx->count();
-        }
+    for (int k = 0; k < sweeps; ++k) gs_sweep<double>(e, L.A.get(), L.gs, L.b.as<double>(), L.x.as<double>());
 }
 
 // One V-cycle pass over the path (the step loop of Solve).
@@ -287,30 +191,7 @@ extern "C" DV_API int dv_gmg_create(dv_context *ctx, int32_t n_levels, const dv_
             }
             const size_t nb = 8 * (size_t)L.n;
             L.b.alloc(nb); L.x.alloc(nb); L.t.alloc(nb); L.r.alloc(nb); L.D.alloc(nb);
-            if (cfg->smoother == DV_SMOOTHER_GS_LEX) {
-                std::vector<int32_t> perm, off;
-                dv_gs_level_sets(A[l], perm, off);
-                L.gs_off = off;
-                L.gs_bs = 1;
-                L.gs_rows.alloc(4 * perm.size());
-                DV_CUDA(cudaMemcpyAsync(L.gs_rows.p, perm.data(), 4 * perm.size(), cudaMemcpyHostToDevice, s));
-                DV_CUDA(cudaStreamSynchronize(s));
-            } else if (cfg->smoother == DV_SMOOTHER_GS_COLOR) {
-                // node blocks of consecutive rows: 3 dofs per node when the size allows it
-                int bs = (L.n % 3 == 0) ? 3 : (L.n % 2 == 0 ? 2 : 1);
-                std::vector<int32_t> color;
-                int nc = dv_block_coloring(A[l], bs, color);
-                std::vector<int32_t> off(nc + 1, 0), rows(color.size());
-                for (int32_t c : color) off[c + 1]++;
-                for (int c = 0; c < nc; ++c) off[c + 1] += off[c];
-                std::vector<int32_t> fill(off.begin(), off.end() - 1);
-                for (size_t b = 0; b < color.size(); ++b) rows[fill[color[b]]++] = (int32_t)b * bs;
-                L.gs_off = off;
-                L.gs_bs = bs;
-                L.gs_rows.alloc(4 * rows.size());
-                DV_CUDA(cudaMemcpyAsync(L.gs_rows.p, rows.data(), 4 * rows.size(), cudaMemcpyHostToDevice, s));
-                DV_CUDA(cudaStreamSynchronize(s));
-            }
+            if (cfg->smoother != DV_SMOOTHER_JACOBI) gs_build_order(A[l], cfg->smoother == DV_SMOOTHER_GS_LEX, s, L.gs);
         }
         // relaxation (GeometricMultigridSolver.cs:209-214 / :109-121 / OpenCLCsrGeometricMultigridSolver.cs:164-171)
         if (cfg->coarse_relaxation) {

@@ -189,11 +189,16 @@ int dv_csr_row_group(const dv_csr_host &a) {
     return 1;
 }
 
-void dv_build_duvi_lanes(const DuviHost &h, int32_t n, DuviLanesHost &L) {
+// Entry bytes of the lane layout: 255 marks a block start (its column comes from
+// the block column list), any other value is gap - 1 (at most 254: blocks break
+// at gaps of 256).  With at most 256 / value_bytes distinct values, 8-bit value
+// indices are stored pre-multiplied by the value size, as byte offsets into the table.
+void dv_build_duvi_lanes(const DuviHost &h, int32_t n, int value_bytes, DuviLanesHost &L) {
     const int g = detect_group(h, n);
     const int vib = h.vi_bits / 8;            // bytes per value index
     const size_t chunk = 4 * (size_t)vib;     // bytes per chunk of 4 indices
     L.group = g;
+    L.scaled = (vib == 1 && (int64_t)h.values.size() * value_bytes <= 256) ? 1 : 0;
     L.ngroups = n / g;
     L.nbundles = (L.ngroups + 31) / 32;
     L.meta.assign(5 * L.nbundles, 0);
@@ -240,9 +245,15 @@ void dv_build_duvi_lanes(const DuviHost &h, int32_t n, DuviLanesHost &L) {
             if (gi >= L.ngroups) break;
             const int32_t r0 = (int32_t)(gi * g);
             const uint32_t d0 = h.row_to_dist[r0], ne = h.row_to_dist[r0 + 1] - d0;
+            uint32_t next_start = 0;
             for (uint32_t e = 0; e < ne; ++e) {
                 uint32_t w = e / 4, k = e % 4;
-                L.dist[dwords[bi] + (uint64_t)w * 32 + t] |= (uint32_t)h.dist[d0 + e] << (8 * k);
+                uint32_t byte = h.dist[d0 + e];
+                if (e == next_start) {
+                    next_start = e + byte + 1;   // the count byte of this block
+                    byte = 255u;
+                }
+                L.dist[dwords[bi] + (uint64_t)w * 32 + t] |= byte << (8 * k);
             }
             for (int d = 0; d < g; ++d) {
                 const uint32_t rd = h.row_to_dist[r0 + d];
@@ -250,6 +261,7 @@ void dv_build_duvi_lanes(const DuviHost &h, int32_t n, DuviLanesHost &L) {
                     uint32_t w = e / 4, k = e % 4;
                     uint64_t c = vchunks[bi] + ((uint64_t)w * g + d) * 32 + t;
                     uint32_t v = h.vidx[rd + e];
+                    if (L.scaled) v *= (uint32_t)value_bytes;
                     std::memcpy(&L.vi[c * chunk + k * vib], &v, vib);   // little-endian low bytes
                 }
             }

@@ -132,9 +132,10 @@ struct DuviHost {   // host copy of the SoA encoding (export / parity)
 // The canonical SoA stays on the device (export, Gauss-Seidel, SpMM).
 struct DuviLanesHost {
     int group = 1;
+    int scaled = 0;                // 1: value-index bytes hold index * value size (byte offsets into the table)
     int64_t ngroups = 0, nbundles = 0;
     std::vector<uint32_t> meta;    // per bundle: d_base, v_base, c_base, words, blocks
-    std::vector<uint32_t> dist;    // leader gap/count bytes, 4 per word
+    std::vector<uint32_t> dist;    // leader entry bytes, 4 per word: 255 at a block start, else gap - 1
     std::vector<uint8_t> vi;       // chunks of 4 value indices (4 * vi_bits / 8 bytes each)
     std::vector<uint32_t> cols;    // leader block column starts
     std::vector<uint32_t> nent;    // entries per leader row
@@ -158,6 +159,7 @@ struct dv_matrix {
     int duvi_batch = 4;        // entries per gather batch in the decode loop (9 when most blocks hold 9)
     int duvi_variant = 0;      // 0: shared-memory staged rows, 1: lane-interleaved groups (autotuned)
     int lanes_group = 1;
+    int lanes_scaled = 0;
     int64_t lanes_bundles = 0, lanes_groups = 0;
     DevMem lanes_meta, lanes_dist, lanes_vi, lanes_cols, lanes_nent;
     int64_t lanes_bytes = 0;   // bytes one product reads from the lane layout
@@ -178,7 +180,7 @@ constexpr int kBundleBlocks = 480;    // block column starts (+ alignment slack)
 // Host helpers (dv_host.cpp)
 void dv_encode_duvi(const dv_csr_host &a, double tol, int force_bits, DuviHost &out);
 void dv_make_bundles(const DuviHost &h, int32_t n_rows, int vi_bits, std::vector<int32_t> &bundles);
-void dv_build_duvi_lanes(const DuviHost &h, int32_t n_rows, DuviLanesHost &out);
+void dv_build_duvi_lanes(const DuviHost &h, int32_t n_rows, int value_bytes, DuviLanesHost &out);
 void dv_extract_diag(const dv_csr_host &a, std::vector<double> &diag);
 // CSR transpose (rows sorted by column of the input).
 void dv_csr_transpose(const dv_csr_host &a, std::vector<int32_t> &rp, std::vector<int32_t> &ci, std::vector<double> &va);

@@ -467,18 +467,22 @@ struct LaunchEnv {
 //
 // One warp per bundle of 32 row groups, one lane per group.  The loop over the
 // bundle's 4-entry words is warp-uniform; each lane decodes its leader row's
-// columns once (count byte at a block start, gap bytes inside a block) and
-// applies every gathered x value to the G rows of its group, which share the
-// column structure.  No shared-memory staging: every stream load is a
-// coalesced 128-byte warp transaction.  Each row still sums its entries in
-// order, so FP64 results equal the reference walk bit for bit.
+// columns once (entry byte 255: next block column; otherwise column += byte + 1)
+// and applies every gathered x value to the G rows of its group, which share
+// the column structure.  Words whose 4 entries all belong to the lane take a
+// path without per-entry predicates; only a lane's last word is predicated.
+// With SCALED, 8-bit value indices are byte offsets into the shared-memory
+// table (one byte extract and one shared load per value).  No staging: every
+// stream load is a coalesced 128-byte warp transaction, issued one word ahead
+// (register double buffer, streaming loads).  Each row still sums its entries
+// in order, so FP64 results equal the reference walk bit for bit.
 // ---------------------------------------------------------------------------
 template <class VI> struct ViChunk;
 template <> struct ViChunk<uint8_t> { using T = uint32_t; };
 template <> struct ViChunk<uint16_t> { using T = uint2; };
 template <> struct ViChunk<uint32_t> { using T = uint4; };
 
-__device__ __forceinline__ uint32_t vi_get(uint32_t c, int k) { return (c >> (8 * k)) & 0xFFu; }
+__device__ __forceinline__ uint32_t vi_get(uint32_t c, int k) { return __byte_perm(c, 0u, 0x4440u + (unsigned)k); }
 __device__ __forceinline__ uint32_t vi_get(uint2 c, int k) { return ((k < 2 ? c.x : c.y) >> (16 * (k & 1))) & 0xFFFFu; }
 __device__ __forceinline__ uint32_t vi_get(uint4 c, int k) { return k == 0 ? c.x : k == 1 ? c.y : k == 2 ? c.z : c.w; }
 
@@ -494,7 +498,15 @@ struct DuviLanesArgs {
     int32_t nuniq;
 };
 
-template <class VI, class AT, class Gather, class Op, int G>
+template <class AT, bool SCALED, bool SMEM, class Chunk>
+__device__ __forceinline__ AT lane_value(const AT *tab, const AT *gtab, const Chunk &c, int k) {
+    const uint32_t idx = vi_get(c, k);
+    if constexpr (SCALED) return *reinterpret_cast<const AT *>(reinterpret_cast<const char *>(tab) + idx);
+    else if constexpr (SMEM) return tab[idx];
+    else return __ldg(gtab + idx);
+}
+
+template <class VI, class AT, class Gather, class Op, int G, bool SCALED>
 __global__ void __launch_bounds__(256) k_duvi_lanes(DuviLanesArgs A, Gather g, Op op, const int *__restrict__ done,
                                                     double *partials, unsigned *ticket) {
     if (done && *(volatile const int *)done) return;
@@ -518,6 +530,7 @@ __global__ void __launch_bounds__(256) k_duvi_lanes(DuviLanesArgs A, Gather g, O
         const int64_t grp = (int64_t)bi * 32 + lane;
         const bool valid = grp < A.ngroups;
         const uint32_t ne = valid ? __ldg(A.nent + grp) : 0u;
+        const uint32_t full = ne >> 2;   // words whose 4 entries are all this lane's
         const int32_t r0 = (int32_t)(grp * G);
         AT s[G];
 #pragma unroll
@@ -525,7 +538,7 @@ __global__ void __launch_bounds__(256) k_duvi_lanes(DuviLanesArgs A, Gather g, O
         const uint32_t *dp = A.dist + d_base + lane;
         const Chunk *vp = vbase + v_base + lane;
         const uint32_t *cp = A.cols + c_base + lane;
-        uint32_t c = 0, rem = 0, b = 0;
+        uint32_t c = 0;
         // register double buffer: the streams of word w+1 are in flight while word w is decoded
         uint32_t dw_next = 0;
         Chunk vw_next[G];
@@ -544,33 +557,51 @@ __global__ void __launch_bounds__(256) k_duvi_lanes(DuviLanesArgs A, Gather g, O
 #pragma unroll
                 for (int d = 0; d < G; ++d) vw_next[d] = __ldcs(vp + ((size_t)(w + 1) * G + d) * 32);
             }
-            uint32_t cols[4];
+            if (w < full) {
+                uint32_t cols[4];
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const uint32_t byte = (dw >> (8 * k)) & 0xFFu;
-                if (w * 4 + k < ne) {
-                    if (rem == 0) {
-                        c = __ldcs(cp + (size_t)b * 32);
-                        ++b;
-                        rem = byte + 1u;
+                for (int k = 0; k < 4; ++k) {
+                    const uint32_t byte = __byte_perm(dw, 0u, 0x4440u + (unsigned)k);
+                    if (byte == 255u) {
+                        c = __ldcs(cp);
+                        cp += 32;
                     } else {
                         c += byte + 1u;
                     }
-                    --rem;
+                    cols[k] = c;
                 }
-                cols[k] = c;
-            }
-            AT xv[4];
+                AT xv[4];
 #pragma unroll
-            for (int k = 0; k < 4; ++k) xv[k] = (w * 4 + k < ne) ? g(cols[k]) : AT(0);
+                for (int k = 0; k < 4; ++k) xv[k] = g(cols[k]);
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                if (w * 4 + k < ne) {
+                for (int k = 0; k < 4; ++k)
 #pragma unroll
-                    for (int d = 0; d < G; ++d) {
-                        const uint32_t idx = vi_get(vw[d], k);
-                        const AT v = kSmemTable ? tab[idx] : __ldg(gtab + idx);
-                        s[d] = madd<AT>(s[d], v, xv[k]);
+                    for (int d = 0; d < G; ++d)
+                        s[d] = madd<AT>(s[d], lane_value<AT, SCALED, kSmemTable>(tab, gtab, vw[d], k), xv[k]);
+            } else if (w * 4 < ne) {   // the lane's last, partial word
+                uint32_t cols[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const uint32_t byte = __byte_perm(dw, 0u, 0x4440u + (unsigned)k);
+                    if (w * 4 + k < ne) {
+                        if (byte == 255u) {
+                            c = __ldcs(cp);
+                            cp += 32;
+                        } else {
+                            c += byte + 1u;
+                        }
+                    }
+                    cols[k] = c;
+                }
+                AT xv[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) xv[k] = (w * 4 + k < ne) ? g(cols[k]) : AT(0);
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    if (w * 4 + k < ne) {
+#pragma unroll
+                        for (int d = 0; d < G; ++d)
+                            s[d] = madd<AT>(s[d], lane_value<AT, SCALED, kSmemTable>(tab, gtab, vw[d], k), xv[k]);
                     }
                 }
             }
@@ -601,7 +632,10 @@ void launch_duvi_lanes_g(const LaunchEnv &e, const dv_matrix *m, Gather g, Op op
     int blocks = (int)((m->lanes_bundles + 7) / 8);
     if (blocks > e.max_blocks) blocks = e.max_blocks;
     if (blocks < 1) blocks = 1;
-    k_duvi_lanes<VI, AT, Gather, Op, G><<<blocks, 256, 0, e.stream>>>(a, g, op, e.done, e.partials, e.ticket);
+    if (sizeof(VI) == 1 && m->lanes_scaled)
+        k_duvi_lanes<VI, AT, Gather, Op, G, true><<<blocks, 256, 0, e.stream>>>(a, g, op, e.done, e.partials, e.ticket);
+    else
+        k_duvi_lanes<VI, AT, Gather, Op, G, false><<<blocks, 256, 0, e.stream>>>(a, g, op, e.done, e.partials, e.ticket);
     DV_CUDA(cudaGetLastError());
     e.ctx->count();
 }
@@ -609,6 +643,7 @@ void launch_duvi_lanes_g(const LaunchEnv &e, const dv_matrix *m, Gather g, Op op
 template <class VI, class AT, class Gather, class Op>
 void launch_duvi_lanes(const LaunchEnv &e, const dv_matrix *m, Gather g, Op op) {
     if (m->lanes_group == 3) launch_duvi_lanes_g<VI, AT, Gather, Op, 3>(e, m, g, op);
+    else if (m->lanes_group == 2) launch_duvi_lanes_g<VI, AT, Gather, Op, 2>(e, m, g, op);
     else launch_duvi_lanes_g<VI, AT, Gather, Op, 1>(e, m, g, op);
 }
 

@@ -153,8 +153,9 @@ static void finish_duvi_upload(dv_matrix *m, cudaStream_t s) {
     }
     {   // lane-interleaved derived layout
         DuviLanesHost L;
-        dv_build_duvi_lanes(h, m->n_rows, L);
+        dv_build_duvi_lanes(h, m->n_rows, m->precision == DV_F64 ? 8 : 4, L);
         m->lanes_group = L.group;
+        m->lanes_scaled = L.scaled;
         m->row_group = L.group;
         m->lanes_groups = L.ngroups;
         m->lanes_bundles = L.nbundles;

@@ -2,6 +2,7 @@
 // object, shared by the single- and multi-right-hand-side drivers.
 #pragma once
 
+#include "dv_gs.cuh"
 #include "dv_kernels.cuh"
 #include "dv_solvers.cuh"
 
@@ -24,6 +25,7 @@ struct VLevel {
     std::unique_ptr<dv_matrix> A, R, P;
     DevMem w, b, x, t, r;
     int32_t n = 0;
+    GsOrder gs;   // Gauss-Seidel row groups (smoother != Jacobi)
 };
 
 template <class T>
@@ -33,6 +35,7 @@ struct VCycle {
     int32_t nc = 0;
     DevMem ainv, bc, xc;
     int nu = 2;
+    int smoother = DV_SMOOTHER_JACOBI;
 
     // x_0 = V(b_0); returns the buffer that holds the result (level-0 x or t).
     T *run(const LaunchEnv &e, const T *b0) { return level(e, 0, b0); }
@@ -47,6 +50,7 @@ struct VCycle {
             return xc.template as<T>();
         }
         VLevel<T> &L = lv[l];
+        if (smoother != DV_SMOOTHER_JACOBI) return level_gs(e, l, b);
         T *x = L.x.template as<T>(), *t = L.t.template as<T>();
         const T *w = L.w.template as<T>();
         if (nu == 1) {
@@ -79,6 +83,31 @@ struct VCycle {
             launch_rows<T>(e, L.A.get(), GatherVec<T, T>{x}, oj);
             std::swap(x, t);
         }
+        return x;
+    }
+
+    // Gauss-Seidel variant: x = 0, nu forward sweeps, coarse correction, nu forward sweeps.
+    T *level_gs(const LaunchEnv &e, size_t l, const T *b) {
+        cudaStream_t s = e.stream;
+        VLevel<T> &L = lv[l];
+        T *x = L.x.template as<T>();
+        k_fill<T><<<grid_for(ctx, L.n), kThreads, 0, s>>>(x, T(0), L.n, e.done);
+        DV_CUDA(cudaGetLastError());
+        ctx->count();
+        for (int k = 0; k < nu; ++k) gs_sweep<T>(e, L.A.get(), L.gs, b, x);
+        OpResid<T> orr{{}, b, L.r.template as<T>()};
+        launch_rows<T>(e, L.A.get(), GatherVec<T, T>{x}, orr);
+        T *bn = l + 1 < lv.size() ? lv[l + 1].b.template as<T>() : bc.template as<T>();
+        OpSpmv<T, T> orst;
+        orst.y = bn;
+        orst.clear = 1;
+        launch_rows<T>(e, L.R.get(), GatherVec<T, T>{L.r.template as<T>()}, orst);
+        T *xn = level(e, l + 1, bn);
+        OpSpmv<T, T> opro;
+        opro.y = x;
+        opro.clear = 0;
+        launch_rows<T>(e, L.P.get(), GatherVec<T, T>{xn}, opro);
+        for (int k = 0; k < nu; ++k) gs_sweep<T>(e, L.A.get(), L.gs, b, x);
         return x;
     }
 };

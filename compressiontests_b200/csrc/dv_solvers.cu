@@ -405,6 +405,7 @@ static std::unique_ptr<VCycle<T>> build_vcycle(dv_context *ctx, SolverWs &ws, in
     auto v = std::make_unique<VCycle<T>>();
     v->ctx = ctx;
     v->nu = cfg.nu;
+    v->smoother = cfg.smoother;
     const int prec = sizeof(T) == 8 ? DV_F64 : DV_F32;
     cudaStream_t s = ctx->stream;
     v->lv.resize(L - 1);
@@ -430,6 +431,7 @@ static std::unique_ptr<VCycle<T>> build_vcycle(dv_context *ctx, SolverWs &ws, in
         omega_eff.push_back(om);
         const size_t vs = sizeof(T) * (size_t)lv.n;
         lv.w.alloc(vs); lv.b.alloc(vs); lv.x.alloc(vs); lv.t.alloc(vs); lv.r.alloc(vs);
+        if (cfg.smoother != DV_SMOOTHER_JACOBI) gs_build_order(A[l], cfg.smoother == DV_SMOOTHER_GS_LEX, s, lv.gs);
         k_make_weights<T><<<grid_for(ctx, lv.n), kThreads, 0, s>>>(lv.A->diag.template as<double>(), lv.w.template as<T>(), om, lv.n);
         DV_CUDA(cudaGetLastError());
     }
@@ -461,6 +463,7 @@ extern "C" DV_API int dv_mgpcg_create(dv_context *ctx, int32_t L, const dv_csr_h
         DV_REQUIRE(cfg->precision == DV_F64 || cfg->precision == DV_MIXED, DV_ERR_ARG, "precision must be DV_F64 or DV_MIXED");
         DV_REQUIRE(cfg->nu >= 1 && cfg->max_iterations >= 1 && cfg->tol > 0, DV_ERR_ARG, "bad smoothing or stop parameters");
         DV_REQUIRE(L >= 2, DV_ERR_ARG, "need at least two levels");
+        DV_REQUIRE(cfg->smoother >= DV_SMOOTHER_JACOBI && cfg->smoother <= DV_SMOOTHER_GS_COLOR, DV_ERR_ARG, "unknown smoother");
         dv_ctx_check(ctx);
         auto s = std::make_unique<dv_mgpcg>();
         s->ctx = ctx;

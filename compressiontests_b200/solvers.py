@@ -237,7 +237,8 @@ class CudaCsrPcgSolver:
 
 
 class MultigridPcgSolver:
-    """Flexible CG preconditioned by a V(nu, nu) weighted-Jacobi cycle.
+    """Flexible CG preconditioned by a V(nu, nu) cycle (weighted Jacobi, or forward Gauss-Seidel
+    in the reference's row order / multicolor with smoother="gs_lex" / "gs_color").
 
     precision='mixed': FP32 V-cycle (values, vectors, accumulation) inside an
     FP64 outer loop; precision='f64': everything FP64.  Stop: ||r||/||b|| <= tol,
@@ -246,14 +247,15 @@ class MultigridPcgSolver:
 
     def __init__(self, context: CudaContext, A_levels, P_levels, precision="mixed", fmt="duvi", outer_fmt=None,
                  nu=2, omega=2.0 / 3.0, omega_mode="spectral", tol=1e-8, max_iterations=500, iterations_per_sync=4,
-                 use_graphs=True):
+                 use_graphs=True, smoother="jacobi"):
         self.context = context
         ah, ka = _hosts(A_levels)
         ph, kp = _hosts(P_levels)
         f = {"csr": N.FORMAT_CSR, "duvi": N.FORMAT_DUVI}
+        sm = {"jacobi": N.SMOOTHER_JACOBI, "gs_lex": N.SMOOTHER_GS_LEX, "gs_color": N.SMOOTHER_GS_COLOR}[smoother]
         cfg = N.MgpcgConfig({"mixed": N.MIXED, "f64": N.F64}[precision], f[fmt], f[outer_fmt or fmt], nu, omega,
                             {"absolute": N.OMEGA_ABSOLUTE, "spectral": N.OMEGA_SPECTRAL}[omega_mode], max_iterations,
-                            tol, iterations_per_sync, 1 if use_graphs else 0)
+                            tol, iterations_per_sync, 1 if use_graphs else 0, sm)
         h = C.c_void_p()
         N.check(N.lib().dv_mgpcg_create(context.h, len(A_levels), ah, ph, C.byref(cfg), C.byref(h)))
         del ka, kp
@@ -325,12 +327,13 @@ class BatchedMultigridSolver:
 
     def __init__(self, context: CudaContext, meshes, precision="mixed", fmt="duvi", outer_fmt=None, nu=2,
                  omega=2.0 / 3.0, omega_mode="spectral", tol=1e-8, max_iterations=500, iterations_per_sync=4,
-                 use_graphs=True):
+                 use_graphs=True, smoother="jacobi"):
         self.context = context
         f = {"csr": N.FORMAT_CSR, "duvi": N.FORMAT_DUVI}
+        sm = {"jacobi": N.SMOOTHER_JACOBI, "gs_lex": N.SMOOTHER_GS_LEX, "gs_color": N.SMOOTHER_GS_COLOR}[smoother]
         cfg = N.MgpcgConfig({"mixed": N.MIXED, "f64": N.F64}[precision], f[fmt], f[outer_fmt or fmt], nu, omega,
                             {"absolute": N.OMEGA_ABSOLUTE, "spectral": N.OMEGA_SPECTRAL}[omega_mode], max_iterations,
-                            tol, iterations_per_sync, 1 if use_graphs else 0)
+                            tol, iterations_per_sync, 1 if use_graphs else 0, sm)
         nm = len(meshes)
         nlev = np.array([len(a) for a, _ in meshes], np.int32)
         keep, a_arrs, p_arrs = [], (C.c_void_p * nm)(), (C.c_void_p * nm)()

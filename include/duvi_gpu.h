@@ -224,6 +224,12 @@ typedef struct {
     double tol;                 /* relative 2-norm */
     int32_t iterations_per_sync;/* outer iterations per host convergence read (0 = 4) */
     int32_t use_graphs;         /* capture the iteration sequence in a CUDA graph */
+    int32_t smoother;           /* DV_SMOOTHER_JACOBI (default, 0): weighted Jacobi as above;
+                                   DV_SMOOTHER_GS_LEX: nu forward Gauss-Seidel sweeps before and after
+                                   the coarse correction, rows in the reference's order
+                                   (GaussSeidelIterationCsrDuVi.cs:22-50; dependency levels on the GPU);
+                                   DV_SMOOTHER_GS_COLOR: the same with multicolor node blocks.
+                                   Gauss-Seidel is unweighted (omega unused); dv_batch_* accept Jacobi only. */
 } dv_mgpcg_config;
 
 DV_API int dv_mgpcg_create(dv_context *ctx, int32_t n_levels, const dv_csr_host *A,

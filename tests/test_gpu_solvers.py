@@ -197,3 +197,31 @@ def test_mgpcg_deterministic_across_solver_lifetimes(ctx, native):
                 assert seen[key] == st.NumIterationsRequired, key
                 s.release()
     assert seen[(4, "csr", "f64")] <= 12 and seen[(3, "duvi", "mixed")] <= 13
+
+
+@pytest.mark.parametrize("smoother,precision,fmt", [("gs_lex", "f64", "csr"), ("gs_lex", "mixed", "duvi"),
+                                                    ("gs_color", "mixed", "duvi"), ("gs_color", "f64", "duvi")])
+def test_mgpcg_gauss_seidel_smoothing(ctx, native, oracle, smoother, precision, fmt):
+    # V(2,2) with forward Gauss-Seidel (the reference's row order, or multicolor) inside the
+    # flexible CG: same system, so the solution must match the oracle's FP64 MG-FCG solve,
+    # and Gauss-Seidel needs fewer outer iterations than weighted Jacobi.
+    ne = (16, 16, 16)
+    A, P = native.hex_hierarchy(ne, coarse_ne=4)
+    b = native.traction_rhs(ne)
+    s = native.MultigridPcgSolver(ctx, A, P, precision=precision, fmt=fmt, nu=2, tol=1e-10, max_iterations=200,
+                                  smoother=smoother)
+    x, st = s.Solve(b)
+    assert st.HasConverged and st.RelativeResidual <= 1e-10
+    Ao = [oracle.Csr.from_scipy(a) for a in A]
+    Po = [oracle.Csr.from_scipy(p) for p in P]
+    x_ref, it_ref, _ = oracle.mg_fcg(Ao, Po, b, 4 / (3 * 3.09), 2, 200, 1e-10)
+    assert rel(x, x_ref) < 1e-8
+    assert st.NumIterationsRequired < it_ref
+    x2, st2 = s.Solve(b)   # graph replay gives the same iterate
+    np.testing.assert_array_equal(x, x2)
+
+
+def test_batch_rejects_gauss_seidel(ctx, native):
+    A, P = native.hex_hierarchy((8, 8, 8), coarse_ne=4)
+    with pytest.raises(native.NotImplementedFeatureError):
+        native.BatchedMultigridSolver(ctx, [(A, P)], smoother="gs_color")
