@@ -189,10 +189,34 @@ int dv_csr_row_group(const dv_csr_host &a) {
     return 1;
 }
 
-// Entry bytes of the lane layout: 255 marks a block start (its column comes from
-// the block column list), any other value is gap - 1 (at most 254: blocks break
-// at gaps of 256).  With at most 256 / value_bytes distinct values, 8-bit value
-// indices are stored pre-multiplied by the value size, as byte offsets into the table.
+// Entry bytes of the lane layout: 255 marks a lane-block start (its column comes
+// from the lane's column list), any other value is gap - 1.  Lane blocks are the
+// SoA blocks, further split before every entry whose gap is exactly 256 (gap - 1 =
+// 255 is legal inside an SoA block), so the marker is never ambiguous.  With at
+// most 256 / value_bytes distinct values, 8-bit value indices are stored
+// pre-multiplied by the value size, as byte offsets into the table.
+namespace {
+// Walks the leader row r0 of a group: calls f(entry, column, starts_lane_block).
+template <class F>
+void walk_lane_blocks(const DuviHost &h, int32_t r0, F f) {
+    const uint32_t d0 = h.row_to_dist[r0], ne = h.row_to_dist[r0 + 1] - d0;
+    uint32_t bl = h.row_to_col[r0], next_start = 0, c = 0;
+    for (uint32_t e = 0; e < ne; ++e) {
+        const uint32_t byte = h.dist[d0 + e];
+        bool start = false;
+        if (e == next_start) {   // SoA block start: byte = entries that follow in the block
+            next_start = e + byte + 1;
+            c = h.col_idx[bl++];
+            start = true;
+        } else {
+            c += byte + 1;
+            start = byte == 255u;
+        }
+        f(e, c, start, byte);
+    }
+}
+}  // namespace
+
 void dv_build_duvi_lanes(const DuviHost &h, int32_t n, int value_bytes, DuviLanesHost &L) {
     const int g = detect_group(h, n);
     const int vib = h.vi_bits / 8;            // bytes per value index
@@ -212,7 +236,8 @@ void dv_build_duvi_lanes(const DuviHost &h, int32_t n, int value_bytes, DuviLane
             int64_t gi = bi * 32 + t;
             if (gi >= L.ngroups) break;
             int32_t r0 = (int32_t)(gi * g);
-            uint32_t ne = h.row_to_dist[r0 + 1] - h.row_to_dist[r0], nb = h.row_to_col[r0 + 1] - h.row_to_col[r0];
+            uint32_t ne = h.row_to_dist[r0 + 1] - h.row_to_dist[r0], nb = 0;
+            walk_lane_blocks(h, r0, [&](uint32_t, uint32_t, bool start, uint32_t) { nb += start; });
             L.nent[gi] = ne;
             le = std::max(le, ne);
             lb = std::max(lb, nb);
@@ -245,16 +270,17 @@ void dv_build_duvi_lanes(const DuviHost &h, int32_t n, int value_bytes, DuviLane
             if (gi >= L.ngroups) break;
             const int32_t r0 = (int32_t)(gi * g);
             const uint32_t d0 = h.row_to_dist[r0], ne = h.row_to_dist[r0 + 1] - d0;
-            uint32_t next_start = 0;
-            for (uint32_t e = 0; e < ne; ++e) {
-                uint32_t w = e / 4, k = e % 4;
-                uint32_t byte = h.dist[d0 + e];
-                if (e == next_start) {
-                    next_start = e + byte + 1;   // the count byte of this block
+            uint32_t nlb = 0;
+            walk_lane_blocks(h, r0, [&](uint32_t e, uint32_t c, bool start, uint32_t byte) {
+                const uint32_t w = e / 4, k = e % 4;
+                if (start) {
                     byte = 255u;
+                    L.cols[cwords[bi] + (uint64_t)nlb * 32 + t] = c;
+                    ++nlb;
                 }
                 L.dist[dwords[bi] + (uint64_t)w * 32 + t] |= byte << (8 * k);
-            }
+            });
+            (void)d0;
             for (int d = 0; d < g; ++d) {
                 const uint32_t rd = h.row_to_dist[r0 + d];
                 for (uint32_t e = 0; e < ne; ++e) {
@@ -265,8 +291,6 @@ void dv_build_duvi_lanes(const DuviHost &h, int32_t n, int value_bytes, DuviLane
                     std::memcpy(&L.vi[c * chunk + k * vib], &v, vib);   // little-endian low bytes
                 }
             }
-            const uint32_t c0 = h.row_to_col[r0], nb = h.row_to_col[r0 + 1] - c0;
-            for (uint32_t b = 0; b < nb; ++b) L.cols[cwords[bi] + (uint64_t)b * 32 + t] = h.col_idx[c0 + b];
             (void)words;
         }
     }

@@ -203,3 +203,34 @@ def test_residual_device(ctx, native, cantilever, rng):
     M.residual_device(db.data_ptr(), dx.data_ptr(), dr.data_ptr())
     ctx.synchronize()
     assert rowwise_rel(dr.cpu().numpy(), b - A @ x, A, x) <= REL64
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_lane_kernel_gaps_of_256_inside_blocks(ctx, native, oracle, prec):
+    # Node-grouped rows (3 rows share columns) whose runs contain gaps of exactly 255, 256
+    # and 257: a gap of 256 stays inside a DuVi block (its byte is 255), which the lane
+    # layout must not take for a block start.
+    n = 3 * 700
+    rows, cols, vals = [], [], []
+    for g in range(n // 3):
+        c, cs = (g * 7) % 50, []
+        for gap in (1, 256, 256, 1, 255, 257, 256, 2, 256):
+            if c >= n:
+                break
+            cs.append(c)
+            c += gap
+        for d in range(3):
+            for x in cs:
+                rows.append(3 * g + d)
+                cols.append(x)
+                vals.append(1.0 + 0.25 * ((x + d) % 5))
+    A = sp.csr_matrix((vals, (rows, cols)), shape=(n, n))
+    A.sort_indices()
+    M = native.SparseMatrix(ctx, A, "duvi", prec)
+    assert M.info()["kernel_variant"] == 103   # the lane kernel, 3-row groups
+    x = np.random.default_rng(3).standard_normal(n)
+    y = M.Multiply(x)
+    if prec == "f64":
+        np.testing.assert_array_equal(y, oracle.DuVi(oracle.Csr.from_scipy(A)).spmv(x))
+    else:
+        assert rowwise_rel(y, A @ x, A, x) <= REL32
