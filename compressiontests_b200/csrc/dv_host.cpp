@@ -146,25 +146,37 @@ void dv_make_bundles(const DuviHost &h, int32_t n_rows, int vi_bits, std::vector
     bundles.push_back(n_rows);
 }
 
-// Group size: g consecutive rows with identical block structure (same block
-// count, same block columns, same gap bytes), e.g. the dofs of one node.
-static int detect_group(const DuviHost &h, int32_t n) {
-    for (int g : {3, 2}) {
-        if (n % g != 0 || n == 0) continue;
-        int ok = 1;
+// Group size: g consecutive rows with the same block structure (same block
+// count, same gap bytes) whose block columns are either identical (the dofs of
+// one node in a stiffness matrix) or shifted by the row's index in the group
+// (shift = 1: component d of a node couples to component d of its neighbours,
+// as in the trilinear transfers).  Returns g (1 if none) and sets shift.
+static int detect_group(const DuviHost &h, int32_t n, int &shift) {
+    for (int sh : {0, 1})
+        for (int g : {3, 2}) {
+            if (n % g != 0 || n == 0) continue;
+            int ok = 1;
 #pragma omp parallel for schedule(static) reduction(min : ok)
-        for (int32_t gi = 0; gi < n / g; ++gi) {
-            const int32_t r0 = gi * g;
-            const uint32_t nb = h.row_to_col[r0 + 1] - h.row_to_col[r0], ne = h.row_to_dist[r0 + 1] - h.row_to_dist[r0];
-            for (int d = 1; d < g && ok; ++d) {
-                const int32_t r = r0 + d;
-                if (h.row_to_col[r + 1] - h.row_to_col[r] != nb || h.row_to_dist[r + 1] - h.row_to_dist[r] != ne) { ok = 0; break; }
-                if (std::memcmp(&h.col_idx[h.row_to_col[r]], &h.col_idx[h.row_to_col[r0]], 4 * (size_t)nb) != 0 ||
-                    std::memcmp(&h.dist[h.row_to_dist[r]], &h.dist[h.row_to_dist[r0]], ne) != 0) ok = 0;
+            for (int32_t gi = 0; gi < n / g; ++gi) {
+                const int32_t r0 = gi * g;
+                const uint32_t nb = h.row_to_col[r0 + 1] - h.row_to_col[r0], ne = h.row_to_dist[r0 + 1] - h.row_to_dist[r0];
+                for (int d = 1; d < g && ok; ++d) {
+                    const int32_t r = r0 + d;
+                    if (h.row_to_col[r + 1] - h.row_to_col[r] != nb || h.row_to_dist[r + 1] - h.row_to_dist[r] != ne) {
+                        ok = 0;
+                        break;
+                    }
+                    if (std::memcmp(&h.dist[h.row_to_dist[r]], &h.dist[h.row_to_dist[r0]], ne) != 0) ok = 0;
+                    for (uint32_t b = 0; b < nb && ok; ++b)
+                        if (h.col_idx[h.row_to_col[r] + b] != h.col_idx[h.row_to_col[r0] + b] + (uint32_t)(sh * d)) ok = 0;
+                }
+            }
+            if (ok) {
+                shift = sh;
+                return g;
             }
         }
-        if (ok) return g;
-    }
+    shift = 0;
     return 1;
 }
 
@@ -218,10 +230,12 @@ void walk_lane_blocks(const DuviHost &h, int32_t r0, F f) {
 }  // namespace
 
 void dv_build_duvi_lanes(const DuviHost &h, int32_t n, int value_bytes, DuviLanesHost &L) {
-    const int g = detect_group(h, n);
+    int shift = 0;
+    const int g = detect_group(h, n, shift);
     const int vib = h.vi_bits / 8;            // bytes per value index
     const size_t chunk = 4 * (size_t)vib;     // bytes per chunk of 4 indices
     L.group = g;
+    L.shift = shift;
     L.scaled = (vib == 1 && (int64_t)h.values.size() * value_bytes <= 256) ? 1 : 0;
     L.ngroups = n / g;
     L.nbundles = (L.ngroups + 31) / 32;

@@ -133,6 +133,7 @@ struct DuviHost {   // host copy of the SoA encoding (export / parity)
 struct DuviLanesHost {
     int group = 1;
     int scaled = 0;                // 1: value-index bytes hold index * value size (byte offsets into the table)
+    int shift = 0;                 // 1: row d of a group reads columns of the leader row + d
     int64_t ngroups = 0, nbundles = 0;
     std::vector<uint32_t> meta;    // per bundle: d_base, v_base, c_base, words, blocks
     std::vector<uint32_t> dist;    // leader entry bytes, 4 per word: 255 at a block start, else gap - 1
@@ -160,6 +161,7 @@ struct dv_matrix {
     int duvi_variant = 0;      // 0: shared-memory staged rows, 1: lane-interleaved groups (autotuned)
     int lanes_group = 1;
     int lanes_scaled = 0;
+    int lanes_shift = 0;
     int64_t lanes_bundles = 0, lanes_groups = 0;
     DevMem lanes_meta, lanes_dist, lanes_vi, lanes_cols, lanes_nent;
     int64_t lanes_bytes = 0;   // bytes one product reads from the lane layout

@@ -506,7 +506,7 @@ __device__ __forceinline__ AT lane_value(const AT *tab, const AT *gtab, const Ch
     else return __ldg(gtab + idx);
 }
 
-template <class VI, class AT, class Gather, class Op, int G, bool SCALED>
+template <class VI, class AT, class Gather, class Op, int G, bool SCALED, bool SHIFT>
 __global__ void __launch_bounds__(256) k_duvi_lanes(DuviLanesArgs A, Gather g, Op op, const int *__restrict__ done,
                                                     double *partials, unsigned *ticket) {
     if (done && *(volatile const int *)done) return;
@@ -570,14 +570,27 @@ __global__ void __launch_bounds__(256) k_duvi_lanes(DuviLanesArgs A, Gather g, O
                     }
                     cols[k] = c;
                 }
-                AT xv[4];
+                if constexpr (SHIFT) {   // row d reads column + d
+                    AT xs[4][G];
 #pragma unroll
-                for (int k = 0; k < 4; ++k) xv[k] = g(cols[k]);
+                    for (int k = 0; k < 4; ++k)
 #pragma unroll
-                for (int k = 0; k < 4; ++k)
+                        for (int d = 0; d < G; ++d) xs[k][d] = g(cols[k] + (uint32_t)d);
 #pragma unroll
-                    for (int d = 0; d < G; ++d)
-                        s[d] = madd<AT>(s[d], lane_value<AT, SCALED, kSmemTable>(tab, gtab, vw[d], k), xv[k]);
+                    for (int k = 0; k < 4; ++k)
+#pragma unroll
+                        for (int d = 0; d < G; ++d)
+                            s[d] = madd<AT>(s[d], lane_value<AT, SCALED, kSmemTable>(tab, gtab, vw[d], k), xs[k][d]);
+                } else {
+                    AT xv[4];
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) xv[k] = g(cols[k]);
+#pragma unroll
+                    for (int k = 0; k < 4; ++k)
+#pragma unroll
+                        for (int d = 0; d < G; ++d)
+                            s[d] = madd<AT>(s[d], lane_value<AT, SCALED, kSmemTable>(tab, gtab, vw[d], k), xv[k]);
+                }
             } else if (w * 4 < ne) {   // the lane's last, partial word
                 uint32_t cols[4];
 #pragma unroll
@@ -593,15 +606,14 @@ __global__ void __launch_bounds__(256) k_duvi_lanes(DuviLanesArgs A, Gather g, O
                     }
                     cols[k] = c;
                 }
-                AT xv[4];
-#pragma unroll
-                for (int k = 0; k < 4; ++k) xv[k] = (w * 4 + k < ne) ? g(cols[k]) : AT(0);
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
                     if (w * 4 + k < ne) {
+                        const AT x0 = SHIFT ? AT(0) : g(cols[k]);
 #pragma unroll
                         for (int d = 0; d < G; ++d)
-                            s[d] = madd<AT>(s[d], lane_value<AT, SCALED, kSmemTable>(tab, gtab, vw[d], k), xv[k]);
+                            s[d] = madd<AT>(s[d], lane_value<AT, SCALED, kSmemTable>(tab, gtab, vw[d], k),
+                                            SHIFT ? g(cols[k] + (uint32_t)d) : x0);
                     }
                 }
             }
@@ -632,10 +644,22 @@ void launch_duvi_lanes_g(const LaunchEnv &e, const dv_matrix *m, Gather g, Op op
     int blocks = (int)((m->lanes_bundles + 7) / 8);
     if (blocks > e.max_blocks) blocks = e.max_blocks;
     if (blocks < 1) blocks = 1;
-    if (sizeof(VI) == 1 && m->lanes_scaled)
-        k_duvi_lanes<VI, AT, Gather, Op, G, true><<<blocks, 256, 0, e.stream>>>(a, g, op, e.done, e.partials, e.ticket);
-    else
-        k_duvi_lanes<VI, AT, Gather, Op, G, false><<<blocks, 256, 0, e.stream>>>(a, g, op, e.done, e.partials, e.ticket);
+    bool done_launch = false;
+    if constexpr (sizeof(VI) == 1) {
+        if (m->lanes_scaled) {
+            if (G > 1 && m->lanes_shift)
+                k_duvi_lanes<VI, AT, Gather, Op, G, true, G != 1><<<blocks, 256, 0, e.stream>>>(a, g, op, e.done, e.partials, e.ticket);
+            else
+                k_duvi_lanes<VI, AT, Gather, Op, G, true, false><<<blocks, 256, 0, e.stream>>>(a, g, op, e.done, e.partials, e.ticket);
+            done_launch = true;
+        }
+    }
+    if (!done_launch) {
+        if (G > 1 && m->lanes_shift)
+            k_duvi_lanes<VI, AT, Gather, Op, G, false, G != 1><<<blocks, 256, 0, e.stream>>>(a, g, op, e.done, e.partials, e.ticket);
+        else
+            k_duvi_lanes<VI, AT, Gather, Op, G, false, false><<<blocks, 256, 0, e.stream>>>(a, g, op, e.done, e.partials, e.ticket);
+    }
     DV_CUDA(cudaGetLastError());
     e.ctx->count();
 }

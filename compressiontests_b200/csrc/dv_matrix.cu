@@ -156,7 +156,8 @@ static void finish_duvi_upload(dv_matrix *m, cudaStream_t s) {
         dv_build_duvi_lanes(h, m->n_rows, m->precision == DV_F64 ? 8 : 4, L);
         m->lanes_group = L.group;
         m->lanes_scaled = L.scaled;
-        m->row_group = L.group;
+        m->lanes_shift = L.shift;
+        m->row_group = L.shift ? 1 : L.group;   // block products need identical columns
         m->lanes_groups = L.ngroups;
         m->lanes_bundles = L.nbundles;
         upload(m->lanes_meta, L.meta.data(), 4 * L.meta.size(), s);

@@ -234,3 +234,18 @@ def test_lane_kernel_gaps_of_256_inside_blocks(ctx, native, oracle, prec):
         np.testing.assert_array_equal(y, oracle.DuVi(oracle.Csr.from_scipy(A)).spmv(x))
     else:
         assert rowwise_rel(y, A @ x, A, x) <= REL32
+
+
+@pytest.mark.parametrize("ne", [(8, 6, 6), (7, 9, 5)])
+def test_transfer_products_shifted_groups_bit_exact(ctx, native, oracle, ne):
+    # Trilinear P and R = P^T: the 3 rows of a node read columns shifted by the dof
+    # component, which the lane layout stores once per node (shifted groups).
+    P = native.hex_trilinear(ne)
+    for M in (P, P.T.tocsr()):
+        M.sort_indices()
+        D = native.SparseMatrix(ctx, M, "duvi", "f64")
+        assert D.info()["kernel_variant"] == 103
+        x = np.random.default_rng(5).standard_normal(M.shape[1])
+        np.testing.assert_array_equal(D.Multiply(x), oracle.DuVi(oracle.Csr.from_scipy(M)).spmv(x))
+        F = native.SparseMatrix(ctx, M, "duvi", "f32")
+        assert rowwise_rel(F.Multiply(x), M @ x, M, x) <= REL32
