@@ -16,7 +16,7 @@
 //
 // Outer loop.  FCG(1) in FP64 on the block-diagonal fine operator with
 // per-mesh scalars (alpha, beta, ||r||/||b|| stop test): reductions run over
-// chunks of at most 2048 rows that never cross a mesh, and the last block sums
+// chunks of at most 512 rows that never cross a mesh, and the last block sums
 // every mesh's chunks in order (deterministic).  A converged mesh is frozen
 // (alpha = 0) while the others continue; the FP64 true residual of every mesh
 // is verified at exit.  The reference solves one model per solver object
@@ -31,7 +31,7 @@
 
 namespace {
 
-constexpr int kChunkRows = 2048;
+constexpr int kChunkRows = 512;
 constexpr int kMaxRefinements = 4;
 constexpr int32_t kMaxCoarseDofs = 16384;
 
