@@ -229,7 +229,7 @@ void walk_lane_blocks(const DuviHost &h, int32_t r0, F f) {
 }
 }  // namespace
 
-void dv_build_duvi_lanes(const DuviHost &h, int32_t n, int value_bytes, DuviLanesHost &L) {
+void dv_build_duvi_lanes(const DuviHost &h, int32_t n, int32_t n_cols, int value_bytes, DuviLanesHost &L) {
     int shift = 0;
     const int g = detect_group(h, n, shift);
     const int vib = h.vi_bits / 8;            // bytes per value index
@@ -238,6 +238,74 @@ void dv_build_duvi_lanes(const DuviHost &h, int32_t n, int value_bytes, DuviLane
     L.shift = shift;
     L.scaled = (vib == 1 && (int64_t)h.values.size() * value_bytes <= 256) ? 1 : 0;
     L.ngroups = n / g;
+    // Node tuples: with 8-bit indices and groups of 2-3 rows, the g value indices of a
+    // node-entry often take few distinct combinations (165 for the hex operators at any
+    // size); up to 256 of them, each node-entry stores one tuple index instead of g
+    // value indices.  Tuples are numbered in first-occurrence order.
+    L.tuples = 0;
+    L.tuple_vi.clear();
+    if (g >= 2 && vib == 1) {
+        std::vector<int16_t> id(1u << (8 * g), -1);
+        int ntup = 0;
+        bool ok = true;
+        for (int64_t gi = 0; gi < L.ngroups && ok; ++gi) {
+            const int32_t r0 = (int32_t)(gi * g);
+            const uint32_t ne = h.row_to_dist[r0 + 1] - h.row_to_dist[r0];
+            for (uint32_t e = 0; e < ne; ++e) {
+                uint32_t key = 0;
+                for (int d = 0; d < g; ++d) key |= h.vidx[h.row_to_dist[r0 + d] + e] << (8 * d);
+                if (id[key] < 0) {
+                    if (ntup == 256) { ok = false; break; }
+                    id[key] = (int16_t)ntup++;
+                    for (int d = 0; d < g; ++d) L.tuple_vi.push_back((key >> (8 * d)) & 0xFFu);
+                }
+            }
+        }
+        if (ok) {
+            L.tuples = 1;
+            L.tuple_id.swap(id);
+        } else {
+            L.tuple_vi.clear();
+        }
+    }
+    const int nv = L.tuples ? 1 : g;   // index chunks per word
+    // Stencil mode (square operators with node tuples, identical columns in a group):
+    // on a structured mesh the column offset of a node-entry from the group's first
+    // row takes few values (81 for the hex operators: 27 neighbours x 3 dofs); up to
+    // 256 of them, the entry byte is an index into an offset table and the column
+    // list, block starts and gaps are not stored at all.
+    L.stencil = 0;
+    L.offsets.clear();
+    if (L.tuples && !shift && n_cols == n) {
+        bool ok = true;
+#pragma omp parallel
+        {
+            OffsetSet local;
+#pragma omp for schedule(static)
+            for (int64_t gi = 0; gi < L.ngroups; ++gi) {
+                if (!ok) continue;
+                const int32_t r0 = (int32_t)(gi * g);
+                walk_lane_blocks(h, r0, [&](uint32_t, uint32_t c, bool, uint32_t) {
+                    if (!local.insert((int64_t)c - r0)) ok = false;
+                });
+            }
+#pragma omp critical
+            {
+                for (int64_t k : local.keys)
+                    if (ok && !L.offset_set.insert(k)) ok = false;
+            }
+        }
+        if (ok) {   // ids in ascending offset order (independent of the thread schedule)
+            std::vector<int64_t> ks = L.offset_set.keys;
+            std::sort(ks.begin(), ks.end());
+            L.offset_set = OffsetSet();
+            for (int64_t k : ks) {
+                L.offset_set.insert(k);
+                L.offsets.push_back((int32_t)k);
+            }
+            L.stencil = 1;
+        }
+    }
     L.nbundles = (L.ngroups + 31) / 32;
     L.meta.assign(5 * L.nbundles, 0);
     L.nent.assign(L.ngroups, 0);
@@ -258,8 +326,8 @@ void dv_build_duvi_lanes(const DuviHost &h, int32_t n, int value_bytes, DuviLane
         }
         const uint32_t words = (le + 3) / 4;
         dwords[bi + 1] = (uint64_t)words * 32;
-        vchunks[bi + 1] = (uint64_t)words * g * 32;
-        cwords[bi + 1] = (uint64_t)lb * 32;
+        vchunks[bi + 1] = (uint64_t)words * nv * 32;
+        cwords[bi + 1] = L.stencil ? 0 : (uint64_t)lb * 32;
         L.meta[5 * bi + 3] = words;
         L.meta[5 * bi + 4] = lb;
     }
@@ -287,7 +355,9 @@ void dv_build_duvi_lanes(const DuviHost &h, int32_t n, int value_bytes, DuviLane
             uint32_t nlb = 0;
             walk_lane_blocks(h, r0, [&](uint32_t e, uint32_t c, bool start, uint32_t byte) {
                 const uint32_t w = e / 4, k = e % 4;
-                if (start) {
+                if (L.stencil) {
+                    byte = (uint32_t)L.offset_set.find((int64_t)c - r0);
+                } else if (start) {
                     byte = 255u;
                     L.cols[cwords[bi] + (uint64_t)nlb * 32 + t] = c;
                     ++nlb;
@@ -295,19 +365,31 @@ void dv_build_duvi_lanes(const DuviHost &h, int32_t n, int value_bytes, DuviLane
                 L.dist[dwords[bi] + (uint64_t)w * 32 + t] |= byte << (8 * k);
             });
             (void)d0;
-            for (int d = 0; d < g; ++d) {
-                const uint32_t rd = h.row_to_dist[r0 + d];
+            if (L.tuples) {
                 for (uint32_t e = 0; e < ne; ++e) {
-                    uint32_t w = e / 4, k = e % 4;
-                    uint64_t c = vchunks[bi] + ((uint64_t)w * g + d) * 32 + t;
-                    uint32_t v = h.vidx[rd + e];
-                    if (L.scaled) v *= (uint32_t)value_bytes;
-                    std::memcpy(&L.vi[c * chunk + k * vib], &v, vib);   // little-endian low bytes
+                    uint32_t key = 0;
+                    for (int d = 0; d < g; ++d) key |= h.vidx[h.row_to_dist[r0 + d] + e] << (8 * d);
+                    const uint32_t w = e / 4, k = e % 4;
+                    const uint64_t c = vchunks[bi] + (uint64_t)w * 32 + t;
+                    L.vi[c * chunk + k] = (uint8_t)L.tuple_id[key];
+                }
+            } else {
+                for (int d = 0; d < g; ++d) {
+                    const uint32_t rd = h.row_to_dist[r0 + d];
+                    for (uint32_t e = 0; e < ne; ++e) {
+                        uint32_t w = e / 4, k = e % 4;
+                        uint64_t c = vchunks[bi] + ((uint64_t)w * g + d) * 32 + t;
+                        uint32_t v = h.vidx[rd + e];
+                        if (L.scaled) v *= (uint32_t)value_bytes;
+                        std::memcpy(&L.vi[c * chunk + k * vib], &v, vib);   // little-endian low bytes
+                    }
                 }
             }
             (void)words;
         }
     }
+    std::vector<int16_t>().swap(L.tuple_id);
+    L.offset_set = OffsetSet();
 }
 
 void dv_extract_diag(const dv_csr_host &a, std::vector<double> &d) {

@@ -10,6 +10,7 @@
 #include <memory>
 #include <stdexcept>
 #include <string>
+#include <climits>
 #include <vector>
 
 // ---------------------------------------------------------------------------
@@ -130,10 +131,43 @@ struct DuviHost {   // host copy of the SoA encoding (export / parity)
 //   value-index chunk (w, d)  at vi[v_base + (w*group + d)*32 + t]  (row d of the group, 4 entries)
 //   block start b of lane t   at cols[c_base + b*32 + t]      (leader row)
 // The canonical SoA stays on the device (export, Gauss-Seidel, SpMM).
+// Set of at most 256 int64 keys (open addressing); find returns the insertion rank.
+struct OffsetSet {
+    static constexpr int kSlots = 2048;
+    std::vector<int64_t> slot_key = std::vector<int64_t>(kSlots, INT64_MIN);
+    std::vector<int16_t> slot_id = std::vector<int16_t>(kSlots, -1);
+    std::vector<int64_t> keys;
+    static int h(int64_t k) { return (int)(((uint64_t)k * 0x9E3779B97F4A7C15ull) >> 53); }
+    bool insert(int64_t k) {   // false when a 257th key arrives
+        for (int i = h(k);; i = (i + 1) & (kSlots - 1)) {
+            if (slot_key[i] == k) return true;
+            if (slot_key[i] == INT64_MIN) {
+                if (keys.size() == 256) return false;
+                slot_key[i] = k;
+                slot_id[i] = (int16_t)keys.size();
+                keys.push_back(k);
+                return true;
+            }
+        }
+    }
+    int find(int64_t k) const {
+        for (int i = h(k);; i = (i + 1) & (kSlots - 1)) {
+            if (slot_key[i] == k) return slot_id[i];
+            if (slot_key[i] == INT64_MIN) return -1;
+        }
+    }
+};
+
 struct DuviLanesHost {
     int group = 1;
     int scaled = 0;                // 1: value-index bytes hold index * value size (byte offsets into the table)
     int shift = 0;                 // 1: row d of a group reads columns of the leader row + d
+    int tuples = 0;                // 1: one 8-bit tuple index per node-entry (tuple_vi: g value indices per tuple)
+    std::vector<uint32_t> tuple_vi;
+    std::vector<int16_t> tuple_id; // build-time map from packed value indices to tuple numbers
+    int stencil = 0;               // 1: entry bytes index `offsets` (column - first row of the group); no column list
+    std::vector<int32_t> offsets;
+    OffsetSet offset_set;
     int64_t ngroups = 0, nbundles = 0;
     std::vector<uint32_t> meta;    // per bundle: d_base, v_base, c_base, words, blocks
     std::vector<uint32_t> dist;    // leader entry bytes, 4 per word: 255 at a block start, else gap - 1
@@ -162,6 +196,12 @@ struct dv_matrix {
     int lanes_group = 1;
     int lanes_scaled = 0;
     int lanes_shift = 0;
+    int lanes_tuples = 0;      // node-tuple mode: lanes_tup holds 4 values (padded) per tuple
+    DevMem lanes_tup;
+    int32_t lanes_ntup = 0;
+    int lanes_stencil = 0;     // stencil mode: lanes_off holds the column offsets (int32)
+    DevMem lanes_off;
+    int32_t lanes_noff = 0;
     int64_t lanes_bundles = 0, lanes_groups = 0;
     DevMem lanes_meta, lanes_dist, lanes_vi, lanes_cols, lanes_nent;
     int64_t lanes_bytes = 0;   // bytes one product reads from the lane layout
@@ -182,7 +222,7 @@ constexpr int kBundleBlocks = 480;    // block column starts (+ alignment slack)
 // Host helpers (dv_host.cpp)
 void dv_encode_duvi(const dv_csr_host &a, double tol, int force_bits, DuviHost &out);
 void dv_make_bundles(const DuviHost &h, int32_t n_rows, int vi_bits, std::vector<int32_t> &bundles);
-void dv_build_duvi_lanes(const DuviHost &h, int32_t n_rows, int value_bytes, DuviLanesHost &out);
+void dv_build_duvi_lanes(const DuviHost &h, int32_t n_rows, int32_t n_cols, int value_bytes, DuviLanesHost &out);
 void dv_extract_diag(const dv_csr_host &a, std::vector<double> &diag);
 // CSR transpose (rows sorted by column of the input).
 void dv_csr_transpose(const dv_csr_host &a, std::vector<int32_t> &rp, std::vector<int32_t> &ci, std::vector<double> &va);

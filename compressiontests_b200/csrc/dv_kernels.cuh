@@ -493,10 +493,25 @@ struct DuviLanesArgs {
     const uint32_t *__restrict__ cols;
     const uint32_t *__restrict__ nent;
     const void *__restrict__ values;
+    const void *__restrict__ tuples;   // node-tuple mode: 4 values per tuple
+    const int32_t *__restrict__ offsets;   // stencil mode: column - first row of the group
     int64_t ngroups;
     int32_t nbundles;
     int32_t nuniq;
+    int32_t ntup;
+    int32_t noff;
 };
+
+// the (up to) 3 row values of a node tuple: one 16-byte shared load (FP32) or two (FP64)
+__device__ __forceinline__ void tup_get(const float *t, uint32_t idx, float (&v)[4]) {
+    const float4 q = reinterpret_cast<const float4 *>(t)[idx];
+    v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+}
+__device__ __forceinline__ void tup_get(const double *t, uint32_t idx, double (&v)[4]) {
+    const double2 *p = reinterpret_cast<const double2 *>(t) + 2 * idx;
+    const double2 a = p[0], b = p[1];
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
 
 template <class AT, bool SCALED, bool SMEM, class Chunk>
 __device__ __forceinline__ AT lane_value(const AT *tab, const AT *gtab, const Chunk &c, int k) {
@@ -506,15 +521,23 @@ __device__ __forceinline__ AT lane_value(const AT *tab, const AT *gtab, const Ch
     else return __ldg(gtab + idx);
 }
 
-template <class VI, class AT, class Gather, class Op, int G, bool SCALED, bool SHIFT>
+template <class VI, class AT, class Gather, class Op, int G, bool SCALED, bool SHIFT, bool TUP, bool STEN>
 __global__ void __launch_bounds__(256) k_duvi_lanes(DuviLanesArgs A, Gather g, Op op, const int *__restrict__ done,
                                                     double *partials, unsigned *ticket) {
     if (done && *(volatile const int *)done) return;
     using Chunk = typename ViChunk<VI>::T;
     constexpr bool kSmemTable = sizeof(VI) == 1;
-    __shared__ AT tab[kSmemTable ? 256 : 1];
+    constexpr int NV = TUP ? 1 : G;   // index chunks per word
+    __shared__ __align__(16) AT tab[TUP ? 1024 : (kSmemTable ? 256 : 1)];
     const AT *gtab = static_cast<const AT *>(A.values);
-    if (kSmemTable) {
+    __shared__ int32_t soff[STEN ? 256 : 1];
+    if constexpr (STEN)
+        for (int i = threadIdx.x; i < A.noff; i += blockDim.x) soff[i] = A.offsets[i];
+    if constexpr (TUP) {
+        const AT *tg = static_cast<const AT *>(A.tuples);
+        for (int i = threadIdx.x; i < 4 * A.ntup; i += blockDim.x) tab[i] = tg[i];
+        __syncthreads();
+    } else if (kSmemTable) {
         for (int i = threadIdx.x; i < A.nuniq; i += blockDim.x) tab[i] = gtab[i];
         __syncthreads();
     }
@@ -541,28 +564,30 @@ __global__ void __launch_bounds__(256) k_duvi_lanes(DuviLanesArgs A, Gather g, O
         uint32_t c = 0;
         // register double buffer: the streams of word w+1 are in flight while word w is decoded
         uint32_t dw_next = 0;
-        Chunk vw_next[G];
+        Chunk vw_next[NV];
         if (words > 0) {
             dw_next = __ldcs(dp);
 #pragma unroll
-            for (int d = 0; d < G; ++d) vw_next[d] = __ldcs(vp + (size_t)d * 32);
+            for (int d = 0; d < NV; ++d) vw_next[d] = __ldcs(vp + (size_t)d * 32);
         }
         for (uint32_t w = 0; w < words; ++w) {
             const uint32_t dw = dw_next;
-            Chunk vw[G];
+            Chunk vw[NV];
 #pragma unroll
-            for (int d = 0; d < G; ++d) vw[d] = vw_next[d];
+            for (int d = 0; d < NV; ++d) vw[d] = vw_next[d];
             if (w + 1 < words) {
                 dw_next = __ldcs(dp + (size_t)(w + 1) * 32);
 #pragma unroll
-                for (int d = 0; d < G; ++d) vw_next[d] = __ldcs(vp + ((size_t)(w + 1) * G + d) * 32);
+                for (int d = 0; d < NV; ++d) vw_next[d] = __ldcs(vp + ((size_t)(w + 1) * NV + d) * 32);
             }
             if (w < full) {
                 uint32_t cols[4];
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
                     const uint32_t byte = __byte_perm(dw, 0u, 0x4440u + (unsigned)k);
-                    if (byte == 255u) {
+                    if constexpr (STEN) {
+                        c = (uint32_t)(r0 + soff[byte]);
+                    } else if (byte == 255u) {
                         c = __ldcs(cp);
                         cp += 32;
                     } else {
@@ -577,19 +602,27 @@ __global__ void __launch_bounds__(256) k_duvi_lanes(DuviLanesArgs A, Gather g, O
 #pragma unroll
                         for (int d = 0; d < G; ++d) xs[k][d] = g(cols[k] + (uint32_t)d);
 #pragma unroll
-                    for (int k = 0; k < 4; ++k)
+                    for (int k = 0; k < 4; ++k) {
+                        AT tv[4];
+                        if constexpr (TUP) tup_get(tab, vi_get(vw[0], k), tv);
 #pragma unroll
                         for (int d = 0; d < G; ++d)
-                            s[d] = madd<AT>(s[d], lane_value<AT, SCALED, kSmemTable>(tab, gtab, vw[d], k), xs[k][d]);
+                            s[d] = madd<AT>(s[d], TUP ? tv[d] : lane_value<AT, SCALED, kSmemTable>(tab, gtab, vw[TUP ? 0 : d], k),
+                                            xs[k][d]);
+                    }
                 } else {
                     AT xv[4];
 #pragma unroll
                     for (int k = 0; k < 4; ++k) xv[k] = g(cols[k]);
 #pragma unroll
-                    for (int k = 0; k < 4; ++k)
+                    for (int k = 0; k < 4; ++k) {
+                        AT tv[4];
+                        if constexpr (TUP) tup_get(tab, vi_get(vw[0], k), tv);
 #pragma unroll
                         for (int d = 0; d < G; ++d)
-                            s[d] = madd<AT>(s[d], lane_value<AT, SCALED, kSmemTable>(tab, gtab, vw[d], k), xv[k]);
+                            s[d] = madd<AT>(s[d], TUP ? tv[d] : lane_value<AT, SCALED, kSmemTable>(tab, gtab, vw[TUP ? 0 : d], k),
+                                            xv[k]);
+                    }
                 }
             } else if (w * 4 < ne) {   // the lane's last, partial word
                 uint32_t cols[4];
@@ -597,7 +630,9 @@ __global__ void __launch_bounds__(256) k_duvi_lanes(DuviLanesArgs A, Gather g, O
                 for (int k = 0; k < 4; ++k) {
                     const uint32_t byte = __byte_perm(dw, 0u, 0x4440u + (unsigned)k);
                     if (w * 4 + k < ne) {
-                        if (byte == 255u) {
+                        if constexpr (STEN) {
+                            c = (uint32_t)(r0 + soff[byte]);
+                        } else if (byte == 255u) {
                             c = __ldcs(cp);
                             cp += 32;
                         } else {
@@ -610,9 +645,11 @@ __global__ void __launch_bounds__(256) k_duvi_lanes(DuviLanesArgs A, Gather g, O
                 for (int k = 0; k < 4; ++k) {
                     if (w * 4 + k < ne) {
                         const AT x0 = SHIFT ? AT(0) : g(cols[k]);
+                        AT tv[4];
+                        if constexpr (TUP) tup_get(tab, vi_get(vw[0], k), tv);
 #pragma unroll
                         for (int d = 0; d < G; ++d)
-                            s[d] = madd<AT>(s[d], lane_value<AT, SCALED, kSmemTable>(tab, gtab, vw[d], k),
+                            s[d] = madd<AT>(s[d], TUP ? tv[d] : lane_value<AT, SCALED, kSmemTable>(tab, gtab, vw[TUP ? 0 : d], k),
                                             SHIFT ? g(cols[k] + (uint32_t)d) : x0);
                     }
                 }
@@ -638,27 +675,38 @@ void launch_duvi_lanes_g(const LaunchEnv &e, const dv_matrix *m, Gather g, Op op
     a.cols = m->lanes_cols.as<uint32_t>();
     a.nent = m->lanes_nent.as<uint32_t>();
     a.values = m->values.p;
+    a.tuples = m->lanes_tup.p;
+    a.offsets = m->lanes_off.as<int32_t>();
+    a.noff = m->lanes_noff;
     a.ngroups = m->lanes_groups;
     a.nbundles = (int32_t)m->lanes_bundles;
     a.nuniq = (int32_t)m->nuniq;
+    a.ntup = m->lanes_ntup;
     int blocks = (int)((m->lanes_bundles + 7) / 8);
     if (blocks > e.max_blocks) blocks = e.max_blocks;
     if (blocks < 1) blocks = 1;
+    const bool sh = G > 1 && m->lanes_shift;
     bool done_launch = false;
     if constexpr (sizeof(VI) == 1) {
-        if (m->lanes_scaled) {
-            if (G > 1 && m->lanes_shift)
-                k_duvi_lanes<VI, AT, Gather, Op, G, true, G != 1><<<blocks, 256, 0, e.stream>>>(a, g, op, e.done, e.partials, e.ticket);
-            else
-                k_duvi_lanes<VI, AT, Gather, Op, G, true, false><<<blocks, 256, 0, e.stream>>>(a, g, op, e.done, e.partials, e.ticket);
+        if constexpr (G > 1) {
+            if (m->lanes_stencil) {
+                k_duvi_lanes<VI, AT, Gather, Op, G, false, false, true, true><<<blocks, 256, 0, e.stream>>>(a, g, op, e.done, e.partials, e.ticket);
+                done_launch = true;
+            } else if (m->lanes_tuples) {
+                if (sh) k_duvi_lanes<VI, AT, Gather, Op, G, false, true, true, false><<<blocks, 256, 0, e.stream>>>(a, g, op, e.done, e.partials, e.ticket);
+                else k_duvi_lanes<VI, AT, Gather, Op, G, false, false, true, false><<<blocks, 256, 0, e.stream>>>(a, g, op, e.done, e.partials, e.ticket);
+                done_launch = true;
+            }
+        }
+        if (!done_launch && m->lanes_scaled) {
+            if (sh) k_duvi_lanes<VI, AT, Gather, Op, G, true, G != 1, false, false><<<blocks, 256, 0, e.stream>>>(a, g, op, e.done, e.partials, e.ticket);
+            else k_duvi_lanes<VI, AT, Gather, Op, G, true, false, false, false><<<blocks, 256, 0, e.stream>>>(a, g, op, e.done, e.partials, e.ticket);
             done_launch = true;
         }
     }
     if (!done_launch) {
-        if (G > 1 && m->lanes_shift)
-            k_duvi_lanes<VI, AT, Gather, Op, G, false, G != 1><<<blocks, 256, 0, e.stream>>>(a, g, op, e.done, e.partials, e.ticket);
-        else
-            k_duvi_lanes<VI, AT, Gather, Op, G, false, false><<<blocks, 256, 0, e.stream>>>(a, g, op, e.done, e.partials, e.ticket);
+        if (sh) k_duvi_lanes<VI, AT, Gather, Op, G, false, G != 1, false, false><<<blocks, 256, 0, e.stream>>>(a, g, op, e.done, e.partials, e.ticket);
+        else k_duvi_lanes<VI, AT, Gather, Op, G, false, false, false, false><<<blocks, 256, 0, e.stream>>>(a, g, op, e.done, e.partials, e.ticket);
     }
     DV_CUDA(cudaGetLastError());
     e.ctx->count();

@@ -153,10 +153,34 @@ static void finish_duvi_upload(dv_matrix *m, cudaStream_t s) {
     }
     {   // lane-interleaved derived layout
         DuviLanesHost L;
-        dv_build_duvi_lanes(h, m->n_rows, m->precision == DV_F64 ? 8 : 4, L);
+        dv_build_duvi_lanes(h, m->n_rows, m->n_cols, m->precision == DV_F64 ? 8 : 4, L);
         m->lanes_group = L.group;
         m->lanes_scaled = L.scaled;
         m->lanes_shift = L.shift;
+        m->lanes_tuples = L.tuples;
+        m->lanes_stencil = L.stencil;
+        if (L.stencil) {
+            m->lanes_noff = (int32_t)L.offsets.size();
+            upload(m->lanes_off, L.offsets.data(), 4 * L.offsets.size(), s);
+            DV_CUDA(cudaStreamSynchronize(s));
+        }
+        if (L.tuples) {   // 4 values (zero-padded) per tuple, in the matrix precision
+            const size_t ntup = L.tuple_vi.size() / L.group;
+            if (m->precision == DV_F64) {
+                std::vector<double> tv(4 * ntup, 0.0);
+                for (size_t t = 0; t < ntup; ++t)
+                    for (int d = 0; d < L.group; ++d) tv[4 * t + d] = h.values[L.tuple_vi[t * L.group + d]];
+                upload(m->lanes_tup, tv.data(), 8 * tv.size(), s);
+                DV_CUDA(cudaStreamSynchronize(s));
+            } else {
+                std::vector<float> tv(4 * ntup, 0.0f);
+                for (size_t t = 0; t < ntup; ++t)
+                    for (int d = 0; d < L.group; ++d) tv[4 * t + d] = (float)h.values[L.tuple_vi[t * L.group + d]];
+                upload(m->lanes_tup, tv.data(), 4 * tv.size(), s);
+                DV_CUDA(cudaStreamSynchronize(s));
+            }
+            m->lanes_ntup = (int32_t)ntup;
+        }
         m->row_group = L.shift ? 1 : L.group;   // block products need identical columns
         m->lanes_groups = L.ngroups;
         m->lanes_bundles = L.nbundles;
@@ -168,7 +192,8 @@ static void finish_duvi_upload(dv_matrix *m, cudaStream_t s) {
         DV_CUDA(cudaStreamSynchronize(s));
         const size_t vs = m->precision == DV_F64 ? 8 : 4;
         m->lanes_bytes = (int64_t)(4 * L.meta.size() + 4 * L.dist.size() + L.vi.size() + 4 * L.cols.size() +
-                                   4 * L.nent.size() + vs * h.values.size());
+                                   4 * L.nent.size() + 4 * L.offsets.size() +
+                                   vs * (L.tuples ? 4 * (size_t)m->lanes_ntup : h.values.size()));
         // the lane kernel is the default when rows come in node groups
         m->duvi_variant = L.group > 1 ? 1 : 0;
     }

@@ -249,3 +249,33 @@ def test_transfer_products_shifted_groups_bit_exact(ctx, native, oracle, ne):
         np.testing.assert_array_equal(D.Multiply(x), oracle.DuVi(oracle.Csr.from_scipy(M)).spmv(x))
         F = native.SparseMatrix(ctx, M, "duvi", "f32")
         assert rowwise_rel(F.Multiply(x), M @ x, M, x) <= REL32
+
+
+@pytest.mark.parametrize("pool", [40, 200])
+def test_lane_kernel_node_tuples_and_fallback(ctx, native, oracle, rng, pool):
+    # 3-row node groups with 8-bit value indices: few distinct (v0, v1, v2) per node-entry
+    # (pool 40 of 2 patterns) use one tuple index per node-entry; random values from a pool
+    # of 200 give far more than 256 combinations and fall back to per-row indices.
+    n = 3 * 900
+    vals_pool = np.round(rng.standard_normal(pool), 6)
+    rows, cols, vals = [], [], []
+    for g in range(n // 3):
+        cs = sorted(set(((g * 3 + np.array([0, 3, 6, 150, 153, 600, 903])) % n).tolist()))
+        for d in range(3):
+            for j, c in enumerate(cs):
+                if pool == 40:
+                    v = vals_pool[(j + 7 * d + (g % 2)) % pool]
+                else:
+                    v = vals_pool[rng.integers(pool)]
+                rows.append(3 * g + d)
+                cols.append(c)
+                vals.append(v)
+    A = sp.csr_matrix((vals, (rows, cols)), shape=(n, n))
+    A.sort_indices()
+    M = native.SparseMatrix(ctx, A, "duvi", "f64", dedup_tol=0.0)
+    info = M.info()
+    assert info["kernel_variant"] == 103 and info["value_index_bits"] == 8
+    x = rng.standard_normal(n)
+    np.testing.assert_array_equal(M.Multiply(x), oracle.DuVi(oracle.Csr.from_scipy(A), 0.0).spmv(x))
+    F = native.SparseMatrix(ctx, A, "duvi", "f32", dedup_tol=0.0)
+    assert rowwise_rel(F.Multiply(x), A @ x, A, x) <= REL32
