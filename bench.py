@@ -394,7 +394,7 @@ def run_ours(args):
     if dom is not None:
         ms_dom, alg = dom
         achieved = alg / ms_dom / 1e6
-        roof = {"kernel": "k_duvi_lanes<u8,float,3> (DuVi FP32 node-group SpMV; fine-level Jacobi sweep body)",
+        roof = {"kernel": "k_duvi_lanes<u8,float,3,tuples,stencil> (DuVi FP32 node-group SpMV; fine-level Jacobi sweep body)",
                 "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 3), "traffic": ncu_traffic(), "peak_kind": peak_kind,
                 "algorithmic_bytes_per_launch": int(alg), "avg_launch_ms": round(ms_dom, 4)}
