@@ -52,7 +52,7 @@ METRIC = "MG-PCG time to 1e-8 rel. residual (mixed FP32/FP64, 128^3 hex elastici
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--size", type=int, default=128)
@@ -102,52 +102,73 @@ def barrier(ws):
 
 
 class ClockSampler:
-    """nvidia-smi samples of SM clock, power and throttle reasons during the timed region."""
+    """nvidia-smi samples (every 50 ms) of SM clock, power and throttle reasons.
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
-         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-         "clocks_event_reasons.sw_power_cap")
+    start() launches the sampler before the warm-up so it is running when the timed region
+    begins; mark() / unmark() bracket the timed region; stop() keeps the samples whose
+    timestamps fall inside it (with 60 ms of slack either side)."""
+
+    Q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, device):
         self.device = device
         self.proc = None
         self.path = os.path.join("/tmp", f"bench_clocks_{os.getpid()}.csv")
+        self.t0 = self.t1 = None
 
     def start(self):
         try:
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                          "--format=csv,noheader,nounits", "-lms", "50"], stdout=self.f,
                                          stderr=subprocess.DEVNULL)
+            time.sleep(0.5)   # let the sampler come up before the timed region
         except Exception:
             self.proc = None
 
+    def mark(self):
+        import datetime
+        self.t0 = datetime.datetime.now()
+
+    def unmark(self):
+        import datetime
+        self.t1 = datetime.datetime.now()
+
     def stop(self):
+        import datetime
         if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        time.sleep(0.1)
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
         except Exception:
             self.proc.kill()
         self.f.close()
+        slack = datetime.timedelta(milliseconds=60)
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in open(self.path):
             parts = [p.strip() for p in line.split(",")]
-            if len(parts) < 9:
+            if len(parts) < 10:
                 continue
             try:
-                sm.append(float(parts[1]))
-                smax = float(parts[2])
+                ts = datetime.datetime.strptime(parts[0], "%Y/%m/%d %H:%M:%S.%f")
+                clk, cmax = float(parts[2]), float(parts[3])
             except ValueError:
                 continue
-            for n, v in zip(names, parts[5:9]):
+            if self.t0 is not None and self.t1 is not None and not (self.t0 - slack <= ts <= self.t1 + slack):
+                continue
+            sm.append(clk)
+            smax = cmax
+            for n, v in zip(names, parts[6:10]):
                 if v.lower().startswith("active"):
                     reasons.add(n)
         os.unlink(self.path)
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "interval_ms": 50}
 
 
 def measured_peaks():
@@ -313,14 +334,15 @@ def run_ours(args):
 
     def timed(solver, steps, warmup):
         st = None
+        sampler = ClockSampler(local)
+        sampler.start()
         for _ in range(warmup):
             st = solver.solve_device(db.data_ptr(), dx.data_ptr())
         barrier(ws)
         torch.cuda.synchronize()
         ctx.synchronize()
         l0 = ctx.launch_count()
-        sampler = ClockSampler(local)
-        sampler.start()
+        sampler.mark()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         its, rel = [], []
@@ -331,6 +353,7 @@ def run_ours(args):
             assert st.HasConverged, st
         e1.record(stream)
         e1.synchronize()
+        sampler.unmark()
         clocks = sampler.stop()
         launches = ctx.launch_count() - l0
         ms = e0.elapsed_time(e1) / steps
@@ -370,7 +393,7 @@ def run_ours(args):
     if not args.no_fp64 and extras:
         for fmt in ("csr", "duvi"):
             s = make("f64", fmt)
-            ms, its, rel, _, _ = timed(s, max(2, args.steps // 2), 1)
+            ms, its, rel, _, _ = timed(s, max(2, min(5, args.steps // 2)), 1)
             fp64[fmt] = {"ms": round(ms, 2), "iterations": its[-1], "rel_residual": rel[-1],
                          "mixed_speedup": round(ms / ms_mixed, 2)}
             s.release()
@@ -402,12 +425,12 @@ def run_ours(args):
     batched = None
     if not args.no_batched and extras:
         batched = {"load_cases": batched_multi_rhs(cb, ctx, stream, args.batch_size, args.batch_k,
-                                                   max(1, args.steps // 2), args.tol),
-                   "meshes": batched_meshes(cb, ctx, stream, args.batch_meshes, max(1, args.steps // 2), args.tol)}
+                                                   max(1, min(5, args.steps // 2)), args.tol),
+                   "meshes": batched_meshes(cb, ctx, stream, args.batch_meshes, max(1, min(5, args.steps // 2)), args.tol)}
 
     adjoint = None
     if not args.no_adjoint and extras:
-        adjoint = adjoint_section(cb, ctx, stream, max(1, args.steps // 2), 1e-10)
+        adjoint = adjoint_section(cb, ctx, stream, max(1, min(5, args.steps // 2)), 1e-10)
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
