@@ -392,6 +392,72 @@ void dv_build_duvi_lanes(const DuviHost &h, int32_t n, int32_t n_cols, int value
     L.offset_set = OffsetSet();
 }
 
+void dv_build_duvi_patterns(const DuviHost &h, int32_t n, int32_t n_cols, int g, int max_patterns, int max_entries,
+                            DuviPatternHost &P) {
+    P = DuviPatternHost();
+    if (n_cols != n || g < 1 || n % g != 0 || n == 0) return;
+    // group signature: entry count, then per entry the column offset and the g value indices
+    const int64_t ngroups = n / g;
+    std::vector<uint64_t> sig(ngroups);
+    auto entries = [&](int64_t gi, std::vector<int64_t> &out) {
+        out.clear();
+        const int32_t r0 = (int32_t)(gi * g);
+        const uint32_t ne = h.row_to_dist[r0 + 1] - h.row_to_dist[r0];
+        walk_lane_blocks(h, r0, [&](uint32_t e, uint32_t c, bool, uint32_t) {
+            out.push_back((int64_t)c - r0);
+            for (int d = 0; d < g; ++d) out.push_back(h.vidx[h.row_to_dist[r0 + d] + e]);
+        });
+        (void)ne;
+    };
+#pragma omp parallel
+    {
+        std::vector<int64_t> buf;
+#pragma omp for schedule(static)
+        for (int64_t gi = 0; gi < ngroups; ++gi) {
+            entries(gi, buf);
+            uint64_t x = 1469598103934665603ull ^ buf.size();
+            for (int64_t v : buf) x = (x ^ (uint64_t)v) * 1099511628211ull;
+            sig[gi] = x;
+        }
+    }
+    // first-occurrence numbering; equal hashes are confirmed entry by entry
+    std::vector<uint64_t> phash;
+    std::vector<std::vector<int64_t>> pent;
+    std::vector<int64_t> buf;
+    P.id.resize(ngroups);
+    for (int64_t gi = 0; gi < ngroups; ++gi) {
+        int found = -1;
+        for (size_t p = 0; p < phash.size(); ++p)
+            if (phash[p] == sig[gi]) {
+                entries(gi, buf);
+                if (buf == pent[p]) { found = (int)p; break; }
+            }
+        if (found < 0) {
+            if ((int)phash.size() == max_patterns) return;
+            entries(gi, buf);
+            phash.push_back(sig[gi]);
+            pent.push_back(buf);
+            found = (int)phash.size() - 1;
+        }
+        P.id[gi] = (uint16_t)found;
+    }
+    int64_t total = 0;
+    for (auto &e : pent) total += (int64_t)e.size() / (1 + g);
+    if (total > max_entries) return;
+    P.start.assign(1, 0);
+    for (auto &e : pent) {
+        const size_t m = e.size() / (1 + g);
+        for (size_t k = 0; k < m; ++k) {
+            P.off.push_back((int32_t)e[k * (1 + g)]);
+            for (int d = 0; d < g; ++d) P.vi.push_back((uint32_t)e[k * (1 + g) + 1 + d]);
+        }
+        P.start.push_back((uint32_t)P.off.size());
+    }
+    P.group = g;
+    P.ngroups = ngroups;
+    P.ok = 1;
+}
+
 void dv_extract_diag(const dv_csr_host &a, std::vector<double> &d) {
     d.assign(a.n_rows, 0.0);
 #pragma omp parallel for schedule(static)

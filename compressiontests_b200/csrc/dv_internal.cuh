@@ -192,13 +192,16 @@ struct dv_matrix {
     DevMem bundles;            // int32 row starts of row bundles (+ sentinel)
     int32_t nbundles = 0;
     int duvi_batch = 4;        // entries per gather batch in the decode loop (9 when most blocks hold 9)
-    int duvi_variant = 0;      // 0: shared-memory staged rows, 1: lane-interleaved groups (autotuned)
+    int duvi_variant = 0;      // 0: shared-memory staged rows, 1: lane-interleaved groups, 2: node patterns (autotuned)
     int lanes_group = 1;
     int lanes_scaled = 0;
     int lanes_shift = 0;
     int lanes_tuples = 0;      // node-tuple mode: lanes_tup holds 4 values (padded) per tuple
     DevMem lanes_tup;
     int32_t lanes_ntup = 0;
+    int pat_ok = 0;            // node-pattern layout available (duvi_variant 2)
+    DevMem pat_id, pat_start, pat_rec;   // u16 per group, u32 per pattern, records {off, values} per entry
+    int32_t pat_count = 0, pat_entries = 0, pat_maxlen = 0;
     int lanes_stencil = 0;     // stencil mode: lanes_off holds the column offsets (int32)
     DevMem lanes_off;
     int32_t lanes_noff = 0;
@@ -212,6 +215,24 @@ struct dv_matrix {
     std::vector<double> host_diag;
     int64_t device_bytes = 0;
 };
+
+// Node-pattern layout (derived, read-only): every group of g rows whose entry list
+// (column offsets from the group's first row, and the g value indices of each
+// entry) repeats elsewhere shares one pattern; the matrix is then one pattern id
+// per group plus a table of patterns.
+struct DuviPatternHost {
+    int ok = 0;
+    int group = 1;
+    int64_t ngroups = 0;
+    std::vector<uint16_t> id;        // pattern of each group
+    std::vector<uint32_t> start;     // first entry of each pattern (+ end)
+    std::vector<int32_t> off;        // column - first row of the group, per pattern entry
+    std::vector<uint32_t> vi;        // g value indices per pattern entry
+};
+// Builds the pattern layout when the operator is square, rows come in groups with
+// identical columns and at most max_patterns patterns of max_entries entries in all exist.
+void dv_build_duvi_patterns(const DuviHost &h, int32_t n_rows, int32_t n_cols, int group, int max_patterns,
+                            int max_entries, DuviPatternHost &out);
 
 // Row bundles for the staged DuVi kernel: at most kBundleRows rows and at most
 // kBundleBytes entry bytes / kBundleBlocks blocks (a longer single row forms its own bundle).

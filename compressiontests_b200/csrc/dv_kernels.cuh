@@ -8,6 +8,8 @@
 // pass over the matrix.
 #pragma once
 
+#include <cstddef>
+
 #include "dv_internal.cuh"
 
 #include <cuda_runtime.h>
@@ -720,6 +722,103 @@ void launch_duvi_lanes(const LaunchEnv &e, const dv_matrix *m, Gather g, Op op) 
 }
 
 
+// ---------------------------------------------------------------------------
+// DuVi node-pattern kernel (derived layout, see DuviPatternHost)
+//
+// One thread per node group.  The group's pattern id selects a run of records
+// {column offset from the group's first row, the G row values} staged in shared
+// memory; the thread gathers x at each offset and applies it to its G rows,
+// summing every row in its entry order (FP64 results equal the reference walk
+// bit for bit).  The matrix costs 2 bytes per group in DRAM; the product is
+// bound by the x gathers.
+// ---------------------------------------------------------------------------
+template <class AT>
+struct alignas(16) PatRec {
+    int32_t off;
+    AT v[3];
+};
+static_assert(sizeof(PatRec<float>) == 16 && offsetof(PatRec<float>, v) == 4, "FP32 pattern record layout");
+static_assert(sizeof(PatRec<double>) == 32 && offsetof(PatRec<double>, v) == 8, "FP64 pattern record layout");
+
+template <class AT, class Gather, class Op, int G>
+__global__ void __launch_bounds__(256) k_duvi_pattern(const uint16_t *__restrict__ pid, const uint32_t *__restrict__ pstart,
+                                                      const PatRec<AT> *__restrict__ grec, int32_t npat, int32_t nrec,
+                                                      int64_t ngroups, Gather g, Op op, const int *__restrict__ done,
+                                                      double *partials, unsigned *ticket) {
+    if (done && *(volatile const int *)done) return;
+    extern __shared__ uint4 pat_smem[];
+    PatRec<AT> *rec = reinterpret_cast<PatRec<AT> *>(pat_smem);
+    uint32_t *st = reinterpret_cast<uint32_t *>(rec + nrec);
+    {
+        const uint4 *src = reinterpret_cast<const uint4 *>(grec);
+        const int n16 = nrec * (int)(sizeof(PatRec<AT>) / 16);
+        for (int i = threadIdx.x; i < n16; i += blockDim.x) pat_smem[i] = __ldg(src + i);
+        for (int i = threadIdx.x; i <= npat; i += blockDim.x) st[i] = __ldg(pstart + i);
+    }
+    __syncthreads();
+    double red[Op::NRED > 0 ? Op::NRED : 1];
+#pragma unroll
+    for (int i = 0; i < (Op::NRED > 0 ? Op::NRED : 1); ++i) red[i] = 0.0;
+    for (int64_t gi = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; gi < ngroups; gi += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t p = __ldg(pid + gi);
+        const uint32_t b = st[p], e = st[p + 1];
+        const int32_t r0 = (int32_t)(gi * G);
+        AT s[G];
+#pragma unroll
+        for (int d = 0; d < G; ++d) s[d] = op.init(r0 + d);
+        uint32_t k = b;
+        for (; k + 4 <= e; k += 4) {
+            PatRec<AT> q[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) q[u] = rec[k + u];
+            AT x[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) x[u] = g((uint32_t)(r0 + q[u].off));
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int d = 0; d < G; ++d) s[d] = madd<AT>(s[d], q[u].v[d], x[u]);
+        }
+        for (; k < e; ++k) {
+            const PatRec<AT> q = rec[k];
+            const AT x = g((uint32_t)(r0 + q.off));
+#pragma unroll
+            for (int d = 0; d < G; ++d) s[d] = madd<AT>(s[d], q.v[d], x);
+        }
+#pragma unroll
+        for (int d = 0; d < G; ++d) op.row(r0 + d, s[d], red);
+    }
+    if constexpr (Op::NRED > 0) {
+        double tot[Op::NRED];
+        if (grid_reduce<Op::NRED, Op::MAXMASK>(red, partials, ticket, tot)) op.finish(tot);
+    }
+}
+
+template <class AT, class Gather, class Op, int G>
+void launch_duvi_pattern_g(const LaunchEnv &e, const dv_matrix *m, Gather g, Op op) {
+    auto kern = k_duvi_pattern<AT, Gather, Op, G>;
+    const size_t smem = sizeof(PatRec<AT>) * (size_t)m->pat_entries + 4 * ((size_t)m->pat_count + 1);
+    static size_t attr_set = 0;   // per instantiation: largest size enabled so far
+    if (smem > 48 * 1024 && smem > attr_set) {
+        DV_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr_set = smem;
+    }
+    const int64_t ng = m->n_rows / G;
+    int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((ng + 255) / 256, e.max_blocks));
+    kern<<<blocks, 256, smem, e.stream>>>(m->pat_id.as<uint16_t>(), m->pat_start.as<uint32_t>(),
+                                          static_cast<const PatRec<AT> *>(m->pat_rec.p), m->pat_count, m->pat_entries,
+                                          ng, g, op, e.done, e.partials, e.ticket);
+    DV_CUDA(cudaGetLastError());
+    e.ctx->count();
+}
+
+template <class AT, class Gather, class Op>
+void launch_duvi_pattern(const LaunchEnv &e, const dv_matrix *m, Gather g, Op op) {
+    if (m->lanes_group == 3) launch_duvi_pattern_g<AT, Gather, Op, 3>(e, m, g, op);
+    else if (m->lanes_group == 2) launch_duvi_pattern_g<AT, Gather, Op, 2>(e, m, g, op);
+    else launch_duvi_pattern_g<AT, Gather, Op, 1>(e, m, g, op);
+}
+
 template <class VI, class AT, class Gather, class Op, int BATCH>
 void launch_duvi_vi(const LaunchEnv &e, const dv_matrix *m, Gather g, Op op) {
     constexpr int W = sizeof(VI) == 4 ? kDuviWarps32 : kDuviWarps;
@@ -764,6 +863,10 @@ void launch_csr_tpr(const LaunchEnv &e, const dv_matrix *m, Gather g, Op op) {
 // Runs op over every row of m with the accumulator type AT (= value precision).
 template <class AT, class Gather, class Op>
 void launch_rows(const LaunchEnv &e, const dv_matrix *m, Gather g, Op op) {
+    if (m->format == DV_FORMAT_DUVI && m->duvi_variant == 2) {
+        launch_duvi_pattern<AT>(e, m, g, op);
+        return;
+    }
     if (m->format == DV_FORMAT_DUVI && m->duvi_variant == 1) {
         if (m->vi_bits == 8) launch_duvi_lanes<uint8_t, AT>(e, m, g, op);
         else if (m->vi_bits == 16) launch_duvi_lanes<uint16_t, AT>(e, m, g, op);

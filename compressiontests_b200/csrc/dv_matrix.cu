@@ -196,6 +196,33 @@ static void finish_duvi_upload(dv_matrix *m, cudaStream_t s) {
                                    vs * (L.tuples ? 4 * (size_t)m->lanes_ntup : h.values.size()));
         // the lane kernel is the default when rows come in node groups
         m->duvi_variant = L.group > 1 ? 1 : 0;
+        const char *pe = getenv("DV_PATTERNS");   // DV_PATTERNS=0 keeps the lane layout (A/B comparisons)
+        if (!L.shift && !(pe && pe[0] == '0')) {   // node patterns: records {offset, 3 values} in shared memory
+            const int rec_bytes = m->precision == DV_F64 ? 32 : 16;
+            DuviPatternHost P;
+            dv_build_duvi_patterns(h, m->n_rows, m->n_cols, L.group, 1024, (96 * 1024) / rec_bytes, P);
+            if (P.ok) {
+                const size_t ne = P.off.size();
+                std::vector<unsigned char> recs(ne * rec_bytes, 0);
+                for (size_t k = 0; k < ne; ++k) {
+                    unsigned char *r = recs.data() + k * rec_bytes;
+                    std::memcpy(r, &P.off[k], 4);
+                    for (int d = 0; d < P.group; ++d) {
+                        const double v = h.values[P.vi[k * P.group + d]];
+                        if (m->precision == DV_F64) std::memcpy(r + 8 + 8 * d, &v, 8);
+                        else { const float f = (float)v; std::memcpy(r + 4 + 4 * d, &f, 4); }
+                    }
+                }
+                upload(m->pat_id, P.id.data(), 2 * P.id.size(), s);
+                upload(m->pat_start, P.start.data(), 4 * P.start.size(), s);
+                upload(m->pat_rec, recs.data(), recs.size(), s);
+                DV_CUDA(cudaStreamSynchronize(s));
+                m->pat_ok = 1;
+                m->pat_count = (int32_t)P.start.size() - 1;
+                m->pat_entries = (int32_t)ne;
+                m->duvi_variant = 2;
+            }
+        }
     }
     std::vector<int32_t> b;
     dv_make_bundles(h, m->n_rows, m->vi_bits, b);
@@ -245,13 +272,18 @@ static void autotune(dv_matrix *m) {
     };
     // CSR: threads per row; DuVi: 4 / 9 = staged kernel with that batch width, 100 = lane kernel
     std::vector<int> cand = m->format == DV_FORMAT_CSR ? std::vector<int>{8, 16, 32} : std::vector<int>{4, 9, 100};
+    if (m->format == DV_FORMAT_DUVI && m->pat_ok) cand.push_back(200);
     cudaEvent_t e0, e1;
     DV_CUDA(cudaEventCreate(&e0));
     DV_CUDA(cudaEventCreate(&e1));
     float best = 1e30f;
-    auto current = [&] { return m->format == DV_FORMAT_CSR ? m->csr_tpr : (m->duvi_variant == 1 ? 100 : m->duvi_batch); };
+    auto current = [&] {
+        return m->format == DV_FORMAT_CSR ? m->csr_tpr
+                                          : (m->duvi_variant == 2 ? 200 : m->duvi_variant == 1 ? 100 : m->duvi_batch);
+    };
     auto apply = [&](int v) {
         if (m->format == DV_FORMAT_CSR) m->csr_tpr = v;
+        else if (v == 200) m->duvi_variant = 2;
         else if (v == 100) m->duvi_variant = 1;
         else { m->duvi_variant = 0; m->duvi_batch = v; }
     };
@@ -400,7 +432,8 @@ extern "C" DV_API int dv_matrix_get_info(const dv_matrix *m, dv_matrix_info *inf
         info->precision = m->precision;
         info->value_index_bits = m->format == DV_FORMAT_DUVI ? m->vi_bits : 0;
         info->kernel_variant = m->format == DV_FORMAT_CSR ? m->csr_tpr
-                               : (m->duvi_variant == 1 ? 100 + m->lanes_group : m->duvi_batch);
+                               : (m->duvi_variant == 2 ? 200 + m->lanes_group
+                                  : m->duvi_variant == 1 ? 100 + m->lanes_group : m->duvi_batch);
         info->device_bytes = m->device_bytes;
         info->row_group = m->row_group;
         info->reserved = 0;

@@ -252,7 +252,7 @@ def test_transfer_products_shifted_groups_bit_exact(ctx, native, oracle, ne):
 
 
 @pytest.mark.parametrize("pool", [40, 200])
-def test_lane_kernel_node_tuples_and_fallback(ctx, native, oracle, rng, pool):
+def test_lane_kernel_node_tuples_and_fallback(ctx, native, oracle, rng, pool, monkeypatch):
     # 3-row node groups with 8-bit value indices: few distinct (v0, v1, v2) per node-entry
     # (pool 40 of 2 patterns) use one tuple index per node-entry; random values from a pool
     # of 200 give far more than 256 combinations and fall back to per-row indices.
@@ -272,10 +272,33 @@ def test_lane_kernel_node_tuples_and_fallback(ctx, native, oracle, rng, pool):
                 vals.append(v)
     A = sp.csr_matrix((vals, (rows, cols)), shape=(n, n))
     A.sort_indices()
+    monkeypatch.setenv("DV_PATTERNS", "0")   # the repeating case would otherwise take the node-pattern kernel
     M = native.SparseMatrix(ctx, A, "duvi", "f64", dedup_tol=0.0)
     info = M.info()
     assert info["kernel_variant"] == 103 and info["value_index_bits"] == 8
     x = rng.standard_normal(n)
     np.testing.assert_array_equal(M.Multiply(x), oracle.DuVi(oracle.Csr.from_scipy(A), 0.0).spmv(x))
     F = native.SparseMatrix(ctx, A, "duvi", "f32", dedup_tol=0.0)
+    assert rowwise_rel(F.Multiply(x), A @ x, A, x) <= REL32
+
+
+
+@pytest.mark.parametrize("ne", [(8, 8, 8), (16, 4, 4), (7, 5, 9)])
+@pytest.mark.parametrize("patterns", ["1", "0"])
+def test_hex_operator_pattern_and_lane_kernels_bit_exact(ctx, native, oracle, rng, ne, patterns, monkeypatch):
+    # The hex stiffness repeats one entry list per node class (interior, faces, edges,
+    # corners): with patterns on, one pattern id per node and a shared-memory pattern
+    # table (variant 203); with them off, the lane layout with stencil offsets and node
+    # tuples (variant 103).  Both sum every row in storage order: bit-exact in FP64.
+    monkeypatch.setenv("DV_PATTERNS", patterns)
+    A = native.hex_stiffness(ne)
+    x = rng.standard_normal(A.shape[1])
+    ref = oracle.DuVi(oracle.Csr.from_scipy(A)).spmv(x)
+    M = native.SparseMatrix(ctx, A, "duvi", "f64")
+    assert M.info()["kernel_variant"] == (203 if patterns == "1" else 103)
+    np.testing.assert_array_equal(M.Multiply(x), ref)
+    y0 = rng.standard_normal(A.shape[0])
+    np.testing.assert_array_equal(M.Multiply(x, y0.copy(), clear=False),
+                                  oracle.DuVi(oracle.Csr.from_scipy(A)).spmv(x, y0.copy(), clear=False))
+    F = native.SparseMatrix(ctx, A, "duvi", "f32")
     assert rowwise_rel(F.Multiply(x), A @ x, A, x) <= REL32
