@@ -392,23 +392,29 @@ void dv_build_duvi_lanes(const DuviHost &h, int32_t n, int32_t n_cols, int value
     L.offset_set = OffsetSet();
 }
 
-void dv_build_duvi_patterns(const DuviHost &h, int32_t n, int32_t n_cols, int g, int max_patterns, int max_entries,
-                            DuviPatternHost &P) {
+void dv_build_duvi_patterns(const DuviHost &h, int32_t n, int32_t n_cols, int g, int shift, int max_patterns,
+                            int max_entries, DuviPatternHost &P) {
     P = DuviPatternHost();
-    if (n_cols != n || g < 1 || n % g != 0 || n == 0) return;
+    if (g < 1 || n % g != 0 || n == 0) return;
+    const bool based = shift || n_cols != n;
     // group signature: entry count, then per entry the column offset and the g value indices
     const int64_t ngroups = n / g;
     std::vector<uint64_t> sig(ngroups);
+    if (based) P.base.assign(ngroups, 0);
     auto entries = [&](int64_t gi, std::vector<int64_t> &out) {
         out.clear();
         const int32_t r0 = (int32_t)(gi * g);
-        const uint32_t ne = h.row_to_dist[r0 + 1] - h.row_to_dist[r0];
+        const int64_t b0 = based ? (int64_t)(h.row_to_col[r0 + 1] > h.row_to_col[r0] ? h.col_idx[h.row_to_col[r0]] : 0) : r0;
         walk_lane_blocks(h, r0, [&](uint32_t e, uint32_t c, bool, uint32_t) {
-            out.push_back((int64_t)c - r0);
+            out.push_back((int64_t)c - b0);
             for (int d = 0; d < g; ++d) out.push_back(h.vidx[h.row_to_dist[r0 + d] + e]);
         });
-        (void)ne;
     };
+    if (based)
+        for (int64_t gi = 0; gi < ngroups; ++gi) {
+            const int32_t r0 = (int32_t)(gi * g);
+            if (h.row_to_col[r0 + 1] > h.row_to_col[r0]) P.base[gi] = h.col_idx[h.row_to_col[r0]];
+        }
 #pragma omp parallel
     {
         std::vector<int64_t> buf;
@@ -454,6 +460,8 @@ void dv_build_duvi_patterns(const DuviHost &h, int32_t n, int32_t n_cols, int g,
         P.start.push_back((uint32_t)P.off.size());
     }
     P.group = g;
+    P.shift = shift;
+    P.based = based ? 1 : 0;
     P.ngroups = ngroups;
     P.ok = 1;
 }

@@ -201,6 +201,8 @@ struct dv_matrix {
     int32_t lanes_ntup = 0;
     int pat_ok = 0;            // node-pattern layout available (duvi_variant 2)
     DevMem pat_id, pat_start, pat_rec;   // u16 per group, u32 per pattern, records {off, values} per entry
+    DevMem pat_base;                     // u32 first column per group (based patterns)
+    int pat_based = 0, pat_shift = 0;
     int32_t pat_count = 0, pat_entries = 0, pat_maxlen = 0;
     int lanes_stencil = 0;     // stencil mode: lanes_off holds the column offsets (int32)
     DevMem lanes_off;
@@ -223,16 +225,21 @@ struct dv_matrix {
 struct DuviPatternHost {
     int ok = 0;
     int group = 1;
+    int shift = 0;                   // 1: row d of a group reads columns + d
+    int based = 0;                   // 1: offsets are from the group's first column (stored in base)
     int64_t ngroups = 0;
     std::vector<uint16_t> id;        // pattern of each group
+    std::vector<uint32_t> base;      // first column of each group (based only)
     std::vector<uint32_t> start;     // first entry of each pattern (+ end)
     std::vector<int32_t> off;        // column - first row of the group, per pattern entry
     std::vector<uint32_t> vi;        // g value indices per pattern entry
 };
-// Builds the pattern layout when the operator is square, rows come in groups with
-// identical columns and at most max_patterns patterns of max_entries entries in all exist.
-void dv_build_duvi_patterns(const DuviHost &h, int32_t n_rows, int32_t n_cols, int group, int max_patterns,
-                            int max_entries, DuviPatternHost &out);
+// Builds the pattern layout for rows in groups of `group` (identical or, with shift,
+// shifted columns) when at most max_patterns patterns of max_entries entries in all
+// exist.  Square operators without shift take offsets from the group's first row;
+// otherwise from the group's first column, which is stored per group.
+void dv_build_duvi_patterns(const DuviHost &h, int32_t n_rows, int32_t n_cols, int group, int shift,
+                            int max_patterns, int max_entries, DuviPatternHost &out);
 
 // Row bundles for the staged DuVi kernel: at most kBundleRows rows and at most
 // kBundleBytes entry bytes / kBundleBlocks blocks (a longer single row forms its own bundle).

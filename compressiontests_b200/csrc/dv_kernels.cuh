@@ -740,11 +740,13 @@ struct alignas(16) PatRec {
 static_assert(sizeof(PatRec<float>) == 16 && offsetof(PatRec<float>, v) == 4, "FP32 pattern record layout");
 static_assert(sizeof(PatRec<double>) == 32 && offsetof(PatRec<double>, v) == 8, "FP64 pattern record layout");
 
-template <class AT, class Gather, class Op, int G>
+// BASED: offsets from the group's first column (base[]), else from its first row;
+// SHIFT: row d of the group reads column + d.
+template <class AT, class Gather, class Op, int G, bool BASED, bool SHIFT>
 __global__ void __launch_bounds__(256) k_duvi_pattern(const uint16_t *__restrict__ pid, const uint32_t *__restrict__ pstart,
-                                                      const PatRec<AT> *__restrict__ grec, int32_t npat, int32_t nrec,
-                                                      int64_t ngroups, Gather g, Op op, const int *__restrict__ done,
-                                                      double *partials, unsigned *ticket) {
+                                                      const PatRec<AT> *__restrict__ grec, const uint32_t *__restrict__ base,
+                                                      int32_t npat, int32_t nrec, int64_t ngroups, Gather g, Op op,
+                                                      const int *__restrict__ done, double *partials, unsigned *ticket) {
     if (done && *(volatile const int *)done) return;
     extern __shared__ uint4 pat_smem[];
     PatRec<AT> *rec = reinterpret_cast<PatRec<AT> *>(pat_smem);
@@ -763,6 +765,7 @@ __global__ void __launch_bounds__(256) k_duvi_pattern(const uint16_t *__restrict
         const uint32_t p = __ldg(pid + gi);
         const uint32_t b = st[p], e = st[p + 1];
         const int32_t r0 = (int32_t)(gi * G);
+        const int32_t c0 = BASED ? (int32_t)__ldg(base + gi) : r0;
         AT s[G];
 #pragma unroll
         for (int d = 0; d < G; ++d) s[d] = op.init(r0 + d);
@@ -771,19 +774,30 @@ __global__ void __launch_bounds__(256) k_duvi_pattern(const uint16_t *__restrict
             PatRec<AT> q[4];
 #pragma unroll
             for (int u = 0; u < 4; ++u) q[u] = rec[k + u];
-            AT x[4];
+            if constexpr (SHIFT) {
+                AT x[4][G];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) x[u] = g((uint32_t)(r0 + q[u].off));
+                for (int u = 0; u < 4; ++u)
 #pragma unroll
-            for (int u = 0; u < 4; ++u)
+                    for (int d = 0; d < G; ++d) x[u][d] = g((uint32_t)(c0 + q[u].off + d));
 #pragma unroll
-                for (int d = 0; d < G; ++d) s[d] = madd<AT>(s[d], q[u].v[d], x[u]);
+                for (int u = 0; u < 4; ++u)
+#pragma unroll
+                    for (int d = 0; d < G; ++d) s[d] = madd<AT>(s[d], q[u].v[d], x[u][d]);
+            } else {
+                AT x[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) x[u] = g((uint32_t)(c0 + q[u].off));
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+#pragma unroll
+                    for (int d = 0; d < G; ++d) s[d] = madd<AT>(s[d], q[u].v[d], x[u]);
+            }
         }
         for (; k < e; ++k) {
             const PatRec<AT> q = rec[k];
-            const AT x = g((uint32_t)(r0 + q.off));
 #pragma unroll
-            for (int d = 0; d < G; ++d) s[d] = madd<AT>(s[d], q.v[d], x);
+            for (int d = 0; d < G; ++d) s[d] = madd<AT>(s[d], q.v[d], g((uint32_t)(c0 + q.off + (SHIFT ? d : 0))));
         }
 #pragma unroll
         for (int d = 0; d < G; ++d) op.row(r0 + d, s[d], red);
@@ -794,22 +808,31 @@ __global__ void __launch_bounds__(256) k_duvi_pattern(const uint16_t *__restrict
     }
 }
 
-template <class AT, class Gather, class Op, int G>
-void launch_duvi_pattern_g(const LaunchEnv &e, const dv_matrix *m, Gather g, Op op) {
-    auto kern = k_duvi_pattern<AT, Gather, Op, G>;
+template <class AT, class Gather, class Op, int G, bool BASED, bool SHIFT>
+void launch_duvi_pattern_gbs(const LaunchEnv &e, const dv_matrix *m, Gather g, Op op) {
+    auto kern = k_duvi_pattern<AT, Gather, Op, G, BASED, SHIFT>;
     const size_t smem = sizeof(PatRec<AT>) * (size_t)m->pat_entries + 4 * ((size_t)m->pat_count + 1);
+    // Raise the kernel's dynamic shared-memory limit to every new largest size: epilogues
+    // that reduce add static shared memory, so even tables under 48 KB can need it.
     static size_t attr_set = 0;   // per instantiation: largest size enabled so far
-    if (smem > 48 * 1024 && smem > attr_set) {
+    if (smem > attr_set) {
         DV_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         attr_set = smem;
     }
     const int64_t ng = m->n_rows / G;
     int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((ng + 255) / 256, e.max_blocks));
     kern<<<blocks, 256, smem, e.stream>>>(m->pat_id.as<uint16_t>(), m->pat_start.as<uint32_t>(),
-                                          static_cast<const PatRec<AT> *>(m->pat_rec.p), m->pat_count, m->pat_entries,
-                                          ng, g, op, e.done, e.partials, e.ticket);
+                                          static_cast<const PatRec<AT> *>(m->pat_rec.p), m->pat_base.as<uint32_t>(),
+                                          m->pat_count, m->pat_entries, ng, g, op, e.done, e.partials, e.ticket);
     DV_CUDA(cudaGetLastError());
     e.ctx->count();
+}
+
+template <class AT, class Gather, class Op, int G>
+void launch_duvi_pattern_g(const LaunchEnv &e, const dv_matrix *m, Gather g, Op op) {
+    if (!m->pat_based) launch_duvi_pattern_gbs<AT, Gather, Op, G, false, false>(e, m, g, op);
+    else if (G > 1 && m->pat_shift) launch_duvi_pattern_gbs<AT, Gather, Op, G, true, (G > 1)>(e, m, g, op);
+    else launch_duvi_pattern_gbs<AT, Gather, Op, G, true, false>(e, m, g, op);
 }
 
 template <class AT, class Gather, class Op>

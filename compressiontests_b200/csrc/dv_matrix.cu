@@ -197,10 +197,10 @@ static void finish_duvi_upload(dv_matrix *m, cudaStream_t s) {
         // the lane kernel is the default when rows come in node groups
         m->duvi_variant = L.group > 1 ? 1 : 0;
         const char *pe = getenv("DV_PATTERNS");   // DV_PATTERNS=0 keeps the lane layout (A/B comparisons)
-        if (!L.shift && !(pe && pe[0] == '0')) {   // node patterns: records {offset, 3 values} in shared memory
+        if (!(pe && pe[0] == '0')) {   // node patterns: records {offset, 3 values} in shared memory
             const int rec_bytes = m->precision == DV_F64 ? 32 : 16;
             DuviPatternHost P;
-            dv_build_duvi_patterns(h, m->n_rows, m->n_cols, L.group, 1024, (96 * 1024) / rec_bytes, P);
+            dv_build_duvi_patterns(h, m->n_rows, m->n_cols, L.group, L.shift, 1024, (96 * 1024) / rec_bytes, P);
             if (P.ok) {
                 const size_t ne = P.off.size();
                 std::vector<unsigned char> recs(ne * rec_bytes, 0);
@@ -216,8 +216,11 @@ static void finish_duvi_upload(dv_matrix *m, cudaStream_t s) {
                 upload(m->pat_id, P.id.data(), 2 * P.id.size(), s);
                 upload(m->pat_start, P.start.data(), 4 * P.start.size(), s);
                 upload(m->pat_rec, recs.data(), recs.size(), s);
+                if (P.based) upload(m->pat_base, P.base.data(), 4 * P.base.size(), s);
                 DV_CUDA(cudaStreamSynchronize(s));
                 m->pat_ok = 1;
+                m->pat_based = P.based;
+                m->pat_shift = P.shift;
                 m->pat_count = (int32_t)P.start.size() - 1;
                 m->pat_entries = (int32_t)ne;
                 m->duvi_variant = 2;

@@ -225,3 +225,18 @@ def test_batch_rejects_gauss_seidel(ctx, native):
     A, P = native.hex_hierarchy((8, 8, 8), coarse_ne=4)
     with pytest.raises(native.NotImplementedFeatureError):
         native.BatchedMultigridSolver(ctx, [(A, P)], smoother="gs_color")
+
+
+def test_mgpcg_on_uneven_galerkin_meshes(ctx, native):
+    # Uneven cantilevers (odd edges, Galerkin levels): node-pattern tables of every size,
+    # including ones just under the default shared-memory limit, with reducing epilogues
+    # (the power method at set-up) and plain ones.
+    for ne in ((29, 25, 19), (19, 35, 15), (46, 29, 9)):
+        A, P = native.galerkin_hierarchy(ne, max_coarse_dofs=1000)
+        b = native.traction_rhs(ne)
+        for prec in ("mixed", "f64"):
+            s = native.MultigridPcgSolver(ctx, A, P, precision=prec, fmt="duvi", tol=1e-8, max_iterations=300)
+            x, st = s.Solve(b)
+            assert st.HasConverged, (ne, prec)
+            assert np.linalg.norm(b - A[0] @ x) / np.linalg.norm(b) <= 1e-8
+            s.release()

@@ -237,14 +237,18 @@ def test_lane_kernel_gaps_of_256_inside_blocks(ctx, native, oracle, prec):
 
 
 @pytest.mark.parametrize("ne", [(8, 6, 6), (7, 9, 5)])
-def test_transfer_products_shifted_groups_bit_exact(ctx, native, oracle, ne):
+@pytest.mark.parametrize("patterns", ["1", "0"])
+def test_transfer_products_shifted_groups_bit_exact(ctx, native, oracle, ne, patterns, monkeypatch):
     # Trilinear P and R = P^T: the 3 rows of a node read columns shifted by the dof
-    # component, which the lane layout stores once per node (shifted groups).
+    # component.  With patterns on, each node stores its first column and a pattern id
+    # (offsets from that column; variant 203); with them off, the lane layout keeps the
+    # shifted groups once per node (variant 103).
+    monkeypatch.setenv("DV_PATTERNS", patterns)
     P = native.hex_trilinear(ne)
     for M in (P, P.T.tocsr()):
         M.sort_indices()
         D = native.SparseMatrix(ctx, M, "duvi", "f64")
-        assert D.info()["kernel_variant"] == 103
+        assert D.info()["kernel_variant"] == (203 if patterns == "1" else 103)
         x = np.random.default_rng(5).standard_normal(M.shape[1])
         np.testing.assert_array_equal(D.Multiply(x), oracle.DuVi(oracle.Csr.from_scipy(M)).spmv(x))
         F = native.SparseMatrix(ctx, M, "duvi", "f32")
