@@ -378,9 +378,115 @@ void launch_bprod_gu(const LaunchEnv &e, const dv_matrix *m, int kc, Gather g, E
 }
 
 // Y-epilogue product over kc <= kMaxCols columns; the matrix's values have type AT.
+// Block product on the node-pattern layout (dvk::PatRec records staged in shared
+// memory): one warp per node group, every record one broadcast shared load, lanes
+// gather their right-hand-side columns.  No decode at all.  BASED: offsets from the
+// group's first column (base[]); SHIFT: row d reads column + d.
+template <class AT, int G, int U, bool EXACT, bool BASED, bool SHIFT, class Gather, class Epi>
+__global__ void __launch_bounds__(kThreads) k_bprod_pattern(const uint16_t *__restrict__ pid,
+                                                            const uint32_t *__restrict__ pstart,
+                                                            const dvk::PatRec<AT> *__restrict__ grec,
+                                                            const uint32_t *__restrict__ base, int32_t npat,
+                                                            int32_t nrec, int32_t ngroups, int kc, Gather g, Epi ep,
+                                                            const int *__restrict__ done, double *partials,
+                                                            unsigned *ticket) {
+    if (done && *(volatile const int *)done) return;
+    extern __shared__ uint4 bpat_smem[];
+    dvk::PatRec<AT> *rec = reinterpret_cast<dvk::PatRec<AT> *>(bpat_smem);
+    uint32_t *st = reinterpret_cast<uint32_t *>(rec + nrec);
+    {
+        const uint4 *src = reinterpret_cast<const uint4 *>(grec);
+        const int n16 = nrec * (int)(sizeof(dvk::PatRec<AT>) / 16);
+        for (int i = threadIdx.x; i < n16; i += blockDim.x) bpat_smem[i] = __ldg(src + i);
+        for (int i = threadIdx.x; i <= npat; i += blockDim.x) st[i] = __ldg(pstart + i);
+    }
+    __syncthreads();
+    constexpr int NC = Epi::NC > 0 ? Epi::NC : 1;
+    double red[U][NC];
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+#pragma unroll
+        for (int c = 0; c < NC; ++c) red[u][c] = 0.0;
+    const int lane = threadIdx.x & 31;
+    const int32_t nw = (gridDim.x * blockDim.x) >> 5;
+    for (int32_t grp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; grp < ngroups; grp += nw) {
+        const uint32_t p = __ldg(pid + grp);
+        const uint32_t b = st[p], e = st[p + 1];
+        const int32_t r0 = grp * G;
+        const uint32_t c0 = BASED ? __ldg(base + grp) : (uint32_t)r0;
+        AT acc[G][U];
+#pragma unroll
+        for (int t = 0; t < G; ++t)
+#pragma unroll
+            for (int u = 0; u < U; ++u) acc[t][u] = AT(0);
+#pragma unroll 2
+        for (uint32_t k = b; k < e; ++k) {
+            const dvk::PatRec<AT> q = rec[k];
+            const uint32_t c = c0 + (uint32_t)q.off;
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int j = lane + 32 * u;
+                if (j < kc) {
+                    if constexpr (SHIFT) {
+#pragma unroll
+                        for (int t = 0; t < G; ++t) {
+                            const AT x = g(c + (uint32_t)t, j);
+                            acc[t][u] = EXACT ? madd<AT>(acc[t][u], q.v[t], x) : fma(q.v[t], x, acc[t][u]);
+                        }
+                    } else {
+                        const AT x = g(c, j);
+#pragma unroll
+                        for (int t = 0; t < G; ++t)
+                            acc[t][u] = EXACT ? madd<AT>(acc[t][u], q.v[t], x) : fma(q.v[t], x, acc[t][u]);
+                    }
+                }
+            }
+        }
+        group_epilogue<AT, G, U>(r0, kc, lane, ep, acc, red);
+    }
+    if constexpr (Epi::NC > 0) col_reduce<Epi::NC, U>(red, kc, partials, ticket, ep.fin);
+}
+
+template <class AT, int U, bool EXACT, bool BASED, bool SHIFT, class Gather, class Epi>
+void launch_bprod_pattern_u(const LaunchEnv &e, const dv_matrix *m, int kc, Gather g, Epi ep) {
+    constexpr int G = 3;
+    auto kern = k_bprod_pattern<AT, G, U, EXACT, BASED, SHIFT, Gather, Epi>;
+    const size_t smem = sizeof(dvk::PatRec<AT>) * (size_t)m->pat_entries + 4 * ((size_t)m->pat_count + 1);
+    static size_t attr_set = 0;   // per instantiation: largest size enabled so far
+    if (smem > attr_set) {
+        DV_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr_set = smem;
+    }
+    const int32_t ngroups = m->n_rows / G;
+    const int blocks = bprod_blocks(e, ngroups, Epi::NC > 0);
+    kern<<<blocks, kThreads, smem, e.stream>>>(m->pat_id.as<uint16_t>(), m->pat_start.as<uint32_t>(),
+                                               static_cast<const dvk::PatRec<AT> *>(m->pat_rec.p),
+                                               m->pat_base.as<uint32_t>(), m->pat_count, m->pat_entries, ngroups, kc,
+                                               g, ep, e.done, e.partials, e.ticket);
+    DV_CUDA(cudaGetLastError());
+    e.ctx->count();
+}
+
+template <class AT, bool EXACT, bool BASED, bool SHIFT, class Gather, class Epi>
+void launch_bprod_pattern(const LaunchEnv &e, const dv_matrix *m, int kc, Gather g, Epi ep) {
+    if (kc <= 32) launch_bprod_pattern_u<AT, 1, EXACT, BASED, SHIFT>(e, m, kc, g, ep);
+    else if (kc <= 64) launch_bprod_pattern_u<AT, 2, EXACT, BASED, SHIFT>(e, m, kc, g, ep);
+    else launch_bprod_pattern_u<AT, 4, EXACT, BASED, SHIFT>(e, m, kc, g, ep);
+}
+
 template <class AT, bool EXACT = true, class Gather, class Epi>
 void launch_bprod(const LaunchEnv &e, const dv_matrix *m, int kc, Gather g, Epi ep) {
     DV_REQUIRE(kc >= 1 && kc <= kMaxCols, DV_ERR_ARG, "block product of more than 128 columns");
+    if (m->format == DV_FORMAT_DUVI && m->pat_ok && m->lanes_group == 3) {   // node patterns, 3-row groups
+        if (!m->pat_based && !m->pat_shift) {
+            launch_bprod_pattern<AT, EXACT, false, false>(e, m, kc, g, ep);
+            return;
+        }
+        if (m->pat_based && m->pat_shift) {
+            launch_bprod_pattern<AT, EXACT, true, true>(e, m, kc, g, ep);
+            return;
+        }
+    }
     const bool g3 = m->row_group == 3;
     if (kc <= 32) {
         if (g3) launch_bprod_gu<AT, 3, 1, EXACT>(e, m, kc, g, ep);

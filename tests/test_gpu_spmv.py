@@ -306,3 +306,19 @@ def test_hex_operator_pattern_and_lane_kernels_bit_exact(ctx, native, oracle, rn
                                   oracle.DuVi(oracle.Csr.from_scipy(A)).spmv(x, y0.copy(), clear=False))
     F = native.SparseMatrix(ctx, A, "duvi", "f32")
     assert rowwise_rel(F.Multiply(x), A @ x, A, x) <= REL32
+
+
+@pytest.mark.parametrize("k", [5, 40, 130])
+def test_spmm_transfers_bit_exact(ctx, native, oracle, rng, k):
+    # Block products of P and R = P^T on the node-pattern layout (offsets from each node's
+    # first column, row d reading column + d): every column equals the oracle's product.
+    P = native.hex_trilinear((8, 6, 6))
+    for M0 in (P, P.T.tocsr()):
+        M0.sort_indices()
+        M = native.SparseMatrix(ctx, M0, "duvi", "f64")
+        assert M.info()["kernel_variant"] == 203
+        X = rng.standard_normal((M0.shape[1], k))
+        Y = _spmm(native, M, X, np.float64)
+        ref = oracle.DuVi(oracle.Csr.from_scipy(M0))
+        for j in (0, k // 2, k - 1):
+            np.testing.assert_array_equal(Y[:, j], ref.spmv(X[:, j]))
