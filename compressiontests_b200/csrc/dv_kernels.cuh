@@ -138,6 +138,19 @@ __device__ __forceinline__ double madd<double>(double acc, double a, double b) {
 template <>
 __device__ __forceinline__ float madd<float>(float acc, float a, float b) { return fmaf(a, b, acc); }
 
+// Epilogues that set FUSED = true accept one fused multiply-add per term in FP64
+// (more accurate, half the FP64 operations); all others keep the reference's order
+// of a rounded product followed by a rounded add.
+template <class Op, class = void>
+struct op_fused : std::false_type {};
+template <class Op>
+struct op_fused<Op, std::void_t<decltype(Op::FUSED)>> : std::integral_constant<bool, Op::FUSED> {};
+template <class AT, bool FUSED>
+__device__ __forceinline__ AT madd_op(AT acc, AT a, AT b) {
+    if constexpr (FUSED) return fma(a, b, acc);
+    else return madd<AT>(acc, a, b);
+}
+
 // ---------------------------------------------------------------------------
 // epilogues (row operators).  Each has NRED reduction slots and MAXMASK.
 // ---------------------------------------------------------------------------
@@ -196,6 +209,34 @@ struct SolverScalars {
     int it, max_it, done, converged, failed, restart, cycle, pad;
 };
 
+// Last Jacobi sweep of the finest level with the flexible-CG dot products of its
+// result z fused in: z.q, z.r and beta = -(z.q)/(p.q) (0 on a restart), as k_fcg_red.
+template <class T>
+struct OpJacobiFcgRed {
+    static constexpr int NRED = 2;
+    static constexpr unsigned MAXMASK = 0;
+    const T *__restrict__ x;
+    const T *__restrict__ w;
+    const T *__restrict__ b;
+    T *__restrict__ y;
+    const double *__restrict__ q;
+    const double *__restrict__ r;
+    SolverScalars *sc;
+    __device__ __forceinline__ T init(int32_t) const { return T(0); }
+    __device__ __forceinline__ void row(int32_t i, T s, double *red) const {
+        const T z = x[i] + w[i] * (b[i] - s);
+        y[i] = z;
+        red[0] += (double)z * q[i];
+        red[1] += (double)z * r[i];
+    }
+    __device__ void finish(const double *t) const {
+        sc->zq = t[0];
+        sc->zr = t[1];
+        sc->beta = sc->restart ? 0.0 : -t[0] / sc->pq;
+        sc->restart = 0;
+    }
+};
+
 // PCG: Ap = A p and p.Ap; alpha = rz / pAp (dot_finalize_and_calc_a, CsrCG.cl:223-241).
 struct OpPcgAp {
     static constexpr int NRED = 1;
@@ -219,6 +260,7 @@ template <class ZT>
 struct OpFcg {
     static constexpr int NRED = 1;
     static constexpr unsigned MAXMASK = 0;
+    static constexpr bool FUSED = true;   // products may use fused multiply-adds (not a parity path)
     const ZT *__restrict__ z;
     double *__restrict__ p;
     double *__restrict__ q;
@@ -783,7 +825,7 @@ __global__ void __launch_bounds__(256) k_duvi_pattern(const uint16_t *__restrict
 #pragma unroll
                 for (int u = 0; u < 4; ++u)
 #pragma unroll
-                    for (int d = 0; d < G; ++d) s[d] = madd<AT>(s[d], q[u].v[d], x[u][d]);
+                    for (int d = 0; d < G; ++d) s[d] = madd_op<AT, op_fused<Op>::value>(s[d], q[u].v[d], x[u][d]);
             } else {
                 AT x[4];
 #pragma unroll
@@ -791,13 +833,13 @@ __global__ void __launch_bounds__(256) k_duvi_pattern(const uint16_t *__restrict
 #pragma unroll
                 for (int u = 0; u < 4; ++u)
 #pragma unroll
-                    for (int d = 0; d < G; ++d) s[d] = madd<AT>(s[d], q[u].v[d], x[u]);
+                    for (int d = 0; d < G; ++d) s[d] = madd_op<AT, op_fused<Op>::value>(s[d], q[u].v[d], x[u]);
             }
         }
         for (; k < e; ++k) {
             const PatRec<AT> q = rec[k];
 #pragma unroll
-            for (int d = 0; d < G; ++d) s[d] = madd<AT>(s[d], q.v[d], g((uint32_t)(c0 + q.off + (SHIFT ? d : 0))));
+            for (int d = 0; d < G; ++d) s[d] = madd_op<AT, op_fused<Op>::value>(s[d], q.v[d], g((uint32_t)(c0 + q.off + (SHIFT ? d : 0))));
         }
 #pragma unroll
         for (int d = 0; d < G; ++d) op.row(r0 + d, s[d], red);

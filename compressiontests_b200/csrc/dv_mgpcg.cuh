@@ -38,6 +38,12 @@ struct VCycle {
     int smoother = DV_SMOOTHER_JACOBI;
 
     // x_0 = V(b_0); returns the buffer that holds the result (level-0 x or t).
+    // Flexible-CG reduction fused into the finest level's last sweep (Jacobi only): set
+    // by the driver, consumed by level 0.
+    const double *fuse_q = nullptr, *fuse_r = nullptr;
+    SolverScalars *fuse_sc = nullptr;
+    bool fused_red() const { return fuse_sc != nullptr && smoother == DV_SMOOTHER_JACOBI; }
+
     T *run(const LaunchEnv &e, const T *b0) { return level(e, 0, b0); }
 
     T *level(const LaunchEnv &e, size_t l, const T *b) {
@@ -79,8 +85,13 @@ struct VCycle {
         opro.clear = 0;
         launch_rows<T>(e, L.P.get(), GatherVec<T, T>{xn}, opro);
         for (int k = 0; k < nu; ++k) {
-            OpJacobi<T> oj{{}, x, w, b, t};
-            launch_rows<T>(e, L.A.get(), GatherVec<T, T>{x}, oj);
+            if (l == 0 && k == nu - 1 && fused_red()) {
+                OpJacobiFcgRed<T> oj{x, w, b, t, fuse_q, fuse_r, fuse_sc};
+                launch_rows<T>(e, L.A.get(), GatherVec<T, T>{x}, oj);
+            } else {
+                OpJacobi<T> oj{{}, x, w, b, t};
+                launch_rows<T>(e, L.A.get(), GatherVec<T, T>{x}, oj);
+            }
             std::swap(x, t);
         }
         return x;

@@ -487,10 +487,12 @@ template <class T>
 static const T *fcg_step(dv_mgpcg *s, const LaunchEnv &e, VCycle<T> &vc, const T *z, T *rin) {
     cudaStream_t st = e.stream;
     const int g = grid_for(s->ctx, s->n);
-    k_fcg_red<T><<<g, kThreads, 0, st>>>(z, s->q.as<double>(), s->r.as<double>(), s->n, s->ws->sc(), e.done,
-                                         e.partials, e.ticket);
-    DV_CUDA(cudaGetLastError());
-    s->ctx->count();
+    if (!vc.fused_red()) {   // otherwise z.q, z.r and beta came with the V-cycle's last sweep
+        k_fcg_red<T><<<g, kThreads, 0, st>>>(z, s->q.as<double>(), s->r.as<double>(), s->n, s->ws->sc(), e.done,
+                                             e.partials, e.ticket);
+        DV_CUDA(cudaGetLastError());
+        s->ctx->count();
+    }
     OpFcg<T> op{z, s->p.as<double>(), s->q.as<double>(), s->ws->sc(), 0.0};
     launch_rows<double>(e, s->Aout.get(), GatherVec<T, double>{z}, op);
     T *rl = std::is_same<T, float>::value ? reinterpret_cast<T *>(s->r32.p) : nullptr;
@@ -521,6 +523,9 @@ static void mgpcg_solve_impl(dv_mgpcg *s, VCycle<T> &vc, dv_stats *stats) {
     h.pq = 1.0;
     ws.push();
     const int g = grid_for(ctx, n);
+    vc.fuse_q = s->q.as<double>();
+    vc.fuse_r = s->r.as<double>();
+    vc.fuse_sc = ws.sc();
     k_norm2<<<g, kThreads, 0, st>>>(s->b.as<double>(), n, ws.sc(), 0, e0.partials, e0.ticket);
     DV_CUDA(cudaGetLastError());
     ctx->count();
