@@ -424,6 +424,9 @@ def run_ours(args):
                 "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 3), "traffic": ncu_traffic(), "peak_kind": peak_kind,
                 "algorithmic_bytes_per_launch": int(alg), "avg_launch_ms": round(ms_dom, 4)}
+        if roof["traffic"]:   # the same time against the DRAM bytes the derived layout actually moves
+            roof["layout_achieved_GBps"] = round(roof["traffic"] / ms_dom / 1e6, 1)
+            roof["layout_frac"] = round(roof["layout_achieved_GBps"] / peak, 3)
 
     batched = None
     if not args.no_batched and extras:
