@@ -233,9 +233,10 @@ def spmv_table(cb, ctx, A0, reps, peak, cases=(("duvi", "f32"), ("duvi", "f64"),
         gbs = alg / ms / 1e6
         out[f"{fmt}_{prec}"] = {"ms": round(ms, 4), "algorithmic_bytes": int(alg), "GBps": round(gbs, 1),
                                 "frac_of_peak": round(gbs / peak, 3), "value_index_bits": info["value_index_bits"],
-                                "nblocks": info["nblocks"], "nuniq": info["nuniq"]}
+                                "nblocks": info["nblocks"], "nuniq": info["nuniq"],
+                                "launch_shape": info["kernel_variant"]}
         if fmt == "duvi" and prec == "f32":
-            dom = (ms, alg)
+            dom = (ms, alg, info["kernel_variant"])
         M.release()
         del x, y
         torch.cuda.empty_cache()
@@ -415,9 +416,10 @@ def run_ours(args):
         spmv["log_uniform_E"] = spmv_log_uniform(cb, ctx, 64, 20, peak)
     roof = None
     if dom is not None:
-        ms_dom, alg = dom
+        ms_dom, alg, shape = dom
         achieved = alg / ms_dom / 1e6
-        roof = {"kernel": "k_duvi_pattern<float,3> (DuVi FP32 node-pattern SpMV; fine-level Jacobi sweep body)",
+        kname = {203: "k_duvi_pattern<float,3>", 103: "k_duvi_lanes<float,3>"}.get(shape, f"launch shape {shape}")
+        roof = {"kernel": f"{kname} (DuVi FP32 node-pattern SpMV; fine-level Jacobi sweep body)",
                 "note": "achieved counts the DuVi SoA format bytes; the derived node-pattern layout reads x plus a "
                         "2-byte pattern id per node (traffic), so the kernel is bound by L1 gathers and shared-memory "
                         "record loads, not by HBM",

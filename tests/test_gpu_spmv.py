@@ -287,13 +287,14 @@ def test_lane_kernel_node_tuples_and_fallback(ctx, native, oracle, rng, pool, mo
 
 
 
-@pytest.mark.parametrize("ne", [(8, 8, 8), (16, 4, 4), (7, 5, 9)])
+@pytest.mark.parametrize("ne", [(8, 8, 8), (16, 4, 4), (7, 5, 9), (40, 21, 13)])
 @pytest.mark.parametrize("patterns", ["1", "0"])
 def test_hex_operator_pattern_and_lane_kernels_bit_exact(ctx, native, oracle, rng, ne, patterns, monkeypatch):
     # The hex stiffness repeats one entry list per node class (interior, faces, edges,
     # corners): with patterns on, one pattern id per node and a shared-memory pattern
     # table (variant 203); with them off, the lane layout with stencil offsets and node
     # tuples (variant 103).  Both sum every row in storage order: bit-exact in FP64.
+    # (40, 21, 13) spans many blocks of the grid-stride loop.
     monkeypatch.setenv("DV_PATTERNS", patterns)
     A = native.hex_stiffness(ne)
     x = rng.standard_normal(A.shape[1])
