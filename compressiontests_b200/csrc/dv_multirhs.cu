@@ -400,6 +400,7 @@ void multi_solve(dv_mgpcg *s, VCycle<T> &vc, MultiState<T> &M, int k, const doub
         DV_CUDA(cudaStreamSynchronize(st));
     };
     int refinements = 0;
+    bool verified = false;   // the last true_residual() was taken on the final iterate
     for (;;) {
         ws.run_chunk(body, s->cfg.use_graphs != 0, 0);
         DV_REQUIRE(zfinal == z, DV_ERR_ARG, "block V-cycle output buffer is not stable across iterations");
@@ -414,7 +415,10 @@ void multi_solve(dv_mgpcg *s, VCycle<T> &vc, MultiState<T> &M, int k, const doub
                 hc[j].converged = 0;
                 ++bad;
             }
-        if (bad == 0 || refinements >= kMaxRefinements || h.it >= h.max_it) break;
+        if (bad == 0 || refinements >= kMaxRefinements || h.it >= h.max_it) {
+            verified = true;
+            break;
+        }
         ++refinements;
         for (int j = 0; j < k; ++j) hc[j].restart = 1;   // every direction restarts from the new residual
         DV_CUDA(cudaMemcpyAsync(cs, hc.data(), sizeof(ColScalars) * k, cudaMemcpyHostToDevice, st));
@@ -425,8 +429,8 @@ void multi_solve(dv_mgpcg *s, VCycle<T> &vc, MultiState<T> &M, int k, const doub
         ws.push();
         z = block_vcycle<T>(ed, vc, M.W, 0, rin, k);
     }
-    // final FP64 true residual of every column
-    true_residual();
+    // final FP64 true residual of every column (already taken when the loop ended on a verification)
+    if (!verified) true_residual();
     DV_CUDA(cudaMemcpyAsync(dX, Xd, 8 * nk, cudaMemcpyDeviceToDevice, st));
     DV_CUDA(cudaStreamSynchronize(st));
     double worst = 0.0, worst_abs = 0.0;

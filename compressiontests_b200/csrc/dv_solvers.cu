@@ -29,7 +29,7 @@ SolverWs::SolverWs(dv_context *c) : ctx(c) {
     DV_CUDA(cudaMallocHost(&host_scal, sizeof(SolverScalars)));
 }
 SolverWs::~SolverWs() {
-    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    for (auto &c : chunks) cudaGraphExecDestroy(c.exec);
     if (host_scal) cudaFreeHost(host_scal);
 }
 LaunchEnv SolverWs::env(bool with_done) const {
@@ -50,15 +50,18 @@ void SolverWs::push() {
     DV_CUDA(cudaMemcpyAsync(scal.p, host_scal, sizeof(SolverScalars), cudaMemcpyHostToDevice, ctx->stream));
 }
 // Runs `body` once eagerly (first call: sets kernel attributes, validates) and
-// afterwards through a captured graph of the same launches.
-void SolverWs::run_chunk(const std::function<void()> &body, bool use_graph, int64_t launches_per_chunk) {
+// afterwards through the graph of the same launches captured for `key`.
+void SolverWs::run_chunk(const std::function<void()> &body, bool use_graph, int key) {
     cudaStream_t s = ctx->stream;
     if (!use_graph || !warmed) {
         body();
         warmed = true;
         return;
     }
-    if (!graph_exec) {
+    const Chunk *c = nullptr;
+    for (const auto &g : chunks)
+        if (g.key == key) c = &g;
+    if (!c) {
         cudaGraph_t g;
         int64_t before = ctx->launches;
         DV_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
@@ -69,14 +72,18 @@ void SolverWs::run_chunk(const std::function<void()> &body, bool use_graph, int6
             throw;
         }
         DV_CUDA(cudaStreamEndCapture(s, &g));
-        graph_launches = ctx->launches - before;
+        const int64_t launches = ctx->launches - before;
         ctx->launches = before;
-        DV_CUDA(cudaGraphInstantiate(&graph_exec, g, 0));
+        cudaGraphExec_t exec;
+        const cudaError_t err = cudaGraphInstantiate(&exec, g, 0);
         cudaGraphDestroy(g);
+        DV_CUDA(err);
+        chunks.push_back({key, exec, launches});
+        c = &chunks.back();
     }
-    DV_CUDA(cudaGraphLaunch(graph_exec, s));
-    ctx->count(graph_launches);
-    (void)launches_per_chunk;
+    DV_CUDA(cudaGraphLaunch(c->exec, s));
+    graph_launches = c->launches;
+    ctx->count(c->launches);
 }
 
 
@@ -503,6 +510,19 @@ static const T *fcg_step(dv_mgpcg *s, const LaunchEnv &e, VCycle<T> &vc, const T
     return vc.run(e, rin);
 }
 
+// Outer iterations to run before the next host read of the stop flag: as many as the
+// convergence rate of the last chunk (||r||^2 from r2_0 at iteration it_0 to r2 at it)
+// needs to bring ||r||^2 down to target, at least 1 and at most per.  Iterations after
+// convergence only launch kernels that return at once; a short last chunk avoids most
+// of them.  Without a measurable rate the chunk stays at per.
+static int next_chunk_length(int per, int it_0, double r2_0, int it, double r2, double target) {
+    if (per <= 1 || it <= it_0 || !(r2 > 0.0) || !(r2_0 > r2) || !(target > 0.0)) return per;
+    const double log_rate = std::log(r2 / r2_0) / (double)(it - it_0);   // < 0
+    const double need = std::log(target / r2) / log_rate;                // iterations left
+    if (!(need > 0.0)) return 1;
+    return (int)std::min<double>((double)per, std::max(1.0, std::ceil(need)));
+}
+
 template <class T>
 static void mgpcg_solve_impl(dv_mgpcg *s, VCycle<T> &vc, dv_stats *stats) {
     dv_context *ctx = s->ctx;
@@ -542,18 +562,27 @@ static void mgpcg_solve_impl(dv_mgpcg *s, VCycle<T> &vc, dv_stats *stats) {
     }
     const T *z = vc.run(ed, rin);
     const int per = s->cfg.iterations_per_sync > 0 ? s->cfg.iterations_per_sync : 4;
+    int len = per;   // outer iterations in the next chunk (one captured graph per length)
     const T *zfinal = z;
     auto body = [&] {
         const T *zz = z;
-        for (int k = 0; k < per; ++k) zz = fcg_step<T>(s, ed, vc, zz, rin);
+        for (int k = 0; k < len; ++k) zz = fcg_step<T>(s, ed, vc, zz, rin);
         zfinal = zz;
     };
     int refinements = 0;
+    bool verified = false;   // p = b - A x and rr already hold the final x's true residual
+    int it0 = 0;             // iteration count and ||r||^2 at the previous host read
+    double rr0 = -1.0;       // (-1: ||b||^2, known on the host after the first read)
     for (;;) {
-        ws.run_chunk(body, s->cfg.use_graphs != 0, 0);
+        ws.run_chunk(body, s->cfg.use_graphs != 0, len);
         DV_REQUIRE(zfinal == z, DV_ERR_ARG, "V-cycle output buffer is not stable across iterations");
         ws.pull();
-        if (!h.done) continue;
+        if (!h.done) {
+            len = next_chunk_length(per, it0, rr0 < 0 ? h.bb : rr0, h.it, h.rr, h.tol2 * h.bb);
+            it0 = h.it;
+            rr0 = h.rr;
+            continue;
+        }
         if (!h.converged) break;
         // FP64 verification of the true residual; restart from it if the
         // recurrence drifted (iterative refinement).
@@ -564,7 +593,7 @@ static void mgpcg_solve_impl(dv_mgpcg *s, VCycle<T> &vc, dv_stats *stats) {
         ctx->count();
         ws.pull();
         if (h.rr <= h.tol2 * h.bb || refinements >= 4 || h.it >= h.max_it) {
-            h.converged = h.rr <= h.tol2 * h.bb;
+            verified = true;
             break;
         }
         ++refinements;
@@ -579,15 +608,21 @@ static void mgpcg_solve_impl(dv_mgpcg *s, VCycle<T> &vc, dv_stats *stats) {
         h.restart = 1;
         ws.push();
         z = vc.run(ed, rin);
+        len = per;
+        it0 = h.it;
+        rr0 = h.rr;
     }
-    // final true residual (FP64)
-    OpResid<double> orr{{}, s->b.as<double>(), s->p.as<double>()};
-    launch_rows<double>(e0, s->Aout.get(), GatherVec<double, double>{s->x.as<double>()}, orr);
-    k_norm2<<<g, kThreads, 0, st>>>(s->p.as<double>(), n, ws.sc(), 1, e0.partials, e0.ticket);
-    DV_CUDA(cudaGetLastError());
-    ctx->count();
+    if (!verified) {   // final true residual (FP64) of a solve that stopped without converging
+        OpResid<double> orr{{}, s->b.as<double>(), s->p.as<double>()};
+        launch_rows<double>(e0, s->Aout.get(), GatherVec<double, double>{s->x.as<double>()}, orr);
+        k_norm2<<<g, kThreads, 0, st>>>(s->p.as<double>(), n, ws.sc(), 1, e0.partials, e0.ticket);
+        DV_CUDA(cudaGetLastError());
+        ctx->count();
+    }
     DV_CUDA(cudaEventRecord(ev1, st));
     ws.pull();
+    // converged: the recurrence stopped below the tolerance and the true residual confirms it
+    h.converged = h.converged && h.rr <= h.tol2 * h.bb;
     float ms = 0;
     cudaEventElapsedTime(&ms, ev0, ev1);
     cudaEventDestroy(ev0);

@@ -11,8 +11,13 @@ struct SolverWs {
     dv_context *ctx;
     DevMem red, scal;
     dvk::SolverScalars *host_scal = nullptr;
-    cudaGraphExec_t graph_exec = nullptr;
-    int64_t graph_launches = 0;
+    struct Chunk {
+        int key;
+        cudaGraphExec_t exec;
+        int64_t launches;
+    };
+    std::vector<Chunk> chunks;   // captured graphs, one per chunk key (e.g. iterations per chunk)
+    int64_t graph_launches = 0;  // launches of the graph run last
     bool warmed = false;
     explicit SolverWs(dv_context *c);
     ~SolverWs();
@@ -20,10 +25,12 @@ struct SolverWs {
     dvk::LaunchEnv env(bool with_done) const;
     void pull();   // device scalars -> host mirror (synchronises the stream)
     void push();   // host mirror -> device scalars (stream ordered)
-    void run_chunk(const std::function<void()> &body, bool use_graph, int64_t launches_per_chunk);
+    // Runs `body` (the same launches for the same key every time) eagerly on first use,
+    // afterwards through the graph captured for `key`.
+    void run_chunk(const std::function<void()> &body, bool use_graph, int key);
     void reset_graph() {
-        if (graph_exec) cudaGraphExecDestroy(graph_exec);
-        graph_exec = nullptr;
+        for (auto &c : chunks) cudaGraphExecDestroy(c.exec);
+        chunks.clear();
     }
 };
 

@@ -240,3 +240,23 @@ def test_mgpcg_on_uneven_galerkin_meshes(ctx, native):
             assert st.HasConverged, (ne, prec)
             assert np.linalg.norm(b - A[0] @ x) / np.linalg.norm(b) <= 1e-8
             s.release()
+
+
+def test_mgpcg_chunk_lengths_do_not_change_the_iterate(ctx, native):
+    # Outer iterations run in captured chunks whose length follows the convergence rate
+    # seen so far (at most iterations_per_sync); the host reads in between change nothing
+    # on the device, so every chunking gives the same iterate bit for bit.
+    ne = (16, 16, 16)
+    A, P = native.hex_hierarchy(ne, coarse_ne=4)
+    b = native.traction_rhs(ne)
+    out = []
+    for per in (1, 3, 4, 16):
+        s = native.MultigridPcgSolver(ctx, A, P, precision="mixed", fmt="duvi", tol=1e-8, iterations_per_sync=per)
+        for _ in range(3):   # the eager first chunk, then a captured graph per chunk length
+            x, st = s.Solve(b)
+            assert st.HasConverged
+            out.append((x, st.NumIterationsRequired))
+        s.release()
+    for x, it in out[1:]:
+        assert it == out[0][1]
+        np.testing.assert_array_equal(x, out[0][0])
