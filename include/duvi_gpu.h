@@ -222,7 +222,9 @@ typedef struct {
                                    radius estimate of D^-1 A per level */
     int32_t max_iterations;
     double tol;                 /* relative 2-norm */
-    int32_t iterations_per_sync;/* outer iterations per host convergence read (0 = 4) */
+    int32_t iterations_per_sync;/* most outer iterations per host convergence read (0 = 4); the single
+                                  right-hand-side solve shortens a chunk when the convergence rate so
+                                  far predicts the tolerance within it */
     int32_t use_graphs;         /* capture the iteration sequence in a CUDA graph */
     int32_t smoother;           /* DV_SMOOTHER_JACOBI (default, 0): weighted Jacobi as above;
                                    DV_SMOOTHER_GS_LEX: nu forward Gauss-Seidel sweeps before and after
