@@ -861,8 +861,24 @@ void launch_duvi_pattern_gbs(const LaunchEnv &e, const dv_matrix *m, Gather g, O
         DV_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         attr_set = smem;
     }
+    // Whole waves: past one wave of resident blocks (SMs x blocks per SM at this table size
+    // and register count), a multiple of it, so that the last wave is not a partial one.
+    static size_t occ_smem[4] = {};
+    static int occ_val[4] = {}, occ_next = 0;
+    int occ = 0;
+    for (int i = 0; i < 4; ++i)
+        if (occ_smem[i] == smem) occ = occ_val[i];
+    if (occ == 0) {
+        DV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 256, smem));
+        occ = std::max(occ, 1);
+        occ_smem[occ_next] = smem;
+        occ_val[occ_next] = occ;
+        occ_next = (occ_next + 1) % 4;
+    }
     const int64_t ng = m->n_rows / G;
-    int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((ng + 255) / 256, e.max_blocks));
+    const int64_t need = std::max<int64_t>(1, (ng + 255) / 256), wave = (int64_t)e.ctx->num_sms * occ;
+    const int64_t cap = std::min<int64_t>(need, e.max_blocks);
+    const int blocks = (int)(cap <= wave ? cap : cap / wave * wave);
     kern<<<blocks, 256, smem, e.stream>>>(m->pat_id.as<uint16_t>(), m->pat_start.as<uint32_t>(),
                                           static_cast<const PatRec<AT> *>(m->pat_rec.p), m->pat_base.as<uint32_t>(),
                                           m->pat_count, m->pat_entries, ng, g, op, e.done, e.partials, e.ticket);
