@@ -1,11 +1,10 @@
 // Jacobi PCG without any device allocation.
 //
 // Some callers cannot allocate device memory at the moment they need a
-// solve: code that records its own CUDA work into a graph (cudaMalloc and
-// cudaFree are not allowed while a stream is being captured, and cudaFree
-// also synchronises the whole device), and host applications that reserve
-// their device memory once at start-up and forbid allocations afterwards.
-// dv_pcg_solve_noalloc serves them: it runs the same kernels as dv_pcg_solve,
+// solve: host applications that reserve all their device memory once at
+// start-up (a pool owned by another allocator) and forbid allocations
+// afterwards, and time-critical loops that cannot afford cudaFree, which
+// synchronises the whole device.  dv_pcg_solve_noalloc serves them: it runs the same kernels as dv_pcg_solve,
 // but its work vectors (r, z, p, Ap), reduction partials and scalars live in
 // one file-scope device array of fixed size, so the call itself allocates
 // nothing.  The caller passes the matrix (already uploaded) and device

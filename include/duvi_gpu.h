@@ -188,10 +188,10 @@ DV_API int dv_pcg_solve(dv_pcg *p, const double *b, const double *x0, double *x,
 DV_API int dv_pcg_destroy(dv_pcg *p);
 
 /* Jacobi PCG that allocates nothing.  No counterpart in the reference: it is for
- * callers that cannot allocate device memory when they solve -- code recording
- * its own work into a CUDA graph (cudaMalloc/cudaFree are not allowed during
- * stream capture, and cudaFree synchronises the device) and hosts that reserve
- * all device memory up front.  Same algorithm and stop test as dv_pcg_solve; the
+ * callers that cannot allocate device memory when they solve -- hosts that
+ * reserve all device memory up front and forbid later allocations, and
+ * time-critical loops that cannot afford cudaFree's device-wide
+ * synchronisation.  Same algorithm and stop test as dv_pcg_solve; the
  * work vectors live in one fixed device array of this library (4,325,632 bytes
  * per device, held until the process exits), which limits A to 131,072 rows
  * (larger: DV_ERR_ARG).  A must be an FP64 square matrix created beforehand;

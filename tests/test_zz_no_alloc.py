@@ -1,8 +1,8 @@
 """The allocation-free Jacobi PCG entry point (dv_pcg_solve_noalloc).
 
-For callers that cannot allocate device memory while they solve (work being
-recorded into a CUDA graph, or a host that reserved all device memory up
-front).  Called through the C ABI, its result must match the allocating entry
+For callers that cannot allocate device memory while they solve (a host that
+reserved all device memory up front, or a time-critical loop that cannot afford
+cudaFree's device-wide synchronisation).  Called through the C ABI, its result must match the allocating entry
 point (dv_pcg_solve) on the same matrix and right-hand side, within the
 tolerance of the other PCG tests, on two calls in a row: the second call finds
 the previous call's data in the shared device array and must not depend on it.
