@@ -11,14 +11,15 @@ from .sparse import CudaContext, SparseMatrix
 from .adjoint import AdjointCantilever, cantilever_solve_function, element_gradient_device
 from .solvers import (CudaCsrGeometricMultigridSolver, CudaCsrPcgSolver, CudaDuViGeometricMultigridSolver,
                       BatchedMultigridSolver, IterativeStatistics, MultigridPcgSolver, make_path)
-from .cantilever import (FemCantilever3D, cantilever_batch, cartesian_transfer, galerkin, galerkin_hierarchy,
-                         hex_hierarchy, hex_stiffness, hex_trilinear, random_face_loads, traction_rhs)
+from .cantilever import (FemCantilever3D, cantilever_batch, cartesian_transfer, duvi_encode, galerkin,
+                         galerkin_hierarchy, hex_hierarchy, hex_stiffness, hex_trilinear, random_face_loads,
+                         traction_rhs)
 
 __all__ = [
     "AdjointCantilever", "cantilever_solve_function", "element_gradient_device",
     "CudaContext", "SparseMatrix", "CudaCsrGeometricMultigridSolver", "CudaDuViGeometricMultigridSolver",
     "CudaCsrPcgSolver", "MultigridPcgSolver", "BatchedMultigridSolver", "cantilever_batch", "IterativeStatistics", "FemCantilever3D", "hex_hierarchy",
-    "hex_stiffness", "hex_trilinear", "galerkin", "galerkin_hierarchy", "traction_rhs", "random_face_loads", "cartesian_transfer", "make_path", "DuviError",
+    "hex_stiffness", "hex_trilinear", "duvi_encode", "galerkin", "galerkin_hierarchy", "traction_rhs", "random_face_loads", "cartesian_transfer", "make_path", "DuviError",
     "NotImplementedFeatureError", "NotInitializedError", "NoDeviceError",
 ]
 

@@ -60,6 +60,25 @@ def galerkin(A, P):
     return sp.csr_matrix((va, ci, rp), shape=(n.value, n.value))
 
 
+def duvi_encode(A, value_index_bits=0, dedup_tol=1e-10):
+    """DuVi SoA arrays of a CSR matrix on the host (FromDokRowMajor), no device needed:
+    dict of row_to_col, row_to_dist, col_idx, dist, vidx (uint32), values, vi_bits."""
+    ah, ka = _host(A)
+    nb, nu, bits = C.c_int64(), C.c_int64(), C.c_int32()
+    N.check(N.lib().dv_duvi_encode(C.byref(ah), value_index_bits, dedup_tol, C.byref(nb), C.byref(nu), C.byref(bits),
+                                   None, None, None, None, None, None))
+    n, nnz = A.shape[0], A.nnz
+    out = dict(row_to_col=np.empty(n + 1, np.uint32), row_to_dist=np.empty(n + 1, np.uint32),
+               col_idx=np.empty(nb.value, np.uint32), dist=np.empty(nnz, np.uint8), vidx=np.empty(nnz, np.uint32),
+               values=np.empty(nu.value, np.float64))
+    N.check(N.lib().dv_duvi_encode(C.byref(ah), value_index_bits, dedup_tol, C.byref(nb), C.byref(nu), C.byref(bits),
+                                   *(N.ptr(out[k]) for k in ("row_to_col", "row_to_dist", "col_idx", "dist", "vidx",
+                                                             "values"))))
+    del ka
+    out["vi_bits"] = bits.value
+    return out
+
+
 def _host(a):
     from .sparse import _csr_arrays
     rp, ci, va, shape = _csr_arrays(a)

@@ -67,6 +67,129 @@ struct NetDoubleDict {
 };
 }  // namespace
 
+namespace {
+// Exact-bit-pattern numbering of one chunk's values in first-occurrence order
+// (open addressing, grows at half load).
+struct BitsTable {
+    std::vector<uint64_t> key;
+    std::vector<int32_t> id;
+    uint64_t mask = 0;
+    uint64_t last_bits = 0;
+    int32_t last_id = -1;
+    BitsTable() { resize(256); }
+    void resize(size_t cap) {
+        std::vector<uint64_t> k(cap, 0);
+        std::vector<int32_t> d(cap, -1);
+        const uint64_t m = cap - 1;
+        for (size_t i = 0; i < key.size(); ++i)
+            if (id[i] >= 0) {
+                uint64_t j = slot(key[i], m);
+                while (d[j] >= 0) j = (j + 1) & m;
+                k[j] = key[i];
+                d[j] = id[i];
+            }
+        key.swap(k);
+        id.swap(d);
+        mask = m;
+    }
+    static uint64_t slot(uint64_t b, uint64_t m) { return ((b ^ (b >> 31)) * 0x9E3779B97F4A7C15ull >> 17) & m; }
+    uint32_t number(double v, std::vector<double> &distinct) {
+        uint64_t b;
+        std::memcpy(&b, &v, 8);
+        if (b == last_bits && last_id >= 0) return (uint32_t)last_id;
+        uint64_t j = slot(b, mask);
+        while (id[j] >= 0 && key[j] != b) j = (j + 1) & mask;
+        int32_t r = id[j];
+        if (r < 0) {
+            r = (int32_t)distinct.size();
+            key[j] = b;
+            id[j] = r;
+            distinct.push_back(v);
+            if (2 * distinct.size() > key.size()) resize(2 * key.size());
+        }
+        last_bits = b;
+        last_id = r;
+        return (uint32_t)r;
+    }
+};
+
+// Value numbering of FromDokRowMajor: find_or_insert of every entry, in CSR
+// order, into the Dictionary above; returns the keys (the values table).
+// In parallel: each chunk of consecutive entries numbers its distinct bit
+// patterns locally; the chunks' distinct values then pass through the
+// dictionary in chunk order, which inserts every key at the same entry as the
+// sequential walk; each entry finally takes its value's key.  That equals the
+// sequential walk when no distinct value is within the tolerance of two keys
+// of its hash code: a value's key is then the one matching key of its code,
+// whenever it is looked up.  Otherwise a lookup can depend on the keys
+// inserted before it, and the sequential walk runs instead; so it does for
+// non-finite values under a tolerance (they equal nothing, not even
+// themselves, so every occurrence becomes a key).
+std::vector<double> number_values(const double *val, int64_t nnz, double tol, uint32_t *vidx) {
+    auto sequential = [&] {
+        NetDoubleDict map(tol);
+        for (int64_t i = 0; i < nnz; ++i) vidx[i] = (uint32_t)map.find_or_insert(val[i]);
+        return map.keys;
+    };
+#ifdef _OPENMP
+    const int T = omp_get_max_threads();
+#else
+    const int T = 1;
+#endif
+    if (T <= 1 || nnz < (int64_t)1 << 16) return sequential();
+    std::vector<std::vector<double>> distinct(T);
+    int nonfinite = 0;
+#pragma omp parallel for schedule(static, 1) reduction(max : nonfinite)
+    for (int t = 0; t < T; ++t) {
+        BitsTable tab;
+        const int64_t b = nnz * t / T, e = nnz * (t + 1) / T;
+        for (int64_t i = b; i < e; ++i) vidx[i] = tab.number(val[i], distinct[t]);
+        for (double v : distinct[t])
+            if (!std::isfinite(v)) nonfinite = 1;
+    }
+    if (nonfinite && tol > 0) return sequential();
+    NetDoubleDict map(tol);
+    std::vector<std::vector<uint32_t>> key(T);
+    for (int t = 0; t < T; ++t) {
+        key[t].reserve(distinct[t].size());
+        for (double v : distinct[t]) key[t].push_back((uint32_t)map.find_or_insert(v));
+    }
+    // codes held by more than one key, and whether a value matches two of them
+    std::vector<std::pair<int32_t, int32_t>> ck(map.keys.size());
+    for (size_t k = 0; k < ck.size(); ++k) ck[k] = {map.codes[k], (int32_t)k};
+    std::sort(ck.begin(), ck.end());
+    std::vector<std::pair<int32_t, std::vector<int32_t>>> shared;
+    for (size_t k = 0; k < ck.size();) {
+        size_t e = k + 1;
+        while (e < ck.size() && ck[e].first == ck[k].first) ++e;
+        if (e - k > 1) {
+            shared.push_back({ck[k].first, {}});
+            for (size_t q = k; q < e; ++q) shared.back().second.push_back(ck[q].second);
+        }
+        k = e;
+    }
+    if (!shared.empty()) {
+        for (int t = 0; t < T; ++t)
+            for (double v : distinct[t]) {
+                const int32_t c = map.code(v);
+                auto it = std::lower_bound(shared.begin(), shared.end(), c,
+                                           [](const std::pair<int32_t, std::vector<int32_t>> &x, int32_t y) { return x.first < y; });
+                if (it == shared.end() || it->first != c) continue;
+                int hits = 0;
+                for (int32_t k : it->second) hits += map.eq(v, map.keys[k]) ? 1 : 0;
+                if (hits > 1) return sequential();
+            }
+    }
+#pragma omp parallel for schedule(static, 1)
+    for (int t = 0; t < T; ++t) {
+        const int64_t b = nnz * t / T, e = nnz * (t + 1) / T;
+        const uint32_t *kt = key[t].data();
+        for (int64_t i = b; i < e; ++i) vidx[i] = kt[vidx[i]];
+    }
+    return map.keys;
+}
+}  // namespace
+
 // FromDokRowMajor (OpenCLDuViGeometricMultigridSolver.cs:753-851).  The block
 // ("DU") part is independent per row and built in parallel; the value ("VI")
 // part is sequential in CSR order because first occurrence defines the index.
@@ -113,10 +236,8 @@ void dv_encode_duvi(const dv_csr_host &a, double tol, int force_bits, DuviHost &
             h.dist[begin] = (uint8_t)cnt;
         }
     }
-    NetDoubleDict map(tol);
     h.vidx.resize(nnz);
-    for (int64_t i = 0; i < nnz; ++i) h.vidx[i] = (uint32_t)map.find_or_insert(a.val[i]);
-    h.values = map.keys;
+    h.values = number_values(a.val, nnz, tol, h.vidx.data());
     int64_t nu = (int64_t)h.values.size();
     int bits = nu <= 256 ? 8 : (nu <= 65536 ? 16 : 32);
     if (force_bits != 0) {
@@ -126,6 +247,34 @@ void dv_encode_duvi(const dv_csr_host &a, double tol, int force_bits, DuviHost &
         bits = force_bits;
     }
     h.vi_bits = bits;
+}
+
+void dv_check_csr(const dv_csr_host &a) {
+    DV_REQUIRE(a.n_rows >= 0 && a.n_cols >= 0, DV_ERR_ARG, "negative dimensions");
+    DV_REQUIRE(a.rowptr != nullptr, DV_ERR_ARG, "null rowptr");
+    DV_REQUIRE(a.rowptr[0] == 0, DV_ERR_FORMAT, "rowptr[0] must be 0");
+    const int64_t nnz = a.rowptr[a.n_rows];
+    DV_REQUIRE(nnz == 0 || (a.col && a.val), DV_ERR_ARG, "null col/val");
+    // rows checked in parallel; the first bad row (lowest index) names the error
+    int32_t bad_row = INT32_MAX;
+    int bad_kind = 0;
+#pragma omp parallel for schedule(static) reduction(min : bad_row)
+    for (int32_t i = 0; i < a.n_rows; ++i) {
+        bool ok = a.rowptr[i + 1] >= a.rowptr[i] && a.rowptr[i + 1] <= nnz;   // past nnz: not monotone later
+        for (int32_t k = a.rowptr[i]; ok && k < a.rowptr[i + 1]; ++k)
+            ok = a.col[k] >= 0 && a.col[k] < a.n_cols && (k == a.rowptr[i] || a.col[k] > a.col[k - 1]);
+        if (!ok) bad_row = std::min(bad_row, i);
+    }
+    if (bad_row != INT32_MAX) {
+        const int32_t i = bad_row;
+        if (a.rowptr[i + 1] < a.rowptr[i] || a.rowptr[i + 1] > nnz) bad_kind = 1;
+        else
+            for (int32_t k = a.rowptr[i]; k < a.rowptr[i + 1] && !bad_kind; ++k)
+                bad_kind = (a.col[k] < 0 || a.col[k] >= a.n_cols) ? 2 : (k > a.rowptr[i] && a.col[k] <= a.col[k - 1]) ? 3 : 0;
+        DV_REQUIRE(bad_kind != 1, DV_ERR_FORMAT, "rowptr not monotone");
+        DV_REQUIRE(bad_kind != 2, DV_ERR_FORMAT, "column index out of range");
+        DV_REQUIRE(false, DV_ERR_FORMAT, "columns must be strictly increasing within a row");
+    }
 }
 
 void dv_make_bundles(const DuviHost &h, int32_t n_rows, int vi_bits, std::vector<int32_t> &bundles) {
@@ -614,6 +763,30 @@ static inline int32_t hex_row_nodes(int32_t i, int32_t j, int32_t k, int32_t nx,
     int cj = (j > 0 ? 1 : 0) + 1 + (j + 1 < ny ? 1 : 0);
     int ck = (k > 0 ? 1 : 0) + 1 + (k + 1 < nz ? 1 : 0);
     return ci * cj * ck;
+}
+
+extern "C" DV_API int dv_duvi_encode(const dv_csr_host *a, int32_t value_index_bits, double dedup_tol,
+                                     int64_t *nblocks, int64_t *nuniq, int32_t *bits, uint32_t *row_to_col,
+                                     uint32_t *row_to_dist, uint32_t *col_idx, uint8_t *dist,
+                                     uint32_t *value_indices, double *values) {
+    return dv_guard([&] {
+        DV_REQUIRE(a && nblocks && nuniq && bits, DV_ERR_ARG, "null argument");
+        dv_check_csr(*a);
+        DuviHost h;
+        dv_encode_duvi(*a, dedup_tol, value_index_bits, h);
+        *nblocks = (int64_t)h.col_idx.size();
+        *nuniq = (int64_t)h.values.size();
+        *bits = h.vi_bits;
+        if (!row_to_col) return;   // sizes only
+        DV_REQUIRE(row_to_dist && col_idx && values && ((dist && value_indices) || h.vidx.empty()), DV_ERR_ARG,
+                   "null output array");
+        std::copy(h.row_to_col.begin(), h.row_to_col.end(), row_to_col);
+        std::copy(h.row_to_dist.begin(), h.row_to_dist.end(), row_to_dist);
+        std::copy(h.col_idx.begin(), h.col_idx.end(), col_idx);
+        std::copy(h.dist.begin(), h.dist.end(), dist);
+        std::copy(h.vidx.begin(), h.vidx.end(), value_indices);
+        std::copy(h.values.begin(), h.values.end(), values);
+    });
 }
 
 extern "C" DV_API int dv_hex_csr_size(const int32_t *ne, int32_t *n_rows, int64_t *nnz) {

@@ -250,6 +250,9 @@ constexpr int kBundleBlocks = 480;    // block column starts (+ alignment slack)
 // Host helpers (dv_host.cpp)
 void dv_encode_duvi(const dv_csr_host &a, double tol, int force_bits, DuviHost &out);
 void dv_make_bundles(const DuviHost &h, int32_t n_rows, int vi_bits, std::vector<int32_t> &bundles);
+// Throws DV_ERR_ARG / DV_ERR_FORMAT unless a is a valid CSR matrix with strictly
+// increasing columns in every row.
+void dv_check_csr(const dv_csr_host &a);
 void dv_build_duvi_lanes(const DuviHost &h, int32_t n_rows, int32_t n_cols, int value_bytes, DuviLanesHost &out);
 void dv_extract_diag(const dv_csr_host &a, std::vector<double> &diag);
 // CSR transpose (rows sorted by column of the input).

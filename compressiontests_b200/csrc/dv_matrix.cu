@@ -83,21 +83,6 @@ static void upload(DevMem &d, const void *h, size_t bytes, cudaStream_t s) {
     if (bytes) DV_CUDA(cudaMemcpyAsync(d.p, h, bytes, cudaMemcpyHostToDevice, s));
 }
 
-static void check_csr(const dv_csr_host &a) {
-    DV_REQUIRE(a.n_rows >= 0 && a.n_cols >= 0, DV_ERR_ARG, "negative dimensions");
-    DV_REQUIRE(a.rowptr != nullptr, DV_ERR_ARG, "null rowptr");
-    DV_REQUIRE(a.rowptr[0] == 0, DV_ERR_FORMAT, "rowptr[0] must be 0");
-    int64_t nnz = a.rowptr[a.n_rows];
-    DV_REQUIRE(nnz == 0 || (a.col && a.val), DV_ERR_ARG, "null col/val");
-    for (int32_t i = 0; i < a.n_rows; ++i) {
-        DV_REQUIRE(a.rowptr[i + 1] >= a.rowptr[i], DV_ERR_FORMAT, "rowptr not monotone");
-        for (int32_t k = a.rowptr[i]; k < a.rowptr[i + 1]; ++k) {
-            DV_REQUIRE(a.col[k] >= 0 && a.col[k] < a.n_cols, DV_ERR_FORMAT, "column index out of range");
-            DV_REQUIRE(k == a.rowptr[i] || a.col[k] > a.col[k - 1], DV_ERR_FORMAT,
-                       "columns must be strictly increasing within a row");
-        }
-    }
-}
 
 static int pick_tpr(double mean_nnz) {
     if (mean_nnz < 6) return 4;
@@ -314,7 +299,7 @@ static void autotune(dv_matrix *m) {
 
 dv_matrix *dv_matrix_build(dv_context *ctx, const dv_csr_host &a, int format, int precision, int vi_bits, double tol) {
     dv_ctx_check(ctx);
-    check_csr(a);
+    dv_check_csr(a);
     DV_REQUIRE(format == DV_FORMAT_CSR || format == DV_FORMAT_DUVI, DV_ERR_ARG, "unknown format");
     DV_REQUIRE(precision == DV_F64 || precision == DV_F32, DV_ERR_ARG, "precision must be DV_F64 or DV_F32");
     auto m = std::make_unique<dv_matrix>();

@@ -126,6 +126,14 @@ DV_API int dv_matrix_create_csr(dv_context *ctx, const dv_csr_host *a, int32_t p
  * the reference encoder's bit for bit. */
 DV_API int dv_matrix_create_duvi(dv_context *ctx, const dv_csr_host *a, int32_t precision,
                                  int32_t value_index_bits, double dedup_tol, dv_matrix **out);
+/* The same DuVi encode on the host only, no device needed: the SoA arrays that
+ * dv_matrix_create_duvi uploads, for storage or interchange.  Call once with
+ * row_to_col == NULL for the sizes (*nblocks, *nuniq, *bits), then with arrays of
+ * n_rows+1, n_rows+1, nblocks, nnz, nnz and nuniq elements (value indices
+ * widened to uint32). */
+DV_API int dv_duvi_encode(const dv_csr_host *a, int32_t value_index_bits, double dedup_tol, int64_t *nblocks,
+                          int64_t *nuniq, int32_t *bits, uint32_t *row_to_col, uint32_t *row_to_dist,
+                          uint32_t *col_idx, uint8_t *dist, uint32_t *value_indices, double *values);
 /* Upload an already encoded DuVi SoA (DuViMat8/16, :16-31). value_indices has
  * value_index_bits per entry. */
 DV_API int dv_matrix_create_duvi_soa(dv_context *ctx, int32_t n_rows, int32_t n_cols,

@@ -142,3 +142,90 @@ def test_cantilever_batch_is_seeded(native):
     assert d1 == d2 and all(8 <= v <= 48 for d in d1 for v in d)
     assert all(np.array_equal(a, b) for a, b in zip(r1, r2))
     assert [m[0][0].shape[0] for m in m1] == [3 * d[0] * (d[1] + 1) * (d[2] + 1) for d in d1]
+
+
+def _encode_matches_oracle(native, oracle, A, tol=1e-10, bits=0):
+    got = native.duvi_encode(A, bits, tol)
+    ref = oracle.DuVi(oracle.Csr.from_scipy(A), tol, bits)
+    exp = ref.arrays()
+    assert got["vi_bits"] == ref.vi_bits
+    for k in ("row_to_col", "row_to_dist", "col_idx", "dist", "vidx"):
+        np.testing.assert_array_equal(got[k], exp[k], err_msg=k)
+    np.testing.assert_array_equal(got["values"].view(np.uint64), exp["values"].view(np.uint64))
+
+
+def _random_csr(rng, n, per_row, values):
+    import scipy.sparse as sp
+    rows = np.repeat(np.arange(n), per_row)
+    cols = np.concatenate([np.sort(rng.choice(n, per_row, replace=False)) for _ in range(n)])
+    A = sp.csr_matrix((np.ones(rows.size), (rows, cols)), shape=(n, n))
+    A.sort_indices()
+    A.data = np.asarray(values, np.float64)[: A.nnz].copy()
+    return A
+
+
+@pytest.mark.parametrize("case", ["hex", "hex_log_moduli", "small"])
+def test_duvi_host_encoder_matches_oracle(native, oracle, rng, case):
+    # The library's encoder numbers values in parallel chunks (exact-bit local tables,
+    # then the chunks' distinct values through the .NET Dictionary semantics in order);
+    # its arrays must equal the oracle's sequential FromDokRowMajor bit for bit.
+    if case == "hex":
+        A = native.hex_stiffness((12, 12, 12))                    # 28 values, 460k entries
+    elif case == "hex_log_moduli":
+        E = 10.0 ** rng.uniform(-2.0, 0.0, 8 * 8 * 8)
+        A = native.hex_stiffness((8, 8, 8), E)                    # nearly every value distinct
+    else:
+        A = native.hex_stiffness((2, 2, 2))                       # below the parallel threshold
+    assert case == "small" or A.nnz >= 1 << 16
+    _encode_matches_oracle(native, oracle, A)
+    if case != "hex":
+        _encode_matches_oracle(native, oracle, A, bits=32)
+
+
+def test_duvi_host_encoder_near_tolerance_values(native, oracle, rng):
+    # Values -0.9, -0.1 and +0.5 x 1e-10 around multiples of 2e-10 share a hash cell;
+    # -0.9 and +0.5 are two keys (1.4e-10 apart) and -0.1 lies within the tolerance of
+    # both, so its key depends on which one was inserted last: the encoder must detect
+    # this and number the values exactly as the sequential walk does.
+    n, per_row = 3000, 40
+    m = rng.integers(1, 50, n * per_row) * 2e-10
+    d = rng.choice([-0.9e-10, -0.1e-10, 0.5e-10], n * per_row)
+    _encode_matches_oracle(native, oracle, _random_csr(rng, n, per_row, m + d))
+
+
+@pytest.mark.parametrize("tol", [1e-10, 0.0])
+def test_duvi_host_encoder_special_values(native, oracle, rng, tol):
+    # NaN and infinities (under a tolerance they equal nothing, not even themselves, so
+    # every occurrence is a new value) and signed zeros, in a matrix large enough for
+    # the parallel path.
+    n, per_row = 2000, 40
+    pool = np.array([0.0, -0.0, 1.5, -2.25, np.inf, -np.inf, np.nan, 3.0])
+    vals = pool[rng.integers(0, pool.size, n * per_row)]
+    vals[rng.random(vals.size) < 0.995] = 1.5   # keep the special values rare
+    _encode_matches_oracle(native, oracle, _random_csr(rng, n, per_row, vals), tol=tol, bits=32)
+
+
+@pytest.mark.parametrize("kind", ["unsorted", "column_range", "rowptr_down", "rowptr_past_nnz"])
+def test_host_encoder_rejects_bad_csr(native, kind):
+    # The CSR checks run over the rows in parallel and report the first bad row's fault.
+    import ctypes as C
+    N = native._native
+    rp = np.array([0, 2, 4, 6], np.int32)
+    ci = np.array([0, 1, 1, 2, 0, 2], np.int32)
+    va = np.ones(6)
+    if kind == "unsorted":
+        ci[2:4] = [2, 1]
+    elif kind == "column_range":
+        ci[5] = 3
+    elif kind == "rowptr_down":
+        rp[2] = 1          # row 0 is valid, row 1 ends before it starts
+    else:
+        rp[1:3] = [2, 9]   # row 1 would read past nnz
+    ah, keep = N.csr_host(rp, ci, va, (3, 3))
+    nb, nu, bits = C.c_int64(), C.c_int64(), C.c_int32()
+    st = N.lib().dv_duvi_encode(C.byref(ah), 0, 1e-10, C.byref(nb), C.byref(nu), C.byref(bits),
+                                None, None, None, None, None, None)
+    assert st == N.DV_ERR_FORMAT
+    msg = N.lib().dv_last_error().decode()
+    assert {"unsorted": "increasing", "column_range": "out of range", "rowptr_down": "monotone",
+            "rowptr_past_nnz": "monotone"}[kind] in msg, msg
