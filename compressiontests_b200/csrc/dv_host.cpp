@@ -4,6 +4,7 @@
 #include "dv_internal.cuh"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <numeric>
 
@@ -138,15 +139,15 @@ std::vector<double> number_values(const double *val, int64_t nnz, double tol, ui
 #endif
     if (T <= 1 || nnz < (int64_t)1 << 16) return sequential();
     std::vector<std::vector<double>> distinct(T);
-    int nonfinite = 0;
-#pragma omp parallel for schedule(static, 1) reduction(max : nonfinite)
+#pragma omp parallel for schedule(static, 1)
     for (int t = 0; t < T; ++t) {
         BitsTable tab;
         const int64_t b = nnz * t / T, e = nnz * (t + 1) / T;
         for (int64_t i = b; i < e; ++i) vidx[i] = tab.number(val[i], distinct[t]);
-        for (double v : distinct[t])
-            if (!std::isfinite(v)) nonfinite = 1;
     }
+    bool nonfinite = false;
+    for (int t = 0; t < T; ++t)
+        for (double v : distinct[t]) nonfinite = nonfinite || !std::isfinite(v);
     if (nonfinite && tol > 0) return sequential();
     NetDoubleDict map(tol);
     std::vector<std::vector<uint32_t>> key(T);
@@ -394,22 +395,43 @@ void dv_build_duvi_lanes(const DuviHost &h, int32_t n, int32_t n_cols, int value
     L.tuples = 0;
     L.tuple_vi.clear();
     if (g >= 2 && vib == 1) {
-        std::vector<int16_t> id(1u << (8 * g), -1);
-        int ntup = 0;
-        bool ok = true;
-        for (int64_t gi = 0; gi < L.ngroups && ok; ++gi) {
-            const int32_t r0 = (int32_t)(gi * g);
-            const uint32_t ne = h.row_to_dist[r0 + 1] - h.row_to_dist[r0];
-            for (uint32_t e = 0; e < ne; ++e) {
-                uint32_t key = 0;
-                for (int d = 0; d < g; ++d) key |= h.vidx[h.row_to_dist[r0 + d] + e] << (8 * d);
-                if (id[key] < 0) {
-                    if (ntup == 256) { ok = false; break; }
-                    id[key] = (int16_t)ntup++;
-                    for (int d = 0; d < g; ++d) L.tuple_vi.push_back((key >> (8 * d)) & 0xFFu);
+        // each chunk of groups lists its tuples in first-occurrence order; merged in
+        // chunk order they give the numbering of one walk over all groups
+#ifdef _OPENMP
+        const int T = omp_get_max_threads();
+#else
+        const int T = 1;
+#endif
+        const size_t nkeys = (size_t)1 << (8 * g);
+        std::vector<std::vector<uint32_t>> first(T);
+#pragma omp parallel for schedule(static, 1)
+        for (int t = 0; t < T; ++t) {
+            std::vector<uint8_t> seen(nkeys / 8 + 1, 0);
+            const int64_t gb = L.ngroups * t / T, ge = L.ngroups * (t + 1) / T;
+            for (int64_t gi = gb; gi < ge && first[t].size() <= 256; ++gi) {
+                const int32_t r0 = (int32_t)(gi * g);
+                const uint32_t ne = h.row_to_dist[r0 + 1] - h.row_to_dist[r0];
+                for (uint32_t e = 0; e < ne && first[t].size() <= 256; ++e) {
+                    uint32_t key = 0;
+                    for (int d = 0; d < g; ++d) key |= h.vidx[h.row_to_dist[r0 + d] + e] << (8 * d);
+                    if (!(seen[key >> 3] & (1u << (key & 7)))) {
+                        seen[key >> 3] |= (uint8_t)(1u << (key & 7));
+                        first[t].push_back(key);
+                    }
                 }
             }
         }
+        std::vector<int16_t> id(nkeys, -1);
+        int ntup = 0;
+        bool ok = true;
+        for (int t = 0; t < T; ++t) ok = ok && first[t].size() <= 256;   // more in one chunk: more in all
+        for (int t = 0; t < T && ok; ++t)
+            for (uint32_t key : first[t]) {
+                if (id[key] >= 0) continue;
+                if (ntup == 256) { ok = false; break; }
+                id[key] = (int16_t)ntup++;
+                for (int d = 0; d < g; ++d) L.tuple_vi.push_back((key >> (8 * d)) & 0xFFu);
+            }
         if (ok) {
             L.tuples = 1;
             L.tuple_id.swap(id);
@@ -575,18 +597,19 @@ void dv_build_duvi_patterns(const DuviHost &h, int32_t n, int32_t n_cols, int g,
             sig[gi] = x;
         }
     }
-    // first-occurrence numbering; equal hashes are confirmed entry by entry
+    // First-occurrence numbering by signature, then every group's entries confirmed
+    // against its pattern's (in parallel).  Two different entry lists with one 64-bit
+    // signature would fail the confirmation; the sequential numbering that compares
+    // entry lists on every signature match then runs instead.
     std::vector<uint64_t> phash;
     std::vector<std::vector<int64_t>> pent;
     std::vector<int64_t> buf;
     P.id.resize(ngroups);
-    for (int64_t gi = 0; gi < ngroups; ++gi) {
+    bool by_signature = true;
+    for (int64_t gi = 0; gi < ngroups && by_signature; ++gi) {
         int found = -1;
         for (size_t p = 0; p < phash.size(); ++p)
-            if (phash[p] == sig[gi]) {
-                entries(gi, buf);
-                if (buf == pent[p]) { found = (int)p; break; }
-            }
+            if (phash[p] == sig[gi]) { found = (int)p; break; }
         if (found < 0) {
             if ((int)phash.size() == max_patterns) return;
             entries(gi, buf);
@@ -595,6 +618,40 @@ void dv_build_duvi_patterns(const DuviHost &h, int32_t n, int32_t n_cols, int g,
             found = (int)phash.size() - 1;
         }
         P.id[gi] = (uint16_t)found;
+    }
+    {
+        std::atomic<bool> mismatch(false);
+#pragma omp parallel
+        {
+            std::vector<int64_t> mine;
+#pragma omp for schedule(static)
+            for (int64_t gi = 0; gi < ngroups; ++gi) {
+                if (mismatch.load(std::memory_order_relaxed)) continue;
+                entries(gi, mine);
+                if (mine != pent[P.id[gi]]) mismatch.store(true, std::memory_order_relaxed);
+            }
+        }
+        by_signature = !mismatch.load();
+    }
+    if (!by_signature) {
+        phash.clear();
+        pent.clear();
+        for (int64_t gi = 0; gi < ngroups; ++gi) {
+            int found = -1;
+            for (size_t p = 0; p < phash.size(); ++p)
+                if (phash[p] == sig[gi]) {
+                    entries(gi, buf);
+                    if (buf == pent[p]) { found = (int)p; break; }
+                }
+            if (found < 0) {
+                if ((int)phash.size() == max_patterns) return;
+                entries(gi, buf);
+                phash.push_back(sig[gi]);
+                pent.push_back(buf);
+                found = (int)phash.size() - 1;
+            }
+            P.id[gi] = (uint16_t)found;
+        }
     }
     int64_t total = 0;
     for (auto &e : pent) total += (int64_t)e.size() / (1 + g);
