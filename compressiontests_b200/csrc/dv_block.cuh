@@ -452,11 +452,8 @@ void launch_bprod_pattern_u(const LaunchEnv &e, const dv_matrix *m, int kc, Gath
     constexpr int G = 3;
     auto kern = k_bprod_pattern<AT, G, U, EXACT, BASED, SHIFT, Gather, Epi>;
     const size_t smem = sizeof(dvk::PatRec<AT>) * (size_t)m->pat_entries + 4 * ((size_t)m->pat_count + 1);
-    static size_t attr_set = 0;   // per instantiation: largest size enabled so far
-    if (smem > attr_set) {
-        DV_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr_set = smem;
-    }
+    static dvk::SmemLimit limit;   // per instantiation and device
+    limit.raise(kern, smem, e.ctx->device);
     const int32_t ngroups = m->n_rows / G;
     const int blocks = bprod_blocks(e, ngroups, Epi::NC > 0);
     kern<<<blocks, kThreads, smem, e.stream>>>(m->pat_id.as<uint16_t>(), m->pat_start.as<uint32_t>(),

@@ -26,6 +26,21 @@ constexpr int kMaxRed = 4;               // doubles per block in a grid reductio
 static_assert(kStageD >= kBundleBytes + 32, "stage too small");
 static_assert(kStageC >= kBundleBlocks + 8, "column stage too small");
 
+// The dynamic shared memory a kernel may use is an attribute of each device: a
+// launcher raises it to every new largest size on each device it launches on.
+constexpr int kMaxDevices = 64;
+struct SmemLimit {
+    size_t set[kMaxDevices] = {};
+    template <class K>
+    void raise(K kern, size_t smem, int device) {
+        DV_REQUIRE(device >= 0 && device < kMaxDevices, DV_ERR_ARG, "device ordinal out of range");
+        if (smem > set[device]) {
+            DV_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            set[device] = smem;
+        }
+    }
+};
+
 // ---------------------------------------------------------------------------
 // reductions
 // ---------------------------------------------------------------------------
@@ -856,11 +871,8 @@ void launch_duvi_pattern_gbs(const LaunchEnv &e, const dv_matrix *m, Gather g, O
     const size_t smem = sizeof(PatRec<AT>) * (size_t)m->pat_entries + 4 * ((size_t)m->pat_count + 1);
     // Raise the kernel's dynamic shared-memory limit to every new largest size: epilogues
     // that reduce add static shared memory, so even tables under 48 KB can need it.
-    static size_t attr_set = 0;   // per instantiation: largest size enabled so far
-    if (smem > attr_set) {
-        DV_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr_set = smem;
-    }
+    static SmemLimit limit;   // per instantiation and device
+    limit.raise(kern, smem, e.ctx->device);
     // Whole waves: past one wave of resident blocks (SMs x blocks per SM at this table size
     // and register count), a multiple of it, so that the last wave is not a partial one.
     static size_t occ_smem[4] = {};
@@ -905,11 +917,8 @@ void launch_duvi_vi(const LaunchEnv &e, const dv_matrix *m, Gather g, Op op) {
     constexpr int W = sizeof(VI) == 4 ? kDuviWarps32 : kDuviWarps;
     const size_t smem = duvi_smem_bytes<VI, AT>(W);
     auto kern = k_duvi<VI, AT, Gather, Op, W, BATCH>;
-    static bool attr_set = false;   // per instantiation
-    if (!attr_set) {
-        DV_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr_set = true;
-    }
+    static SmemLimit limit;   // per instantiation and device
+    limit.raise(kern, smem, e.ctx->device);
     DuviArgs a;
     a.row_to_col = m->row_to_col.as<uint32_t>();
     a.row_to_dist = m->row_to_dist.as<uint32_t>();
