@@ -139,6 +139,10 @@ _SIGNATURES = {
     "dv_hex_trilinear": (C.c_int, [_vp, _vp, _vp, _vp]),
     "dv_duvi_encode": (C.c_int, [_P(CsrHost), C.c_int32, C.c_double, _P(C.c_int64), _P(C.c_int64), _P(C.c_int32),
                                  _vp, _vp, _vp, _vp, _vp, _vp]),
+    "dv_units_encode": (C.c_int, [_P(CsrHost), C.c_double, _P(C.c_int64), _P(C.c_int64), _P(C.c_int64),
+                                  _P(C.c_int64), _vp, _vp, _vp, _vp]),
+    "dv_units_decode": (C.c_int, [C.c_int32, C.c_int32, _vp, C.c_int64, _vp, C.c_int64, _vp, C.c_int64,
+                                  _P(C.c_int64), _vp, _vp, _vp]),
     "dv_galerkin_size": (C.c_int, [_P(CsrHost), _P(CsrHost), _P(C.c_int32), _P(C.c_int64)]),
     "dv_galerkin": (C.c_int, [_P(CsrHost), _P(CsrHost), _vp, _vp, _vp]),
     "dv_cartesian_transfer_size": (C.c_int, [C.c_int32, _vp, _vp, C.c_int32, C.c_int32, _vp, C.c_int32, _vp,

@@ -79,6 +79,38 @@ def duvi_encode(A, value_index_bits=0, dedup_tol=1e-10):
     return out
 
 
+def units_encode(A, dedup_tol=1e-10):
+    """CPU DuVi Unit stream of a CSR matrix (DuViCompressedSparseMatrix's units, flat):
+    dict of bytes (uint8), unit_offsets (int64, n_units + 1), vidx (int32), values."""
+    ah, ka = _host(A)
+    nu_, nb, ni, nq = C.c_int64(), C.c_int64(), C.c_int64(), C.c_int64()
+    N.check(N.lib().dv_units_encode(C.byref(ah), dedup_tol, C.byref(nu_), C.byref(nb), C.byref(ni), C.byref(nq),
+                                    None, None, None, None))
+    out = dict(bytes=np.empty(nb.value, np.uint8), unit_offsets=np.empty(nu_.value + 1, np.int64),
+               vidx=np.empty(ni.value, np.int32), values=np.empty(nq.value, np.float64))
+    N.check(N.lib().dv_units_encode(C.byref(ah), dedup_tol, C.byref(nu_), C.byref(nb), C.byref(ni), C.byref(nq),
+                                    *(N.ptr(out[k]) for k in ("bytes", "unit_offsets", "vidx", "values"))))
+    del ka
+    return out
+
+
+def units_decode(shape, units):
+    """CSR matrix (scipy) of a Unit stream produced by units_encode (or the reference)."""
+    n, m = shape
+    b, vi, va = (np.ascontiguousarray(units[k]) for k in ("bytes", "vidx", "values"))
+    b = b.astype(np.uint8, copy=False)
+    vi = vi.astype(np.int32, copy=False)
+    va = va.astype(np.float64, copy=False)
+    nnz = C.c_int64()
+    args = (n, m, N.ptr(b), b.size, N.ptr(vi), vi.size, N.ptr(va), va.size, C.byref(nnz))
+    N.check(N.lib().dv_units_decode(*args, None, None, None))
+    rp = np.empty(n + 1, np.int32)
+    ci = np.empty(nnz.value, np.int32)
+    vv = np.empty(nnz.value, np.float64)
+    N.check(N.lib().dv_units_decode(*args, N.ptr(rp), N.ptr(ci), N.ptr(vv)))
+    return sp.csr_matrix((vv, ci, rp), shape=(n, m))
+
+
 def _host(a):
     from .sparse import _csr_arrays
     rp, ci, va, shape = _csr_arrays(a)

@@ -126,7 +126,9 @@ struct BitsTable {
 // inserted before it, and the sequential walk runs instead; so it does for
 // non-finite values under a tolerance (they equal nothing, not even
 // themselves, so every occurrence becomes a key).
-std::vector<double> number_values(const double *val, int64_t nnz, double tol, uint32_t *vidx) {
+}  // namespace
+
+std::vector<double> dv_number_values(const double *val, int64_t nnz, double tol, uint32_t *vidx) {
     auto sequential = [&] {
         NetDoubleDict map(tol);
         for (int64_t i = 0; i < nnz; ++i) vidx[i] = (uint32_t)map.find_or_insert(val[i]);
@@ -189,7 +191,6 @@ std::vector<double> number_values(const double *val, int64_t nnz, double tol, ui
     }
     return map.keys;
 }
-}  // namespace
 
 // FromDokRowMajor (OpenCLDuViGeometricMultigridSolver.cs:753-851).  The block
 // ("DU") part is independent per row and built in parallel; the value ("VI")
@@ -238,7 +239,7 @@ void dv_encode_duvi(const dv_csr_host &a, double tol, int force_bits, DuviHost &
         }
     }
     h.vidx.resize(nnz);
-    h.values = number_values(a.val, nnz, tol, h.vidx.data());
+    h.values = dv_number_values(a.val, nnz, tol, h.vidx.data());
     int64_t nu = (int64_t)h.values.size();
     int bits = nu <= 256 ? 8 : (nu <= 65536 ? 16 : 32);
     if (force_bits != 0) {

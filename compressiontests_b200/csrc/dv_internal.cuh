@@ -250,6 +250,11 @@ constexpr int kBundleBlocks = 480;    // block column starts (+ alignment slack)
 // Host helpers (dv_host.cpp)
 void dv_encode_duvi(const dv_csr_host &a, double tol, int force_bits, DuviHost &out);
 void dv_make_bundles(const DuviHost &h, int32_t n_rows, int vi_bits, std::vector<int32_t> &bundles);
+// Value numbering of the reference's DuVi constructors: every value, in order, looked up in
+// (or added to) a .NET Dictionary<double,int> with the ToleranceComparer of tolerance tol
+// (default double comparer for tol == 0); idx[i] receives the value's key, the keys are
+// returned in insertion order.
+std::vector<double> dv_number_values(const double *val, int64_t n, double tol, uint32_t *idx);
 // Throws DV_ERR_ARG / DV_ERR_FORMAT unless a is a valid CSR matrix with strictly
 // increasing columns in every row.
 void dv_check_csr(const dv_csr_host &a);

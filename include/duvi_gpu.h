@@ -134,6 +134,26 @@ DV_API int dv_matrix_create_duvi(dv_context *ctx, const dv_csr_host *a, int32_t 
 DV_API int dv_duvi_encode(const dv_csr_host *a, int32_t value_index_bits, double dedup_tol, int64_t *nblocks,
                           int64_t *nuniq, int32_t *bits, uint32_t *row_to_col, uint32_t *row_to_dist,
                           uint32_t *col_idx, uint8_t *dist, uint32_t *value_indices, double *values);
+/* The CPU DuVi Unit stream (DuViCompressedSparseMatrix, DuViCompressedSparseMatrix.cs:11-152 and
+ * its CSR constructor :285-400) as one flat byte stream, for storage and interchange; host only.
+ * Each row is one or more units (header byte: new-row bit | step width class << 1; step count
+ * byte; column gap as a 1-4 byte big-endian prefix code; little-endian column steps of 1, 2
+ * or 4 bytes); an empty row is one unit of gap 0 whose value is 0.0.  value_indices (int32,
+ * one per entry and per empty row) number the values in entry order with the reference's
+ * Dictionary semantics (dedup_tol as in dv_matrix_create_duvi).  Call with bytes == NULL for
+ * the sizes, then with bytes[n_bytes], unit_offsets[n_units + 1], value_indices[n_indices]
+ * and values[nuniq].  Rows that would need a unit of more than 255 steps (the reference
+ * wraps its one-byte count) or a gap of 2^29 + 2,113,664 or more: DV_ERR_FORMAT. */
+DV_API int dv_units_encode(const dv_csr_host *a, double dedup_tol, int64_t *n_units, int64_t *n_bytes,
+                           int64_t *n_indices, int64_t *nuniq, uint8_t *bytes, int64_t *unit_offsets,
+                           int32_t *value_indices, double *values);
+/* Unit stream back to CSR, walking the units as DuViCompressedSparseMatrix.Multiply does
+ * (:419-441): *nnz with rowptr == NULL, then rowptr[n_rows + 1], col[nnz], val[nnz].  An
+ * empty row comes back as one entry (column 0, value of its index: 0.0).  Malformed streams
+ * (truncated units, columns past n_cols, index or row counts that do not match): DV_ERR_FORMAT. */
+DV_API int dv_units_decode(int32_t n_rows, int32_t n_cols, const uint8_t *bytes, int64_t n_bytes,
+                           const int32_t *value_indices, int64_t n_indices, const double *values, int64_t nuniq,
+                           int64_t *nnz, int32_t *rowptr, int32_t *col, double *val);
 /* Upload an already encoded DuVi SoA (DuViMat8/16, :16-31). value_indices has
  * value_index_bits per entry. */
 DV_API int dv_matrix_create_duvi_soa(dv_context *ctx, int32_t n_rows, int32_t n_cols,

@@ -229,3 +229,84 @@ def test_host_encoder_rejects_bad_csr(native, kind):
     msg = N.lib().dv_last_error().decode()
     assert {"unsorted": "increasing", "column_range": "out of range", "rowptr_down": "monotone",
             "rowptr_past_nnz": "monotone"}[kind] in msg, msg
+
+
+def _units_match_oracle(native, oracle, A, tol=1e-10):
+    got = native.units_encode(A, tol)
+    exp = oracle.Units.from_csr(oracle.Csr.from_scipy(A), tol).arrays()
+    np.testing.assert_array_equal(got["bytes"], exp["bytes"])
+    np.testing.assert_array_equal(got["unit_offsets"], exp["offsets"])
+    np.testing.assert_array_equal(got["vidx"], exp["vidx"])
+    np.testing.assert_array_equal(got["values"].view(np.uint64), exp["values"].view(np.uint64))
+    return got
+
+
+def test_units_kat_matches_oracle_and_reference_product(native, oracle):
+    # CompressedSparseMatrixTests.cs:15-39: 2 x 1024 from CSR; y = A x with x = row 0 is [11, 0]
+    import scipy.sparse as sp
+    w = 1024
+    A = sp.csr_matrix(([1, 1, 1, 2, 2, 3, 3.0], [5, 6, 8, w - 24, w - 1, 50, w - 4], [0, 5, 7]), shape=(2, w))
+    got = _units_match_oracle(native, oracle, A)
+    B = native.units_decode(A.shape, got)
+    assert (B != A).nnz == 0
+    x = A.toarray()[0]
+    np.testing.assert_array_equal(B @ x, [11.0, 0.0])
+
+
+def test_units_every_width_and_gap_length(native, oracle):
+    # steps of 1, 2 and 4 bytes in every order, gaps in each of the four prefix-code lengths
+    # (< 128, < 16,512, < 2,113,664, above), width changes on empty and non-empty units
+    import scipy.sparse as sp
+    rng = np.random.default_rng(20261203)
+    n, m = 60, 6_000_000
+    rows, cols = [], []
+    for i in range(n):
+        c, cs = int(rng.integers(0, 3_000_000)) if i % 4 == 3 else int(rng.integers(0, 20000)), []
+        for _ in range(int(rng.integers(1, 40))):
+            if c >= m:
+                break
+            cs.append(c)
+            c += int(rng.choice([1, 2, 200, 255, 256, 300, 65535, 65536, 70000]))
+        rows += [i] * len(cs)
+        cols += cs
+    A = sp.csr_matrix((rng.integers(1, 6, len(rows)).astype(float), (rows, cols)), shape=(n, m))
+    A.sort_indices()
+    got = _units_match_oracle(native, oracle, A)
+    b, off = got["bytes"], got["unit_offsets"][:-1]
+    assert set(b[off] >> 1) == {0, 1, 2}                                       # step widths 1, 2, 4 bytes
+    g = b[off + 2]
+    kinds = np.where(g < 0x80, 1, np.where(g < 0xC0, 2, np.where(g < 0xE0, 3, 4)))
+    assert set(kinds) == {1, 2, 3, 4}                                          # every gap code length
+    B = native.units_decode(A.shape, got)
+    assert (B != A).nnz == 0 and np.array_equal(B.indptr, A.indptr)
+
+
+def test_units_empty_rows_and_hex_operator(native, oracle, rng):
+    import scipy.sparse as sp
+    # empty rows: one unit of gap 0 numbered as the value 0.0; decoded as an explicit zero
+    A = sp.csr_matrix(np.array([[0, 2.0, 0], [0, 0, 0], [1.0, 0, 3.0], [0, 0, 0]]))
+    got = _units_match_oracle(native, oracle, A)
+    B = native.units_decode(A.shape, got)
+    assert B.nnz == A.nnz + 2 and B[1, 0] == 0.0 and B[3, 0] == 0.0
+    np.testing.assert_array_equal(B.toarray(), A.toarray())
+    # a 12^3 hex operator (460k entries: the parallel value numbering), round trip
+    H = native.hex_stiffness((12, 12, 12))
+    got = _units_match_oracle(native, oracle, H)
+    B = native.units_decode(H.shape, got)
+    assert (B != H).nnz == 0
+
+
+def test_units_reject_unrepresentable_rows_and_malformed_streams(native):
+    import scipy.sparse as sp
+    # 300 one-byte steps in one unit: the reference's count byte would wrap
+    A = sp.csr_matrix((np.ones(301), (np.zeros(301, int), np.arange(301))), shape=(1, 400))
+    with pytest.raises(native.DuviError) as e:
+        native.units_encode(A)
+    assert e.value.status == native._native.DV_ERR_FORMAT and "255" in str(e.value)
+    H = native.hex_stiffness((2, 2, 2))
+    u = native.units_encode(H)
+    bad = dict(u, bytes=u["bytes"][:-1])   # truncated inside the last unit
+    with pytest.raises(native.DuviError):
+        native.units_decode(H.shape, bad)
+    with pytest.raises(native.DuviError):   # one row too few
+        native.units_decode((H.shape[0] + 1, H.shape[1]), u)
