@@ -17,7 +17,6 @@ import ctypes as C
 from dataclasses import dataclass
 
 import numpy as np
-import scipy.sparse as sp
 
 from . import _native as N
 from .sparse import CudaContext, _csr_arrays
