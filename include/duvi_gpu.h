@@ -2,7 +2,7 @@
  * duvi_gpu.h -- C ABI of the B200 sparse solver path (libduvigpu.so).
  *
  * Drop-in replacement for the OpenCL layer of nickreserved/CompressionTests
- * (src/MGroup.OCL/*.cl and the three solver classes that drive it), callable
+ * (the OpenCL kernels in src/MGroup.OCL and the three solver classes that drive them), callable
  * from C# through [DllImport] or from any C FFI.  Plain pointers and sizes
  * only.  One CUDA device per context, one stream per context; every call that
  * takes host arrays copies them and returns after the device work finished
