@@ -210,7 +210,6 @@ struct dv_matrix {
     int64_t lanes_bundles = 0, lanes_groups = 0;
     DevMem lanes_meta, lanes_dist, lanes_vi, lanes_cols, lanes_nent;
     int64_t lanes_bytes = 0;   // bytes one product reads from the lane layout
-    DuviHost host;             // kept for export
     // shared
     int row_group = 1;         // g consecutive rows share one column list (node dofs); 1 otherwise
     DevMem diag;               // FP64 diagonal (0 where absent)
@@ -276,5 +275,7 @@ int dv_block_coloring(const dv_csr_host &a, int bs, std::vector<int32_t> &color_
 int dv_gs_level_sets(const dv_csr_host &a, std::vector<int32_t> &perm, std::vector<int32_t> &offsets);
 
 // Matrix creation (dv_matrix.cu)
+// encoded: a DuVi encoding of a made with the same vi_bits and tol, used instead of
+// encoding again (one encoding serves matrices of both precisions).
 dv_matrix *dv_matrix_build(dv_context *ctx, const dv_csr_host &a, int format, int precision,
-                           int vi_bits, double tol);
+                           int vi_bits, double tol, const DuviHost *encoded = nullptr);

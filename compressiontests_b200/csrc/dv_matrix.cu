@@ -91,8 +91,9 @@ static int pick_tpr(double mean_nnz) {
     return 32;
 }
 
-static void finish_duvi_upload(dv_matrix *m, cudaStream_t s) {
-    const DuviHost &h = m->host;
+// Uploads the SoA arrays of encoding h and derives the device layouts; h is only read
+// here (export reads the device arrays back), so callers keep it only while building.
+static void finish_duvi_upload(dv_matrix *m, const DuviHost &h, cudaStream_t s) {
     m->vi_bits = h.vi_bits;
     m->nblocks = (int64_t)h.col_idx.size();
     m->nuniq = (int64_t)h.values.size();
@@ -104,12 +105,14 @@ static void finish_duvi_upload(dv_matrix *m, cudaStream_t s) {
     size_t nnz = h.vidx.size();
     if (m->vi_bits == 8) {
         std::vector<uint8_t> v(nnz);
-        for (size_t i = 0; i < nnz; ++i) v[i] = (uint8_t)h.vidx[i];
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < (int64_t)nnz; ++i) v[i] = (uint8_t)h.vidx[i];
         upload(m->vidx, v.data(), nnz, s);
         DV_CUDA(cudaStreamSynchronize(s));
     } else if (m->vi_bits == 16) {
         std::vector<uint16_t> v(nnz);
-        for (size_t i = 0; i < nnz; ++i) v[i] = (uint16_t)h.vidx[i];
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < (int64_t)nnz; ++i) v[i] = (uint16_t)h.vidx[i];
         upload(m->vidx, v.data(), 2 * nnz, s);
         DV_CUDA(cudaStreamSynchronize(s));
     } else {
@@ -297,7 +300,8 @@ static void autotune(dv_matrix *m) {
     ctx->launches -= (int64_t)cand.size() * 4;   // tuning launches are not part of any solve
 }
 
-dv_matrix *dv_matrix_build(dv_context *ctx, const dv_csr_host &a, int format, int precision, int vi_bits, double tol) {
+dv_matrix *dv_matrix_build(dv_context *ctx, const dv_csr_host &a, int format, int precision, int vi_bits, double tol,
+                           const DuviHost *encoded) {
     dv_ctx_check(ctx);
     dv_check_csr(a);
     DV_REQUIRE(format == DV_FORMAT_CSR || format == DV_FORMAT_DUVI, DV_ERR_ARG, "unknown format");
@@ -326,8 +330,13 @@ dv_matrix *dv_matrix_build(dv_context *ctx, const dv_csr_host &a, int format, in
         m->row_group = dv_csr_row_group(a);
         m->device_bytes = m->nnz * (4 + (precision == DV_F64 ? 8 : 4)) + 4 * ((int64_t)a.n_rows + 1);
     } else {
-        dv_encode_duvi(a, tol, vi_bits, m->host);
-        finish_duvi_upload(m.get(), s);
+        if (encoded) {
+            finish_duvi_upload(m.get(), *encoded, s);
+        } else {
+            DuviHost h;
+            dv_encode_duvi(a, tol, vi_bits, h);
+            finish_duvi_upload(m.get(), h, s);
+        }
     }
     if (a.n_rows == a.n_cols) {
         dv_extract_diag(a, m->host_diag);
@@ -373,7 +382,7 @@ extern "C" DV_API int dv_matrix_create_duvi_soa(dv_context *ctx, int32_t n_rows,
         m->nnz = nnz;
         m->format = DV_FORMAT_DUVI;
         m->precision = precision;
-        DuviHost &h = m->host;
+        DuviHost h;
         h.row_to_col.assign(rc, rc + n_rows + 1);
         h.row_to_dist.assign(rd, rd + n_rows + 1);
         h.col_idx.assign(ci, ci + nblocks);
@@ -403,7 +412,7 @@ extern "C" DV_API int dv_matrix_create_duvi_soa(dv_context *ctx, int32_t n_rows,
         }
         for (int64_t i = 0; i < nnz; ++i) DV_REQUIRE(h.vidx[i] < (uint64_t)nuniq, DV_ERR_FORMAT, "value index out of range");
         m->nuniq = nuniq;
-        finish_duvi_upload(m.get(), ctx->stream);
+        finish_duvi_upload(m.get(), h, ctx->stream);
         *out = m.release();
     });
 }

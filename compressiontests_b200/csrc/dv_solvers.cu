@@ -408,7 +408,7 @@ extern "C" DV_API int dv_pcg_destroy(dv_pcg *s) {
 template <class T>
 static std::unique_ptr<VCycle<T>> build_vcycle(dv_context *ctx, SolverWs &ws, int32_t L, const dv_csr_host *A,
                                                const dv_csr_host *P, const dv_mgpcg_config &cfg,
-                                               std::vector<double> &omega_eff) {
+                                               std::vector<double> &omega_eff, const DuviHost *encoded0) {
     auto v = std::make_unique<VCycle<T>>();
     v->ctx = ctx;
     v->nu = cfg.nu;
@@ -422,7 +422,7 @@ static std::unique_ptr<VCycle<T>> build_vcycle(dv_context *ctx, SolverWs &ws, in
         DV_REQUIRE(P[l].n_rows == A[l].n_rows && P[l].n_cols == A[l + 1].n_rows, DV_ERR_ARG,
                    "prolongation shape does not match the levels");
         lv.n = A[l].n_rows;
-        lv.A.reset(dv_matrix_build(ctx, A[l], cfg.format, prec, 0, 1e-10));
+        lv.A.reset(dv_matrix_build(ctx, A[l], cfg.format, prec, 0, 1e-10, l == 0 ? encoded0 : nullptr));
         lv.P.reset(dv_matrix_build(ctx, P[l], cfg.format, prec, 0, 1e-10));
         std::vector<int32_t> rp, ci;
         std::vector<double> va;
@@ -477,9 +477,17 @@ extern "C" DV_API int dv_mgpcg_create(dv_context *ctx, int32_t L, const dv_csr_h
         s->cfg = *cfg;
         s->ws = std::make_unique<SolverWs>(ctx);
         s->n = A[0].n_rows;
-        s->Aout.reset(dv_matrix_build(ctx, A[0], cfg->outer_format, DV_F64, 0, 1e-10));
-        if (cfg->precision == DV_MIXED) s->v32 = build_vcycle<float>(ctx, *s->ws, L, A, P, *cfg, s->omega_eff);
-        else s->v64 = build_vcycle<double>(ctx, *s->ws, L, A, P, *cfg, s->omega_eff);
+        // the finest operator is encoded once for the outer matrix and the V-cycle's level 0
+        const bool outer_duvi = cfg->outer_format == DV_FORMAT_DUVI, inner_duvi = cfg->format == DV_FORMAT_DUVI;
+        DuviHost h0;
+        if (outer_duvi && inner_duvi) {
+            dv_check_csr(A[0]);
+            dv_encode_duvi(A[0], 1e-10, 0, h0);
+        }
+        const DuviHost *shared = outer_duvi && inner_duvi ? &h0 : nullptr;
+        s->Aout.reset(dv_matrix_build(ctx, A[0], cfg->outer_format, DV_F64, 0, 1e-10, shared));
+        if (cfg->precision == DV_MIXED) s->v32 = build_vcycle<float>(ctx, *s->ws, L, A, P, *cfg, s->omega_eff, shared);
+        else s->v64 = build_vcycle<double>(ctx, *s->ws, L, A, P, *cfg, s->omega_eff, shared);
         const size_t nb = 8 * (size_t)s->n;
         s->b.alloc(nb); s->x.alloc(nb); s->r.alloc(nb); s->p.alloc(nb); s->q.alloc(nb);
         if (cfg->precision == DV_MIXED) s->r32.alloc(4 * (size_t)s->n);
