@@ -1015,6 +1015,49 @@ void dv_csr_transpose(const dv_csr_host &a, std::vector<int32_t> &rp, std::vecto
     rp.assign((size_t)a.n_cols + 1, 0);
     ci.resize(nnz);
     va.resize(nnz);
+#ifdef _OPENMP
+    const int64_t nc = std::max<int32_t>(a.n_cols, 1);
+    const int T = (int)std::min<int64_t>(omp_get_max_threads(), std::max<int64_t>(1, ((int64_t)1 << 26) / nc));
+    if (T > 1 && nnz >= ((int64_t)1 << 20)) {
+        // Thread t counts, then places, the entries of rows [n t / T, n (t + 1) / T): inside a
+        // column its entries follow those of threads before it, so every transposed row
+        // lists its entries by increasing original row, as the sequential pass does.
+        std::vector<int32_t> cnt((size_t)T * nc, 0);
+        auto rows = [&](int t) {
+            return std::make_pair((int32_t)((int64_t)a.n_rows * t / T), (int32_t)((int64_t)a.n_rows * (t + 1) / T));
+        };
+#pragma omp parallel for schedule(static, 1)
+        for (int t = 0; t < T; ++t) {
+            int32_t *ct = cnt.data() + (size_t)t * nc;
+            const auto [r0, r1] = rows(t);
+            for (int64_t k = a.rowptr[r0]; k < a.rowptr[r1]; ++k) ct[a.col[k]]++;
+        }
+#pragma omp parallel for schedule(static)
+        for (int64_t c = 0; c < a.n_cols; ++c) {
+            int32_t run = 0;
+            for (int t = 0; t < T; ++t) {
+                const int32_t v = cnt[(size_t)t * nc + c];
+                cnt[(size_t)t * nc + c] = run;
+                run += v;
+            }
+            rp[c + 1] = run;
+        }
+        for (int32_t c = 0; c < a.n_cols; ++c) rp[c + 1] += rp[c];
+#pragma omp parallel for schedule(static, 1)
+        for (int t = 0; t < T; ++t) {
+            int32_t *ct = cnt.data() + (size_t)t * nc;
+            const auto [r0, r1] = rows(t);
+            for (int32_t r = r0; r < r1; ++r)
+                for (int32_t k = a.rowptr[r]; k < a.rowptr[r + 1]; ++k) {
+                    const int32_t c = a.col[k];
+                    const int64_t pos = rp[c] + ct[c]++;
+                    ci[pos] = r;
+                    va[pos] = a.val[k];
+                }
+        }
+        return;
+    }
+#endif
     for (int64_t k = 0; k < nnz; ++k) rp[a.col[k] + 1]++;
     for (int32_t i = 0; i < a.n_cols; ++i) rp[i + 1] += rp[i];
     std::vector<int32_t> fill(rp.begin(), rp.end() - 1);
