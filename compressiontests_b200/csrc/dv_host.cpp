@@ -716,6 +716,11 @@ bool dv_dense_inverse(int32_t n, std::vector<double> &a, double pivot_tol) {
             f[(size_t)i * n + j] = s / d;
         }
     }
+    // the strict upper triangle is free after the factorisation: L^T there lets the
+    // backward substitution read rows instead of columns (same operations, same order)
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int32_t i = 0; i < n; ++i)
+        for (int32_t k = i + 1; k < n; ++k) f[(size_t)i * n + k] = f[(size_t)k * n + i];
 #pragma omp parallel for schedule(dynamic, 8)
     for (int32_t c = 0; c < n; ++c) {
         std::vector<double> x(n, 0.0);
@@ -729,7 +734,8 @@ bool dv_dense_inverse(int32_t n, std::vector<double> &a, double pivot_tol) {
         for (int32_t i = 0; i < n; ++i) x[i] /= f[(size_t)i * n + i];
         for (int32_t i = n - 1; i >= 0; --i) {
             double s = x[i];
-            for (int32_t k = i + 1; k < n; ++k) s -= f[(size_t)k * n + i] * x[k];
+            const double *lti = &f[(size_t)i * n];
+            for (int32_t k = i + 1; k < n; ++k) s -= lti[k] * x[k];
             x[i] = s;
         }
         for (int32_t i = 0; i < n; ++i) a[(size_t)i * n + c] = x[i];
