@@ -310,3 +310,19 @@ def test_units_reject_unrepresentable_rows_and_malformed_streams(native):
         native.units_decode(H.shape, bad)
     with pytest.raises(native.DuviError):   # one row too few
         native.units_decode((H.shape[0] + 1, H.shape[1]), u)
+
+
+def test_host_encoders_reproduce_golden_vectors(native):
+    # tests/golden/oracle_small.npz (committed, made by tests/golden/make_golden.py): the
+    # product's DuVi SoA encoder and Unit-stream encoder on the fixture's stiffness matrix
+    # give the committed arrays byte for byte.
+    import scipy.sparse as sp
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "oracle_small.npz"))
+    n = g["kff_rowptr"].size - 1
+    K = sp.csr_matrix((g["kff_val"], g["kff_col"], g["kff_rowptr"]), shape=(n, n))
+    d = native.duvi_encode(K)
+    for k in ("row_to_col", "row_to_dist", "col_idx", "dist", "vidx", "values"):
+        np.testing.assert_array_equal(d[k], g["duvi_" + k], err_msg=k)
+    u = native.units_encode(K)
+    np.testing.assert_array_equal(u["bytes"], g["units_bytes"])
+    np.testing.assert_array_equal(u["vidx"], g["units_vidx"])
