@@ -9,6 +9,7 @@
 #pragma once
 
 #include <cstddef>
+#include <mutex>
 
 #include "dv_internal.cuh"
 
@@ -28,16 +29,45 @@ static_assert(kStageC >= kBundleBlocks + 8, "column stage too small");
 
 // The dynamic shared memory a kernel may use is an attribute of each device: a
 // launcher raises it to every new largest size on each device it launches on.
+// Host threads may launch on several contexts at once: the caches of launch settings
+// below are updated under one lock, so a raise never lowers a limit another thread set.
+inline std::mutex &launch_cache_mutex() {
+    static std::mutex m;
+    return m;
+}
+
 constexpr int kMaxDevices = 64;
 struct SmemLimit {
     size_t set[kMaxDevices] = {};
     template <class K>
     void raise(K kern, size_t smem, int device) {
         DV_REQUIRE(device >= 0 && device < kMaxDevices, DV_ERR_ARG, "device ordinal out of range");
+        std::lock_guard<std::mutex> lock(launch_cache_mutex());
         if (smem > set[device]) {
             DV_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             set[device] = smem;
         }
+    }
+};
+
+// Resident blocks per SM of a kernel at a dynamic shared-memory size (occupancy query,
+// remembered for the last few sizes).
+struct OccupancyCache {
+    size_t smem[4] = {};
+    int blocks[4] = {};
+    int next = 0;
+    template <class K>
+    int get(K kern, int threads, size_t smem_bytes) {
+        std::lock_guard<std::mutex> lock(launch_cache_mutex());
+        for (int i = 0; i < 4; ++i)
+            if (blocks[i] > 0 && smem[i] == smem_bytes) return blocks[i];
+        int occ = 0;
+        DV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, threads, smem_bytes));
+        occ = std::max(occ, 1);
+        smem[next] = smem_bytes;
+        blocks[next] = occ;
+        next = (next + 1) % 4;
+        return occ;
     }
 };
 
@@ -875,18 +905,8 @@ void launch_duvi_pattern_gbs(const LaunchEnv &e, const dv_matrix *m, Gather g, O
     limit.raise(kern, smem, e.ctx->device);
     // Whole waves: past one wave of resident blocks (SMs x blocks per SM at this table size
     // and register count), a multiple of it, so that the last wave is not a partial one.
-    static size_t occ_smem[4] = {};
-    static int occ_val[4] = {}, occ_next = 0;
-    int occ = 0;
-    for (int i = 0; i < 4; ++i)
-        if (occ_smem[i] == smem) occ = occ_val[i];
-    if (occ == 0) {
-        DV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 256, smem));
-        occ = std::max(occ, 1);
-        occ_smem[occ_next] = smem;
-        occ_val[occ_next] = occ;
-        occ_next = (occ_next + 1) % 4;
-    }
+    static OccupancyCache occupancy;   // per instantiation
+    const int occ = occupancy.get(kern, 256, smem);
     const int64_t ng = m->n_rows / G;
     const int64_t need = std::max<int64_t>(1, (ng + 255) / 256), wave = (int64_t)e.ctx->num_sms * occ;
     const int64_t cap = std::min<int64_t>(need, e.max_blocks);
