@@ -326,3 +326,22 @@ def test_host_encoders_reproduce_golden_vectors(native):
     u = native.units_encode(K)
     np.testing.assert_array_equal(u["bytes"], g["units_bytes"])
     np.testing.assert_array_equal(u["vidx"], g["units_vidx"])
+
+
+def test_duvi_host_encoder_index_widths(native, oracle, rng):
+    # value_index_bits 0 picks the narrowest width; a wider forced width keeps the same
+    # indices; a width too narrow for the distinct values is a format error
+    import scipy.sparse as sp
+    A = _random_csr(rng, 400, 20, np.round(rng.standard_normal(8000), 3))   # ~2,000 distinct values
+    auto = native.duvi_encode(A)
+    assert auto["vi_bits"] == 16
+    wide = native.duvi_encode(A, 32)
+    assert wide["vi_bits"] == 32
+    np.testing.assert_array_equal(wide["vidx"], auto["vidx"])
+    _encode_matches_oracle(native, oracle, A, bits=16)
+    with pytest.raises(native.DuviError) as e:
+        native.duvi_encode(A, 8)
+    assert e.value.status == native._native.DV_ERR_FORMAT
+    with pytest.raises(native.DuviError) as e:
+        native.duvi_encode(A, 12)
+    assert e.value.status == native._native.DV_ERR_ARG
