@@ -66,6 +66,7 @@ def parse():
     p.add_argument("--adjoint-only", action="store_true", help="only the adjoint section (96x48x48)")
     p.add_argument("--no-gs", action="store_true", help="skip the Gauss-Seidel-smoothed MG-PCG lines")
     p.add_argument("--no-adjoint", action="store_true", help="skip the adjoint section")
+    p.add_argument("--no-pcg", action="store_true", help="skip the Jacobi-PCG section (16^3, CSR and DuVi)")
     p.add_argument("--batch-size", type=int, default=64, help="mesh edge of the multi-load-case section")
     p.add_argument("--batch-k", type=int, default=64, help="load cases of the multi-load-case section")
     p.add_argument("--batch-meshes", type=int, default=32, help="meshes of the batched-mesh section")
@@ -440,6 +441,13 @@ def run_ours(args):
     if not args.no_adjoint and extras:
         adjoint = adjoint_section(cb, ctx, stream, max(1, min(5, args.steps // 2)), 1e-10)
 
+    jacobi_pcg = None
+    if not args.no_pcg and extras:
+        try:   # a reported extra: a failure here is recorded, not fatal to the headline line
+            jacobi_pcg = jacobi_pcg_section(cb, ctx, 16, max(1, min(5, args.steps // 2)))
+        except Exception as e:
+            jacobi_pcg = {"error": f"{type(e).__name__}: {e}"}
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         try:
@@ -466,7 +474,7 @@ def run_ours(args):
             "iterations": its_mixed[-1], "relative_residual_fp64": true_rel,
             "e2e": {"value": round(ms_e2e, 3), "unit": "ms", "h2d_bytes_per_step": int(8 * nf),
                     "d2h_bytes_per_step": int(8 * nf)},
-            "gpu_launches": int(launches), "fp64": fp64, "spmv": spmv, "gauss_seidel": gauss_seidel, "batched": batched, "adjoint": adjoint, "roofline": roof,
+            "gpu_launches": int(launches), "fp64": fp64, "spmv": spmv, "gauss_seidel": gauss_seidel, "batched": batched, "adjoint": adjoint, "jacobi_pcg": jacobi_pcg, "roofline": roof,
             "cpu_baseline": cpu,
             "clocks": clocks, "setup_s": {"hierarchy": round(t_build, 1), "solver": round(t_setup, 1)},
         }
@@ -579,6 +587,32 @@ def batched_meshes(cb, ctx, stream, n_meshes, steps, tol):
             "speedup_vs_sequential": round(ms_seq / ms_batch, 2), "gpu_launches_per_solve": int(launches),
             "launches_per_graph_chunk": info["launches_per_chunk"],
             "setup_s": {"hierarchies": round(t_build, 1), "solver": round(t_setup, 1)}}
+
+
+def jacobi_pcg_section(cb, ctx, n, reps, tol=1e-8):
+    """Jacobi-PCG (OpenCLCsrPcgSolver's algorithm) on the n^3 cantilever, unit traction, FP64, to the
+    reference's stop test max |r_i| <= tol, CSR then DuVi: the solver's device time per solve, the
+    time through the host API (b in, x out) and the FP64 relative residual of the result."""
+    ne = (n, n, n)
+    A = cb.hex_stiffness(ne)
+    b = cb.traction_rhs(ne)
+    out = {"workload": f"Jacobi-PCG, {n}^3 cantilever, unit traction, FP64, stop max|r_i| <= {tol:g}",
+           "n_dofs": int(A.shape[0])}
+    for fmt in ("csr", "duvi"):
+        s = cb.CudaCsrPcgSolver(ctx, 20000, tol, fmt=fmt).Initialize(A=A, b=b)
+        s.Solve()   # warm-up (the first call captures the iteration graph)
+        dev, host = [], []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            x, st = s.Solve()
+            host.append((time.perf_counter() - t0) * 1e3)
+            dev.append(st.SolveMilliseconds)
+        rel = float(np.linalg.norm(b - A @ x) / np.linalg.norm(b))
+        out[fmt] = {"device_ms": round(min(dev), 3) if np.isfinite(min(dev)) else None,
+                    "host_api_ms": round(min(host), 3), "iterations": st.NumIterationsRequired,
+                    "converged": st.HasConverged, "relative_residual_fp64": rel if np.isfinite(rel) else None}
+        s.release()
+    return out
 
 
 def adjoint_section(cb, ctx, stream, steps, tol):
