@@ -215,6 +215,7 @@ extern "C" DV_API int dv_units_decode(int32_t n_rows, int32_t n_cols, const uint
                                ((int64_t)bytes[o + 2] << 8) | bytes[o + 3]);
                 o += 4;
             }
+            DV_REQUIRE(gap > 0 || (h & 1), DV_ERR_FORMAT, "columns of a row not increasing (zero gap between units)");
             c += gap;
             put(c);
             const int w = 1 << cls;
@@ -223,6 +224,7 @@ extern "C" DV_API int dv_units_decode(int32_t n_rows, int32_t n_cols, const uint
                 uint32_t step = 0;
                 for (int q = 0; q < w; ++q) step |= (uint32_t)bytes[o + q] << (8 * q);
                 o += w;
+                DV_REQUIRE(step > 0, DV_ERR_FORMAT, "columns of a row not increasing (zero step)");
                 c += step;
                 put(c);
             }

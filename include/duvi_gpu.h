@@ -150,7 +150,8 @@ DV_API int dv_units_encode(const dv_csr_host *a, double dedup_tol, int64_t *n_un
 /* Unit stream back to CSR, walking the units as DuViCompressedSparseMatrix.Multiply does
  * (:419-441): *nnz with rowptr == NULL, then rowptr[n_rows + 1], col[nnz], val[nnz].  An
  * empty row comes back as one entry (column 0, value of its index: 0.0).  Malformed streams
- * (truncated units, columns past n_cols, index or row counts that do not match): DV_ERR_FORMAT. */
+ * (truncated units, columns past n_cols or not increasing within a row, index or row counts
+ * that do not match): DV_ERR_FORMAT. */
 DV_API int dv_units_decode(int32_t n_rows, int32_t n_cols, const uint8_t *bytes, int64_t n_bytes,
                            const int32_t *value_indices, int64_t n_indices, const double *values, int64_t nuniq,
                            int64_t *nnz, int32_t *rowptr, int32_t *col, double *val);

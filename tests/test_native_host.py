@@ -310,6 +310,13 @@ def test_units_reject_unrepresentable_rows_and_malformed_streams(native):
         native.units_decode(H.shape, bad)
     with pytest.raises(native.DuviError):   # one row too few
         native.units_decode((H.shape[0] + 1, H.shape[1]), u)
+    # a zero column step (the first unit of row 0 has steps of one byte after its 3 header bytes)
+    b = u["bytes"].copy()
+    assert b[0] == 1 and b[1] > 0 and b[2] < 0x80
+    b[3] = 0
+    with pytest.raises(native.DuviError) as e:
+        native.units_decode(H.shape, dict(u, bytes=b))
+    assert "increasing" in str(e.value)
 
 
 def test_host_encoders_reproduce_golden_vectors(native):
