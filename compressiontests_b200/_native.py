@@ -23,12 +23,12 @@ DV_ERR_NOMEM = -5
 DV_ERR_FORMAT = -6
 DV_ERR_NO_DEVICE = -7
 DV_ERR_SINGULAR = -8
-DV_ERR_TIMEOUT = -9
 
 FORMAT_CSR, FORMAT_DUVI = 0, 1
 F64, F32, MIXED = 0, 1, 2
 SMOOTHER_JACOBI, SMOOTHER_GS_LEX, SMOOTHER_GS_COLOR = 0, 1, 2
 OMEGA_ABSOLUTE, OMEGA_SPECTRAL = 0, 1
+TOL_ABS_MAX, TOL_REL_L2 = 0, 1
 
 
 class DuviError(RuntimeError):
@@ -58,7 +58,7 @@ class CsrHost(C.Structure):
 
 class Stats(C.Structure):
     _fields_ = [("iterations", C.c_int32), ("converged", C.c_int32), ("failed", C.c_int32),
-                ("device_status", C.c_int32), ("residual_max", C.c_double), ("residual_norm2", C.c_double),
+                ("reserved", C.c_int32), ("residual_max", C.c_double), ("residual_norm2", C.c_double),
                 ("relative_residual", C.c_double), ("solve_ms", C.c_double)]
 
 
@@ -111,6 +111,7 @@ _SIGNATURES = {
     "dv_gmg_destroy": (C.c_int, [_vp]),
     "dv_pcg_create": (C.c_int, [_vp, _P(CsrHost), C.c_int32, C.c_int32, C.c_double, _P(_vp)]),
     "dv_pcg_solve": (C.c_int, [_vp, _vp, _vp, _vp, _P(Stats)]),
+    "dv_pcg_set_tolerance_kind": (C.c_int, [_vp, C.c_int32]),
     "dv_pcg_destroy": (C.c_int, [_vp]),
     "dv_pcg_solve_noalloc": (C.c_int, [_vp, _vp, _vp, C.c_int32, C.c_int32, C.c_double, _P(Stats)]),
     "dv_mgpcg_create": (C.c_int, [_vp, C.c_int32, _P(CsrHost), _P(CsrHost), _P(MgpcgConfig), _P(_vp)]),

@@ -564,7 +564,7 @@ void batch_solve_impl(dv_batch *B, BCycle<T> &vc, int32_t *conv_per_mesh, int32_
         stats->iterations = h.it;
         stats->converged = all && !h.failed;
         stats->failed = h.failed;
-        stats->device_status = 0;
+        stats->reserved = 0;
         stats->residual_max = NAN;
         stats->residual_norm2 = worst_abs;
         stats->relative_residual = worst;

@@ -28,6 +28,18 @@ static int grid_n(dv_context *ctx, int64_t n) {
     return (int)std::max<int64_t>(1, std::min<int64_t>(b, ctx->num_sms * 8));
 }
 
+// ||v||^2 into sc->bb (slot 0) or sc->rr (slot 1), for the exit check of a solve.
+static __global__ void k_gmg_norm2(const double *__restrict__ v, int32_t n, SolverScalars *sc, int slot,
+                                   double *partials, unsigned *ticket) {
+    double red[1] = {0.0};
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) red[0] += v[i] * v[i];
+    double t[1];
+    if (grid_reduce<1, 0>(red, partials, ticket, t)) {
+        if (slot == 0) sc->bb = t[0];
+        else sc->rr = t[0];
+    }
+}
+
 // ---------------------------------------------------------------------------
 // solver object
 // ---------------------------------------------------------------------------
@@ -255,7 +267,20 @@ extern "C" DV_API int dv_gmg_solve(dv_gmg *g, const double *b, const double *x0,
         }
         DV_CUDA(cudaEventRecord(e1, s));
         DV_CUDA(cudaMemcpyAsync(x, L0.x.p, nb, cudaMemcpyDeviceToHost, s));
-        DV_CUDA(cudaStreamSynchronize(s));
+        // relative residual of the returned x, recomputed in FP64: r = b - A x, ||r||^2 and ||b||^2
+        {
+            LaunchEnv ec = ws.env(false);
+            OpResid<double> op{{}, L0.b.as<double>(), L0.r.as<double>()};
+            launch_rows<double>(ec, L0.A.get(), GatherVec<double, double>{L0.x.as<double>()}, op);
+            k_gmg_norm2<<<grid_n(ctx, L0.n), kThreads, 0, s>>>(L0.r.as<double>(), L0.n, ws.sc(), 1, ec.partials,
+                                                              ec.ticket);
+            DV_CUDA(cudaGetLastError());
+            k_gmg_norm2<<<grid_n(ctx, L0.n), kThreads, 0, s>>>(L0.b.as<double>(), L0.n, ws.sc(), 0, ec.partials,
+                                                              ec.ticket);
+            DV_CUDA(cudaGetLastError());
+            ctx->count(2);
+        }
+        ws.pull();
         float ms = 0;
         cudaEventElapsedTime(&ms, e0, e1);
         cudaEventDestroy(e0);
@@ -264,10 +289,10 @@ extern "C" DV_API int dv_gmg_solve(dv_gmg *g, const double *b, const double *x0,
             stats->iterations = h.cycle;
             stats->converged = h.converged;
             stats->failed = h.failed;
-            stats->device_status = 0;
+            stats->reserved = 0;
             stats->residual_max = h.res_max;
             stats->residual_norm2 = h.res_norm2;
-            stats->relative_residual = NAN;
+            stats->relative_residual = h.bb > 0 ? std::sqrt(h.rr / h.bb) : (h.rr > 0 ? INFINITY : 0.0);
             stats->solve_ms = ms;
         }
     });

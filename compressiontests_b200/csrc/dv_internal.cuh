@@ -104,10 +104,26 @@ struct dv_context {
     cudaStream_t stream = nullptr;
     int num_sms = 0;
     int max_smem_optin = 0;
-    int64_t launches = 0;
-    DevMem status;       // int[4]: device error word, bounded-wait sentinel
+    // Kernel launches, counted by where they go: work done for the caller (dv_context_launch_count),
+    // the autotuner's trial launches at matrix upload, and launches recorded into a CUDA graph
+    // (counted into `launches` each time the graph runs).
+    enum CountInto { kCountWork = 0, kCountTuning = 1, kCountCapture = 2 };
+    int64_t launches = 0, tuning_launches = 0, captured_launches = 0;
+    int count_into = kCountWork;
     DevMem red;          // default grid-reduction workspace (ticket + partials)
-    void count(int64_t n = 1) { launches += n; }
+    void count(int64_t n = 1) {
+        if (count_into == kCountTuning) tuning_launches += n;
+        else if (count_into == kCountCapture) captured_launches += n;
+        else launches += n;
+    }
+};
+
+// Sends the context's launch counts to `into` while in scope.
+struct CountScope {
+    dv_context *ctx;
+    int saved;
+    CountScope(dv_context *c, int into) : ctx(c), saved(c->count_into) { c->count_into = into; }
+    ~CountScope() { ctx->count_into = saved; }
 };
 
 void dv_ctx_check(dv_context *ctx);   // throws DV_ERR_NO_DEVICE / DV_ERR_CUDA
@@ -214,6 +230,7 @@ struct dv_matrix {
     int row_group = 1;         // g consecutive rows share one column list (node dofs); 1 otherwise
     DevMem diag;               // FP64 diagonal (0 where absent)
     std::vector<double> host_diag;
+    int zero_diag = 0;         // 1 when a diagonal entry is 0 or absent (square matrices)
     int64_t device_bytes = 0;
 };
 

@@ -50,23 +50,25 @@ struct SmemLimit {
     }
 };
 
-// Resident blocks per SM of a kernel at a dynamic shared-memory size (occupancy query,
-// remembered for the last few sizes).
+// Resident blocks per SM of a kernel at a dynamic shared-memory size on a device (occupancy
+// query, remembered for the last few (device, size) pairs; the current device is `device`).
 struct OccupancyCache {
-    size_t smem[4] = {};
-    int blocks[4] = {};
+    size_t smem[8] = {};
+    int dev[8] = {};
+    int blocks[8] = {};
     int next = 0;
     template <class K>
-    int get(K kern, int threads, size_t smem_bytes) {
+    int get(K kern, int threads, size_t smem_bytes, int device) {
         std::lock_guard<std::mutex> lock(launch_cache_mutex());
-        for (int i = 0; i < 4; ++i)
-            if (blocks[i] > 0 && smem[i] == smem_bytes) return blocks[i];
+        for (int i = 0; i < 8; ++i)
+            if (blocks[i] > 0 && smem[i] == smem_bytes && dev[i] == device) return blocks[i];
         int occ = 0;
         DV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, threads, smem_bytes));
         occ = std::max(occ, 1);
         smem[next] = smem_bytes;
+        dev[next] = device;
         blocks[next] = occ;
-        next = (next + 1) % 4;
+        next = (next + 1) % 8;
         return occ;
     }
 };
@@ -906,7 +908,7 @@ void launch_duvi_pattern_gbs(const LaunchEnv &e, const dv_matrix *m, Gather g, O
     // Whole waves: past one wave of resident blocks (SMs x blocks per SM at this table size
     // and register count), a multiple of it, so that the last wave is not a partial one.
     static OccupancyCache occupancy;   // per instantiation
-    const int occ = occupancy.get(kern, 256, smem);
+    const int occ = occupancy.get(kern, 256, smem, e.ctx->device);
     const int64_t ng = m->n_rows / G;
     const int64_t need = std::max<int64_t>(1, (ng + 255) / 256), wave = (int64_t)e.ctx->num_sms * occ;
     const int64_t cap = std::min<int64_t>(need, e.max_blocks);

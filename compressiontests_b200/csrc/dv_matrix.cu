@@ -21,7 +21,6 @@ extern "C" DV_API const char *dv_status_string(int s) {
         case DV_ERR_FORMAT: return "format error";
         case DV_ERR_NO_DEVICE: return "no CUDA device";
         case DV_ERR_SINGULAR: return "singular matrix";
-        case DV_ERR_TIMEOUT: return "device wait timed out";
         default: return "unknown status";
     }
 }
@@ -49,7 +48,6 @@ extern "C" DV_API int dv_context_create(int device, dv_context **out) {
         ctx->num_sms = prop.multiProcessorCount;
         ctx->max_smem_optin = (int)prop.sharedMemPerBlockOptin;
         DV_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
-        ctx->status.alloc(64);
         ctx->red.alloc(sizeof(double) * dvk::kMaxRed * ctx->num_sms * 16 + 64);
         *out = ctx.release();
     });
@@ -60,7 +58,6 @@ extern "C" DV_API int dv_context_destroy(dv_context *ctx) {
         if (!ctx) return;
         cudaSetDevice(ctx->device);
         cudaStreamSynchronize(ctx->stream);
-        ctx->status.release();
         ctx->red.release();
         cudaStreamDestroy(ctx->stream);
         delete ctx;
@@ -245,8 +242,22 @@ static void autotune(dv_matrix *m) {
     if (m->n_rows < 100000 || m->n_rows != m->n_cols) return;
     dv_context *ctx = m->ctx;
     cudaStream_t s = ctx->stream;
+    CountScope tuning(ctx, dv_context::kCountTuning);   // trial launches are not part of any solve
     const size_t vs = m->precision == DV_F64 ? 8 : 4;
     DevMem x(vs * (size_t)m->n_cols), y(vs * (size_t)m->n_rows);
+    {   // a representative x: values of one sign and magnitude ~1 (1 + i/n)
+        const int32_t nc = m->n_cols;
+        if (m->precision == DV_F64) {
+            std::vector<double> h(nc);
+            for (int32_t i = 0; i < nc; ++i) h[i] = 1.0 + (double)i / nc;
+            upload(x, h.data(), 8 * (size_t)nc, s);
+        } else {
+            std::vector<float> h(nc);
+            for (int32_t i = 0; i < nc; ++i) h[i] = 1.0f + (float)i / nc;
+            upload(x, h.data(), 4 * (size_t)nc, s);
+        }
+        DV_CUDA(cudaStreamSynchronize(s));
+    }
     auto e = env_for(ctx);
     auto run = [&] {
         if (m->precision == DV_F64) {
@@ -297,7 +308,6 @@ static void autotune(dv_matrix *m) {
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     apply(best_v);
-    ctx->launches -= (int64_t)cand.size() * 4;   // tuning launches are not part of any solve
 }
 
 dv_matrix *dv_matrix_build(dv_context *ctx, const dv_csr_host &a, int format, int precision, int vi_bits, double tol,
@@ -340,6 +350,7 @@ dv_matrix *dv_matrix_build(dv_context *ctx, const dv_csr_host &a, int format, in
     }
     if (a.n_rows == a.n_cols) {
         dv_extract_diag(a, m->host_diag);
+        m->zero_diag = std::any_of(m->host_diag.begin(), m->host_diag.end(), [](double d) { return d == 0.0; });
         upload(m->diag, m->host_diag.data(), 8 * m->host_diag.size(), s);
         DV_CUDA(cudaStreamSynchronize(s));
     }

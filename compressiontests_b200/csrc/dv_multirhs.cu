@@ -447,7 +447,7 @@ void multi_solve(dv_mgpcg *s, VCycle<T> &vc, MultiState<T> &M, int k, const doub
         stats->iterations = h.it;
         stats->converged = all && !h.failed;
         stats->failed = h.failed;
-        stats->device_status = 0;
+        stats->reserved = 0;
         stats->residual_max = NAN;
         stats->residual_norm2 = worst_abs;
         stats->relative_residual = worst;

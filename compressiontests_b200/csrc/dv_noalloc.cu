@@ -20,7 +20,14 @@
 //  - the array keeps the previous call's contents; the call clears what must
 //    start from zero (the reduction ticket) and initialises the rest;
 //  - the first call on a device looks up the array's device address
-//    (cudaGetSymbolAddress); make that first call before any stream capture.
+//    (cudaGetSymbolAddress); make that first call before any stream capture;
+//  - the array, like the kernels' code, is device memory that CUDA allocates
+//    when it loads this part of the library.  Under CUDA's default lazy module
+//    loading that happens at the first call on each device (and a kernel's code
+//    at its first launch), not when the context is created.  A caller that
+//    reserves all free device memory should either make one call with each
+//    matrix format it will use before reserving it, or run with
+//    CUDA_MODULE_LOADING=EAGER, which loads everything when CUDA initialises.
 #include "dv_kernels.cuh"
 
 #include <chrono>
@@ -121,6 +128,21 @@ __global__ void k_na_p(const double *__restrict__ z, double *__restrict__ p, int
     for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = z[i] + b * p[i];
 }
 
+// ||b||^2 and ||r||^2 of the exit check (r = b - A x recomputed in FP64).
+__global__ void k_na_norms(const double *__restrict__ b, const double *__restrict__ r, int32_t n, SolverScalars *sc,
+                           double *partials, unsigned *ticket) {
+    double red[2] = {0.0, 0.0};
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        red[0] += b[i] * b[i];
+        red[1] += r[i] * r[i];
+    }
+    double t[2];
+    if (grid_reduce<2, 0>(red, partials, ticket, t)) {
+        sc->bb = t[0];
+        sc->rr = t[1];
+    }
+}
+
 }  // namespace
 
 extern "C" DV_API int dv_pcg_solve_noalloc(dv_matrix *A, const double *d_b, double *d_x, int32_t use_x0,
@@ -132,7 +154,7 @@ extern "C" DV_API int dv_pcg_solve_noalloc(dv_matrix *A, const double *d_b, doub
         DV_REQUIRE(A->n_rows <= kNoAllocMaxRows, DV_ERR_ARG,
                    "system larger than the allocation-free limit of 131072 rows; use dv_pcg_solve");
         DV_REQUIRE(max_iterations >= 0 && tol >= 0, DV_ERR_ARG, "bad iteration limit or tolerance");
-        for (double d : A->host_diag) DV_REQUIRE(d != 0.0, DV_ERR_SINGULAR, "zero diagonal entry");
+        DV_REQUIRE(!A->zero_diag, DV_ERR_SINGULAR, "zero diagonal entry");
         dv_context *ctx = A->ctx;
         dv_ctx_check(ctx);
         const auto t0 = std::chrono::steady_clock::now();
@@ -187,14 +209,24 @@ extern "C" DV_API int dv_pcg_solve_noalloc(dv_matrix *A, const double *d_b, doub
             DV_CUDA(cudaStreamSynchronize(st));
             if (h.done) break;
         }
+        // relative residual of the returned x in FP64: z = b - A x (z is free now), ||b||, ||z||
+        {
+            OpResid<double> op{{}, d_b, z};
+            launch_rows<double>(e, A, GatherVec<double, double>{d_x}, op);
+            k_na_norms<<<grid, kThreads, 0, st>>>(d_b, z, n, sc, partials, ticket);
+            DV_CUDA(cudaGetLastError());
+            ctx->count();
+            DV_CUDA(cudaMemcpyAsync(&h, sc, sizeof(h), cudaMemcpyDeviceToHost, st));
+            DV_CUDA(cudaStreamSynchronize(st));
+        }
         if (stats) {
             stats->iterations = h.it;
             stats->converged = h.converged;
             stats->failed = h.failed;
-            stats->device_status = 0;
+            stats->reserved = 0;
             stats->residual_max = h.res_max;
             stats->residual_norm2 = h.res_norm2;
-            stats->relative_residual = NAN;
+            stats->relative_residual = h.bb > 0 ? std::sqrt(h.rr / h.bb) : (h.rr > 0 ? INFINITY : 0.0);
             stats->solve_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
         }
     });

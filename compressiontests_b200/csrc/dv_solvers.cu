@@ -63,17 +63,20 @@ void SolverWs::run_chunk(const std::function<void()> &body, bool use_graph, int 
         if (g.key == key) c = &g;
     if (!c) {
         cudaGraph_t g;
-        int64_t before = ctx->launches;
-        DV_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-        try {
-            body();
-        } catch (...) {
-            cudaStreamEndCapture(s, &g);
-            throw;
+        int64_t launches = 0;
+        {
+            CountScope capture(ctx, dv_context::kCountCapture);   // counted when the graph runs
+            const int64_t before = ctx->captured_launches;
+            DV_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+            try {
+                body();
+            } catch (...) {
+                cudaStreamEndCapture(s, &g);
+                throw;
+            }
+            DV_CUDA(cudaStreamEndCapture(s, &g));
+            launches = ctx->captured_launches - before;
         }
-        DV_CUDA(cudaStreamEndCapture(s, &g));
-        const int64_t launches = ctx->launches - before;
-        ctx->launches = before;
         cudaGraphExec_t exec;
         const cudaError_t err = cudaGraphInstantiate(&exec, g, 0);
         cudaGraphDestroy(g);
@@ -105,11 +108,12 @@ __global__ void k_pcg_init(const double *__restrict__ M, const double *__restric
 }
 
 // x += a p; r -= a Ap; z = M r; convergence flags; r.z (update_x_r_z_check_r,
-// CsrCG.cl:257-277, then dot_finalize_and_calc_b, :289-301).
+// CsrCG.cl:257-277, then dot_finalize_and_calc_b, :289-301).  The stop test is the
+// reference's max |r_i| <= tol, or with rel_l2 ||r||_2 <= tol ||b||_2 (sc->bb = ||b||^2).
 __global__ void k_pcg_update(const double *__restrict__ M, const double *__restrict__ ap, const double *__restrict__ p,
                              double *__restrict__ x, double *__restrict__ r, double *__restrict__ z, int32_t n,
-                             double tol, SolverScalars *sc, const int *__restrict__ done, double *partials,
-                             unsigned *ticket) {
+                             double tol, int rel_l2, SolverScalars *sc, const int *__restrict__ done,
+                             double *partials, unsigned *ticket) {
     if (*(volatile const int *)done) return;
     const double a = sc->alpha;
     double red[4] = {0.0, 0.0, 0.0, 0.0};   // max|r|, failed flag, r.z, r.r
@@ -128,7 +132,7 @@ __global__ void k_pcg_update(const double *__restrict__ M, const double *__restr
     double t[4];
     if (grid_reduce<4, 0b0011>(red, partials, ticket, t)) {
         bool failed = t[1] != 0.0;
-        bool converged = !failed && t[0] <= tol;
+        bool converged = !failed && (rel_l2 ? t[3] <= tol * tol * sc->bb : t[0] <= tol);
         sc->res_max = t[0];
         sc->res_norm2 = sqrt(t[3]);
         sc->converged = converged;
@@ -291,8 +295,18 @@ struct dv_pcg {
     std::unique_ptr<SolverWs> ws;
     int32_t n = 0, max_iter = 0;
     double tol = 0;
+    int32_t tol_kind = DV_TOL_ABS_MAX;
     DevMem M, b, x, r, z, p, ap;
 };
+
+extern "C" DV_API int dv_pcg_set_tolerance_kind(dv_pcg *s, int32_t tol_kind) {
+    return dv_guard([&] {
+        DV_REQUIRE(s != nullptr, DV_ERR_NOT_INITIALIZED, "You must call Initialize(model) first");
+        DV_REQUIRE(tol_kind == DV_TOL_ABS_MAX || tol_kind == DV_TOL_REL_L2, DV_ERR_ARG,
+                   "tol_kind must be DV_TOL_ABS_MAX or DV_TOL_REL_L2");
+        s->tol_kind = tol_kind;
+    });
+}
 
 extern "C" DV_API int dv_pcg_create(dv_context *ctx, const dv_csr_host *A, int32_t format, int32_t max_iter,
                                     double tol, dv_pcg **out) {
@@ -349,10 +363,13 @@ extern "C" DV_API int dv_pcg_solve(dv_pcg *s, const double *b, const double *x0,
             DV_CUDA(cudaMemcpyAsync(s->r.p, s->b.p, nb, cudaMemcpyDeviceToDevice, st));
         }
         const int g = grid_for(ctx, n);
+        k_norm2<<<g, kThreads, 0, st>>>(s->b.as<double>(), n, s->ws->sc(), 0, e.partials, e.ticket);   // ||b||^2
+        DV_CUDA(cudaGetLastError());
         k_pcg_init<<<g, kThreads, 0, st>>>(s->M.as<double>(), s->r.as<double>(), s->z.as<double>(), s->p.as<double>(), n,
                                           s->ws->sc(), e.partials, e.ticket);
         DV_CUDA(cudaGetLastError());
-        ctx->count();
+        ctx->count(2);
+        const int rel_l2 = s->tol_kind == DV_TOL_REL_L2;
         LaunchEnv ed = s->ws->env(true);
         const int chunk = 16;
         auto body = [&] {
@@ -361,7 +378,7 @@ extern "C" DV_API int dv_pcg_solve(dv_pcg *s, const double *b, const double *x0,
                 launch_rows<double>(ed, s->A.get(), GatherVec<double, double>{s->p.as<double>()}, op);
                 k_pcg_update<<<g, kThreads, 0, st>>>(s->M.as<double>(), s->ap.as<double>(), s->p.as<double>(),
                                                      s->x.as<double>(), s->r.as<double>(), s->z.as<double>(), n, s->tol,
-                                                     s->ws->sc(), ed.done, ed.partials, ed.ticket);
+                                                     rel_l2, s->ws->sc(), ed.done, ed.partials, ed.ticket);
                 DV_CUDA(cudaGetLastError());
                 k_pcg_p<<<g, kThreads, 0, st>>>(s->z.as<double>(), s->p.as<double>(), n, s->ws->sc(), ed.done);
                 DV_CUDA(cudaGetLastError());
@@ -375,7 +392,15 @@ extern "C" DV_API int dv_pcg_solve(dv_pcg *s, const double *b, const double *x0,
         }
         DV_CUDA(cudaEventRecord(e1, st));
         DV_CUDA(cudaMemcpyAsync(xout, s->x.p, nb, cudaMemcpyDeviceToHost, st));
-        DV_CUDA(cudaStreamSynchronize(st));
+        // relative residual of the returned x, recomputed in FP64: z = b - A x, ||z||^2
+        {
+            OpResid<double> op{{}, s->b.as<double>(), s->z.as<double>()};
+            launch_rows<double>(e, s->A.get(), GatherVec<double, double>{s->x.as<double>()}, op);
+            k_norm2<<<g, kThreads, 0, st>>>(s->z.as<double>(), n, s->ws->sc(), 1, e.partials, e.ticket);
+            DV_CUDA(cudaGetLastError());
+            ctx->count();
+        }
+        s->ws->pull();
         float ms = 0;
         cudaEventElapsedTime(&ms, e0, e1);
         cudaEventDestroy(e0);
@@ -384,10 +409,10 @@ extern "C" DV_API int dv_pcg_solve(dv_pcg *s, const double *b, const double *x0,
             stats->iterations = h.it;
             stats->converged = h.converged;
             stats->failed = h.failed;
-            stats->device_status = 0;
+            stats->reserved = 0;
             stats->residual_max = h.res_max;
             stats->residual_norm2 = h.res_norm2;
-            stats->relative_residual = NAN;
+            stats->relative_residual = h.bb > 0 ? std::sqrt(h.rr / h.bb) : (h.rr > 0 ? INFINITY : 0.0);
             stats->solve_ms = ms;
         }
     });
@@ -639,7 +664,7 @@ static void mgpcg_solve_impl(dv_mgpcg *s, VCycle<T> &vc, dv_stats *stats) {
         stats->iterations = h.it;
         stats->converged = h.converged;
         stats->failed = h.failed;
-        stats->device_status = 0;
+        stats->reserved = 0;
         stats->residual_max = NAN;
         stats->residual_norm2 = std::sqrt(h.rr);
         stats->relative_residual = std::sqrt(h.rr / h.bb);

@@ -184,15 +184,19 @@ class CudaDuViGeometricMultigridSolver(_GeometricMultigridBase):
 
 
 class CudaCsrPcgSolver:
-    """Jacobi-preconditioned CG, FP64, stop when every |r_i| <= tol."""
+    """Jacobi-preconditioned CG, FP64.  Stop when every |r_i| <= tol (the reference's test,
+    tol_kind="abs_max"), or when ||r||_2 <= tol ||b||_2 (tol_kind="rel_l2")."""
 
     FORMAT = N.FORMAT_CSR
 
-    def __init__(self, context: CudaContext, maxIterations, convergenceTolerance, fmt="csr"):
+    def __init__(self, context: CudaContext, maxIterations, convergenceTolerance, fmt="csr", tol_kind="abs_max"):
         self.context = context
         self.MaxIterations = maxIterations
         self.ConvergenceTolerance = convergenceTolerance
         self.fmt = N.FORMAT_DUVI if fmt == "duvi" else N.FORMAT_CSR
+        if tol_kind not in ("abs_max", "rel_l2"):
+            raise ValueError("tol_kind must be 'abs_max' or 'rel_l2'")
+        self.tol_kind = N.TOL_REL_L2 if tol_kind == "rel_l2" else N.TOL_ABS_MAX
         self.h = None
         self.DoFs = 0
 
@@ -205,6 +209,7 @@ class CudaCsrPcgSolver:
                                       C.byref(h)))
         del keep
         self.h = h
+        N.check(N.lib().dv_pcg_set_tolerance_kind(h, self.tol_kind))
         self.context.register(self)
         self.b = None if b is None else np.asarray(b, np.float64)
         self.DoFs = A.shape[0]

@@ -49,8 +49,7 @@ enum {
     DV_ERR_NOMEM = -5,
     DV_ERR_FORMAT = -6,
     DV_ERR_NO_DEVICE = -7,
-    DV_ERR_SINGULAR = -8,
-    DV_ERR_TIMEOUT = -9
+    DV_ERR_SINGULAR = -8
 };
 
 enum { DV_FORMAT_CSR = 0, DV_FORMAT_DUVI = 1 };
@@ -75,11 +74,20 @@ typedef struct {
     const double *val;
 } dv_csr_host;
 
+/* Solve statistics.  Every solver fills iterations, converged, failed,
+ * relative_residual (||b - A x||_2 / ||b||_2 of the returned x, recomputed in FP64
+ * at exit; for dv_mgpcg_solve_multi and dv_batch_solve the worst load case or mesh)
+ * and solve_ms (device time of the solve, CUDA events).  residual_norm2 is the
+ * 2-norm of the last residual the stop test checked (the worst one for several
+ * load cases or meshes).  residual_max, its max-norm, is filled by the solvers
+ * whose stop test can use it (dv_gmg_solve, dv_pcg_solve, dv_pcg_solve_noalloc);
+ * the flexible-CG solvers (dv_mgpcg_*, dv_batch_*, dv_adjoint_*) stop on the
+ * 2-norm and leave it NaN. */
 typedef struct {
     int32_t iterations;        /* NumIterationsRequired (cycles or PCG iterations) */
     int32_t converged;         /* HasConverged: flag bit 1 of the reference kernels */
     int32_t failed;            /* NaN or |r_i| > 1e50: flag bit 2 (CsrCG.cl:274-276) */
-    int32_t device_status;     /* 0, or DV_ERR_TIMEOUT when a bounded device wait expired */
+    int32_t reserved;          /* always 0 */
     double residual_max;       /* max_i |r_i| of the last checked residual */
     double residual_norm2;     /* ||r||_2 of the last checked residual */
     double relative_residual;  /* ||b - A x||_2 / ||b||_2, recomputed in FP64 at exit */
@@ -213,6 +221,11 @@ DV_API int dv_gmg_destroy(dv_gmg *g);
 /* ---- Jacobi PCG (OpenCLCsrPcgSolver, FP64, absolute max-norm stop) ------- */
 DV_API int dv_pcg_create(dv_context *ctx, const dv_csr_host *A, int32_t format, int32_t max_iterations,
                          double tol, dv_pcg **out);
+/* Stop test of later solves: DV_TOL_ABS_MAX (default) stops when every |r_i| <= tol,
+ * the reference's test (CsrCG.cl:257-277, GMCantileverTests.cs:420-424); DV_TOL_REL_L2
+ * stops when ||r||_2 <= tol ||b||_2 (r the recurrence residual, checked at the same
+ * place of the iteration). */
+DV_API int dv_pcg_set_tolerance_kind(dv_pcg *p, int32_t tol_kind);
 DV_API int dv_pcg_solve(dv_pcg *p, const double *b, const double *x0, double *x, dv_stats *stats);
 DV_API int dv_pcg_destroy(dv_pcg *p);
 
@@ -225,10 +238,19 @@ DV_API int dv_pcg_destroy(dv_pcg *p);
  * per device, held until the process exits), which limits A to 131,072 rows
  * (larger: DV_ERR_ARG).  A must be an FP64 square matrix created beforehand;
  * d_b and d_x are device pointers (x: initial guess if use_x0, else zeroed; the
- * solution on return).  All calls on a device share the array: calls that
- * overlap on the GPU race and must be serialised by the caller.  The first call
- * on a device looks up the array's device address; make it before any stream
- * capture. */
+ * solution on return), read and written on A's context stream
+ * (dv_context_stream): work the caller queued on another stream to fill d_b or
+ * d_x must be ordered before the call (an event wait or a synchronize).  The
+ * call returns after the solve finished.  All calls on a device share the
+ * array: calls that overlap on the GPU race and must be serialised by the
+ * caller.  The first call on a device looks up the array's device address;
+ * make it before any stream capture.  The array and the kernels' code are
+ * device memory that CUDA allocates when it loads them; with CUDA's default
+ * lazy module loading that is at the first call on a device (a kernel's code at
+ * its first launch), so a caller that reserves all free device memory makes
+ * one call with each matrix format it will use before reserving, or runs with
+ * CUDA_MODULE_LOADING=EAGER.  stats->relative_residual is recomputed in FP64 at
+ * exit, inside the same array. */
 DV_API int dv_pcg_solve_noalloc(dv_matrix *A, const double *d_b, double *d_x, int32_t use_x0,
                                 int32_t max_iterations, double tol, dv_stats *stats);
 

@@ -122,6 +122,8 @@ double or_gmg_omega_scale(const or_gmg *g, int32_t level);
 /* Jacobi PCG as written in GMCantileverTests.cs:400-433 (absolute max-norm stop).
  * Returns the iteration index at convergence, or -1. */
 int32_t or_pcg_jacobi(const or_csr *a, const double *b, double *x, int32_t max_iter, double tol);
+/* The same with the stop test ||r||_2 <= tol ||b||_2 (build-defined option). */
+int32_t or_pcg_jacobi_rel(const or_csr *a, const double *b, double *x, int32_t max_iter, double tol);
 
 /* ---- build-defined extensions (no reference counterpart; FP64 checkers) --- */
 /* Structured hex assembly at element size h: K = h * sum_e E_e Ke (3-D). */

@@ -264,9 +264,10 @@ extern "C" void or_gmg_solve(or_gmg *g, const double *x0, double *xout, int32_t 
 }
 
 // ---------------------------------------------------------------------------
-// Jacobi PCG, GMCantileverTests.cs:400-433
+// Jacobi PCG, GMCantileverTests.cs:400-433.  rel_l2 = 0: the reference's stop test
+// (every |r_i| <= tol, :420-424); rel_l2 = 1: ||r||_2 <= tol ||b||_2 at the same place.
 // ---------------------------------------------------------------------------
-extern "C" int32_t or_pcg_jacobi(const or_csr *A, const double *b, double *x, int32_t iterations, double tol) {
+static int32_t pcg_jacobi(const or_csr *A, const double *b, double *x, int32_t iterations, double tol, int rel_l2) {
     int32_t n = A->n_rows;
     std::vector<double> M(n), r(n), z(n), p(n), Ap(n), tmp(n);
     for (int32_t i = 0; i < n; ++i) {
@@ -288,7 +289,14 @@ extern "C" int32_t or_pcg_jacobi(const or_csr *A, const double *b, double *x, in
         for (int32_t i = 0; i < n; ++i) x[i] = x[i] + p[i] * a;
         for (int32_t i = 0; i < n; ++i) r[i] = r[i] + Ap[i] * -a;
         bool nobreak = false;
-        for (int32_t i = 0; i < n; ++i) if (std::fabs(r[i]) > tol) nobreak = true;
+        if (rel_l2) {
+            double rr = 0.0, bb = 0.0;
+            for (int32_t i = 0; i < n; ++i) rr += r[i] * r[i];
+            for (int32_t i = 0; i < n; ++i) bb += b[i] * b[i];
+            nobreak = !(rr <= tol * tol * bb);
+        } else {
+            for (int32_t i = 0; i < n; ++i) if (std::fabs(r[i]) > tol) nobreak = true;
+        }
         if (!nobreak) return it;
         for (int32_t i = 0; i < n; ++i) z[i] = M[i] * r[i];
         double rz2 = 0.0;
@@ -299,6 +307,13 @@ extern "C" int32_t or_pcg_jacobi(const or_csr *A, const double *b, double *x, in
         rz = rz2;
     }
     return -1;
+}
+
+extern "C" int32_t or_pcg_jacobi(const or_csr *A, const double *b, double *x, int32_t iterations, double tol) {
+    return pcg_jacobi(A, b, x, iterations, tol, 0);
+}
+extern "C" int32_t or_pcg_jacobi_rel(const or_csr *A, const double *b, double *x, int32_t iterations, double tol) {
+    return pcg_jacobi(A, b, x, iterations, tol, 1);
 }
 
 // ---------------------------------------------------------------------------

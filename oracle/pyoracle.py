@@ -82,6 +82,7 @@ def lib():
             "or_gmg_num_levels": (C.c_int32, [_vp]),
             "or_gmg_omega_scale": (C.c_double, [_vp, C.c_int32]),
             "or_pcg_jacobi": (C.c_int32, [_vp, _f64p, _f64p, C.c_int32, C.c_double]),
+            "or_pcg_jacobi_rel": (C.c_int32, [_vp, _f64p, _f64p, C.c_int32, C.c_double]),
             "or_hex_stiffness": (_vp, [_i32p, _vp, C.c_double, C.c_double, C.c_double]),
             "or_hex_trilinear": (_vp, [_i32p]),
             "or_galerkin": (_vp, [_vp, _vp]),
@@ -333,9 +334,12 @@ class Gmg:
             self.h = None
 
 
-def pcg_jacobi(csr: Csr, b, max_iter=2000, tol=1e-5, x0=None):
+def pcg_jacobi(csr: Csr, b, max_iter=2000, tol=1e-5, x0=None, rel_l2=False):
+    """Jacobi PCG of GMCantileverTests.cs:400-433; rel_l2 stops on ||r||_2 <= tol ||b||_2 instead of
+    the reference's max |r_i| <= tol.  Returns (x, iteration index at the stop, -1 if not converged)."""
     x = np.zeros(csr.shape[0]) if x0 is None else np.array(x0, np.float64)
-    it = lib().or_pcg_jacobi(csr.h, np.ascontiguousarray(b, np.float64), x, max_iter, tol)
+    f = lib().or_pcg_jacobi_rel if rel_l2 else lib().or_pcg_jacobi
+    it = f(csr.h, np.ascontiguousarray(b, np.float64), x, max_iter, tol)
     return x, it
 
 

@@ -34,6 +34,34 @@ def test_pcg_matches_oracle(ctx, native, oracle, fmt):
     s.ReleaseCudaResources()
 
 
+@pytest.mark.parametrize("fmt", ["csr", "duvi"])
+@pytest.mark.parametrize("tol_kind", ["abs_max", "rel_l2"])
+def test_pcg_cantilever_16cube_traction_matches_oracle(ctx, native, oracle, fmt, tol_kind):
+    """The 16^3 cantilever under unit traction (13,872 dofs), Jacobi-PCG from zero to 1e-8, in CSR
+    and in DuVi: the reference's stop test (every |r_i| <= 1e-8) and the relative one
+    (||r||_2 <= 1e-8 ||b||_2).  Same system as the oracle's own assembly; iterations within 1,
+    solution within 1e-7."""
+    ne = (16, 16, 16)
+    K = oracle.hex_stiffness(ne)
+    b = oracle.traction_rhs(ne, ne, (0.0, 0.0, -1.0))
+    rel_l2 = tol_kind == "rel_l2"
+    x_ref, it_ref = oracle.pcg_jacobi(K, b, 20000, 1e-8, rel_l2=rel_l2)
+    assert it_ref > 0
+    A = K.to_scipy()
+    s = native.CudaCsrPcgSolver(ctx, 20000, 1e-8, fmt=fmt, tol_kind=tol_kind).Initialize(A=A, b=b)
+    x, st = s.Solve()
+    s.ReleaseCudaResources()
+    assert st.HasConverged and not st.Failed
+    assert abs(st.NumIterationsRequired - it_ref) <= 1, (st.NumIterationsRequired, it_ref)
+    assert rel(x, x_ref) < 1e-7
+    true_rel = np.linalg.norm(b - A @ x) / np.linalg.norm(b)
+    assert abs(st.RelativeResidual - true_rel) <= 1e-3 * true_rel
+    if rel_l2:
+        assert true_rel <= 1.01e-8
+    else:
+        assert st.ResidualMaxNorm <= 1e-8 and np.max(np.abs(b - A @ x)) <= 1.01e-8
+
+
 def test_pcg_max_iterations_and_not_initialized(ctx, native, oracle):
     m = oracle.Model((8, 2, 2), (20, 1, 1))
     s = native.CudaCsrPcgSolver(ctx, 3, 1e-14).Initialize(A=m.kff.to_scipy(), b=m.rhs())

@@ -34,12 +34,21 @@ def test_noalloc_pcg_matches_allocating_pcg(ctx, native, oracle, fmt):
     torch.cuda.synchronize()
     for call in range(2):
         st = N.Stats()
+        # free device memory around the call: the warm (second) call must not allocate
+        free_before = torch.cuda.mem_get_info()[0]
         N.check(N.lib().dv_pcg_solve_noalloc(M.h, C.c_void_p(db.data_ptr()), C.c_void_p(dx.data_ptr()), 0, 2000,
                                              1e-8, C.byref(st)))
+        free_after = torch.cuda.mem_get_info()[0]
+        if call == 1:
+            assert free_after == free_before, (free_before, free_after)
         x = dx.cpu().numpy()
         assert st.converged and not st.failed, call
         assert st.iterations == st_ref.NumIterationsRequired, call
         assert np.max(np.abs(x - x_ref)) <= REL * np.max(np.abs(x_ref)), call
+        # the relative residual is recomputed in FP64 at exit, as for the allocating solver
+        true_rel = np.linalg.norm(b - A @ x) / np.linalg.norm(b)
+        assert abs(st.relative_residual - true_rel) <= 1e-3 * true_rel, call
+        assert abs(st.relative_residual - st_ref.RelativeResidual) <= 1e-3 * st_ref.RelativeResidual, call
         dx.fill_(float("nan"))   # the next call must not read the old solution
         torch.cuda.synchronize()
     # warm start from the solution: converged at once
