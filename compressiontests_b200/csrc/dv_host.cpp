@@ -673,6 +673,50 @@ void dv_build_duvi_patterns(const DuviHost &h, int32_t n, int32_t n_cols, int g,
     P.ok = 1;
 }
 
+void dv_build_duvi_grid(const DuviPatternHost &P, DuviGridHost &G) {
+    G = DuviGridHost();
+    if (!P.ok || P.group != 3 || P.based || P.shift || P.ngroups < 27) return;
+    const int npat = (int)P.start.size() - 1;
+    std::vector<int64_t> cnt(npat, 0);
+    for (uint16_t id : P.id) cnt[id]++;
+    const int hot = (int)(std::max_element(cnt.begin(), cnt.end()) - cnt.begin());
+    const uint32_t s0 = P.start[hot];
+    if (P.start[hot + 1] - s0 != 81) return;
+    // the 27 neighbour groups, each with its 3 consecutive columns, in column order
+    int64_t no[27];
+    for (int j = 0; j < 27; ++j) {
+        const int64_t o = P.off[s0 + 3 * j];
+        for (int c = 1; c < 3; ++c)
+            if (P.off[s0 + 3 * j + c] != o + c) return;
+        if (((o % 3) + 3) % 3 != 0) return;
+        no[j] = o / 3;
+    }
+    const int64_t lx = no[16], lxy = no[22];   // offsets of the +y and +z neighbours
+    if (lx < 3 || lxy < 3 * lx || lxy % lx != 0) return;
+    for (int dz = -1; dz <= 1; ++dz)
+        for (int dy = -1; dy <= 1; ++dy)
+            for (int dx = -1; dx <= 1; ++dx)
+                if (no[9 * (dz + 1) + 3 * (dy + 1) + dx + 1] != dx + lx * dy + lxy * dz) return;
+    const int64_t ly = lxy / lx, ng = P.ngroups;
+    if (ly < 3 || ng % lxy != 0 || ng / lxy < 3 || lx > INT32_MAX || ly > INT32_MAX) return;
+    const int64_t lz = ng / lxy;
+    bool all_hot = true;
+    for (int64_t gi = 0; gi < ng; ++gi) {
+        const int64_t ix = gi % lx, iy = (gi / lx) % ly, iz = gi / lxy;
+        const bool inner = ix >= 1 && ix <= lx - 2 && iy >= 1 && iy <= ly - 2 && iz >= 1 && iz <= lz - 2;
+        if (inner && P.id[gi] == hot) continue;
+        if (inner) all_hot = false;
+        G.boundary.push_back((uint32_t)gi);
+    }
+    G.vi.assign(P.vi.begin() + 3 * (size_t)s0, P.vi.begin() + 3 * (size_t)(s0 + 81));
+    G.lx = (int32_t)lx;
+    G.ly = (int32_t)ly;
+    G.lz = (int32_t)lz;
+    G.hot = hot;
+    G.all_hot = all_hot ? 1 : 0;
+    G.ok = 1;
+}
+
 void dv_extract_diag(const dv_csr_host &a, std::vector<double> &d) {
     d.assign(a.n_rows, 0.0);
 #pragma omp parallel for schedule(static)

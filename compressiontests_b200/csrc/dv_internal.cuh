@@ -208,7 +208,8 @@ struct dv_matrix {
     DevMem bundles;            // int32 row starts of row bundles (+ sentinel)
     int32_t nbundles = 0;
     int duvi_batch = 4;        // entries per gather batch in the decode loop (9 when most blocks hold 9)
-    int duvi_variant = 0;      // 0: shared-memory staged rows, 1: lane-interleaved groups, 2: node patterns (autotuned)
+    int duvi_variant = 0;      // 0: shared-memory staged rows, 1: lane-interleaved groups, 2: node patterns,
+                               // 3: grid stencil (autotuned)
     int lanes_group = 1;
     int lanes_scaled = 0;
     int lanes_shift = 0;
@@ -220,6 +221,14 @@ struct dv_matrix {
     DevMem pat_base;                     // u32 first column per group (based patterns)
     int pat_based = 0, pat_shift = 0;
     int32_t pat_count = 0, pat_entries = 0, pat_maxlen = 0;
+    int grid_ok = 0;           // grid-stencil layout in use (duvi_variant 3), see DuviGridHost
+    int32_t grid_lx = 0, grid_ly = 0, grid_lz = 0;
+    int grid_hot = -1, grid_all_hot = 0;
+    std::vector<double> grid_coef;       // 81 x 3 values of the hot pattern (entry k, row d at 3 * k + d)
+    int grid_hex = 0;                    // 1: grid_coef has the hex stencil structure (dvk::hex_class)
+    double grid_cls[10] = {};            // its class values
+    DevMem grid_bnode;                   // u32 boundary groups
+    int64_t grid_nb = 0;
     int lanes_stencil = 0;     // stencil mode: lanes_off holds the column offsets (int32)
     DevMem lanes_off;
     int32_t lanes_noff = 0;
@@ -250,6 +259,23 @@ struct DuviPatternHost {
     std::vector<int32_t> off;        // column - first row of the group, per pattern entry
     std::vector<uint32_t> vi;        // g value indices per pattern entry
 };
+// Grid-stencil layout (derived from the node patterns, read-only).  A square operator
+// with 3 rows per node group, groups numbered x-fastest on an lx x ly x lz box, whose most
+// frequent pattern ("hot") couples a group with its 27 box neighbours (3 columns each, in
+// column order).  Groups off the box faces with the hot pattern are computed by a stencil
+// that streams the box plane by plane, with the hot pattern's values as kernel parameters;
+// every other group (faces, and interior groups of other patterns) keeps its pattern
+// records and is listed in `boundary`.
+struct DuviGridHost {
+    int ok = 0;
+    int32_t lx = 0, ly = 0, lz = 0;
+    int hot = -1;                    // pattern id of the stencil groups
+    int all_hot = 0;                 // 1: every group off the faces has the hot pattern
+    std::vector<uint32_t> vi;        // value indices of the hot pattern, entry k, row d at 3 * k + d
+    std::vector<uint32_t> boundary;  // groups computed from their pattern records, ascending
+};
+void dv_build_duvi_grid(const DuviPatternHost &P, DuviGridHost &out);
+
 // Builds the pattern layout for rows in groups of `group` (identical or, with shift,
 // shifted columns) when at most max_patterns patterns of max_entries entries in all
 // exist.  Square operators without shift take offsets from the group's first row;

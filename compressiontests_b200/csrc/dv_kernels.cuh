@@ -829,8 +829,65 @@ struct alignas(16) PatRec {
 static_assert(sizeof(PatRec<float>) == 16 && offsetof(PatRec<float>, v) == 4, "FP32 pattern record layout");
 static_assert(sizeof(PatRec<double>) == 32 && offsetof(PatRec<double>, v) == 8, "FP64 pattern record layout");
 
+// Stages a pattern table (records and pattern starts) in shared memory.
+template <class AT>
+__device__ __forceinline__ void stage_patterns(uint4 *smem, const PatRec<AT> *__restrict__ grec,
+                                               const uint32_t *__restrict__ pstart, int32_t npat, int32_t nrec) {
+    uint32_t *st = reinterpret_cast<uint32_t *>(reinterpret_cast<PatRec<AT> *>(smem) + nrec);
+    const uint4 *src = reinterpret_cast<const uint4 *>(grec);
+    const int n16 = nrec * (int)(sizeof(PatRec<AT>) / 16);
+    for (int i = threadIdx.x; i < n16; i += blockDim.x) smem[i] = __ldg(src + i);
+    for (int i = threadIdx.x; i <= npat; i += blockDim.x) st[i] = __ldg(pstart + i);
+}
+
+// One node group from its pattern records (shared memory): every row summed in entry order.
 // BASED: offsets from the group's first column (base[]), else from its first row;
 // SHIFT: row d of the group reads column + d.
+template <class AT, class Gather, class Op, int G, bool BASED, bool SHIFT>
+__device__ __forceinline__ void pattern_group(int64_t gi, const PatRec<AT> *rec, const uint32_t *st,
+                                              const uint16_t *__restrict__ pid, const uint32_t *__restrict__ base,
+                                              const Gather &g, const Op &op, double *red) {
+    const uint32_t p = __ldg(pid + gi);
+    const uint32_t b = st[p], e = st[p + 1];
+    const int32_t r0 = (int32_t)(gi * G);
+    const int32_t c0 = BASED ? (int32_t)__ldg(base + gi) : r0;
+    AT s[G];
+#pragma unroll
+    for (int d = 0; d < G; ++d) s[d] = op.init(r0 + d);
+    uint32_t k = b;
+    for (; k + 4 <= e; k += 4) {
+        PatRec<AT> q[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) q[u] = rec[k + u];
+        if constexpr (SHIFT) {
+            AT x[4][G];
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int d = 0; d < G; ++d) x[u][d] = g((uint32_t)(c0 + q[u].off + d));
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int d = 0; d < G; ++d) s[d] = madd_op<AT, op_fused<Op>::value>(s[d], q[u].v[d], x[u][d]);
+        } else {
+            AT x[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) x[u] = g((uint32_t)(c0 + q[u].off));
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int d = 0; d < G; ++d) s[d] = madd_op<AT, op_fused<Op>::value>(s[d], q[u].v[d], x[u]);
+        }
+    }
+    for (; k < e; ++k) {
+        const PatRec<AT> q = rec[k];
+#pragma unroll
+        for (int d = 0; d < G; ++d) s[d] = madd_op<AT, op_fused<Op>::value>(s[d], q.v[d], g((uint32_t)(c0 + q.off + (SHIFT ? d : 0))));
+    }
+#pragma unroll
+    for (int d = 0; d < G; ++d) op.row(r0 + d, s[d], red);
+}
+
 template <class AT, class Gather, class Op, int G, bool BASED, bool SHIFT>
 __global__ void __launch_bounds__(256) k_duvi_pattern(const uint16_t *__restrict__ pid, const uint32_t *__restrict__ pstart,
                                                       const PatRec<AT> *__restrict__ grec, const uint32_t *__restrict__ base,
@@ -838,58 +895,219 @@ __global__ void __launch_bounds__(256) k_duvi_pattern(const uint16_t *__restrict
                                                       const int *__restrict__ done, double *partials, unsigned *ticket) {
     if (done && *(volatile const int *)done) return;
     extern __shared__ uint4 pat_smem[];
-    PatRec<AT> *rec = reinterpret_cast<PatRec<AT> *>(pat_smem);
-    uint32_t *st = reinterpret_cast<uint32_t *>(rec + nrec);
-    {
-        const uint4 *src = reinterpret_cast<const uint4 *>(grec);
-        const int n16 = nrec * (int)(sizeof(PatRec<AT>) / 16);
-        for (int i = threadIdx.x; i < n16; i += blockDim.x) pat_smem[i] = __ldg(src + i);
-        for (int i = threadIdx.x; i <= npat; i += blockDim.x) st[i] = __ldg(pstart + i);
-    }
+    const PatRec<AT> *rec = reinterpret_cast<const PatRec<AT> *>(pat_smem);
+    const uint32_t *st = reinterpret_cast<const uint32_t *>(rec + nrec);
+    stage_patterns<AT>(pat_smem, grec, pstart, npat, nrec);
     __syncthreads();
     double red[Op::NRED > 0 ? Op::NRED : 1];
 #pragma unroll
     for (int i = 0; i < (Op::NRED > 0 ? Op::NRED : 1); ++i) red[i] = 0.0;
-    for (int64_t gi = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; gi < ngroups; gi += (int64_t)gridDim.x * blockDim.x) {
-        const uint32_t p = __ldg(pid + gi);
-        const uint32_t b = st[p], e = st[p + 1];
-        const int32_t r0 = (int32_t)(gi * G);
-        const int32_t c0 = BASED ? (int32_t)__ldg(base + gi) : r0;
-        AT s[G];
+    for (int64_t gi = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; gi < ngroups; gi += (int64_t)gridDim.x * blockDim.x)
+        pattern_group<AT, Gather, Op, G, BASED, SHIFT>(gi, rec, st, pid, base, g, op, red);
+    if constexpr (Op::NRED > 0) {
+        double tot[Op::NRED];
+        if (grid_reduce<Op::NRED, Op::MAXMASK>(red, partials, ticket, tot)) op.finish(tot);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// DuVi grid-stencil kernel (derived layout, see DuviGridHost)
+//
+// Operators whose node groups sit on an lx x ly x lz box (x fastest, 3 rows per group) and
+// whose interior groups share one pattern coupling the 27 box neighbours.  A block owns a
+// tile of 32 x 8 groups of the xy plane and a run of zc planes; it streams the planes z0-1 ..
+// z1 through shared memory (the tile plus a one-group halo, 3 values per group, double
+// buffered, the next plane's loads in flight during the current plane's arithmetic).  Each
+// staged value is read once per thread and applied to the three groups it couples to in z
+// (the plane below, at and above it), so a group's three rows collect the 81 columns in
+// column order: plane z-1, then z, then z+1, each plane by y, x and dof.  With the same
+// multiply-add rounding this is the node-pattern kernel's sum bit for bit.  The interior
+// pattern's values are kernel parameters (constant-bank operands of the FMAs): no record
+// loads, one shared-memory load per staged value.  Groups on the box faces, and interior
+// groups of other patterns, are listed and run through their pattern records by the first
+// blocks of the same launch.
+// ---------------------------------------------------------------------------
+
+// Structure of the interior row block of an isotropic trilinear hexahedron operator on a uniform
+// grid (3 rows of a node against its 27 neighbours x 3 dofs, entry k and row d at 3 k + d): the
+// entries of one class are equal and class -1 entries are zero, for every modulus and Poisson
+// ratio.  The equalities come from the element's reflection and rotation symmetries, the zeros
+// from the cancellation of the 8 elements that share the node (90 of the 243 entries).  Ten
+// values then describe the whole stencil.  A matrix is checked against this table when its
+// grid layout is built and uses it only if every equality and zero holds exactly.
+constexpr int kHexClasses = 10;
+__host__ __device__ constexpr int hex_class(int i) {
+    constexpr signed char t[243] = {
+         0,  1,  1,  1,  0,  1,  1,  1,  0,  2, -1, -1, -1,  3,  4, -1,  4,  3,  0,  5,  5,  5,  0,  1,  5,  1,  0,
+         3, -1,  4, -1,  2, -1,  4, -1,  3,  6, -1, -1, -1,  6, -1, -1, -1,  7,  3, -1,  8, -1,  2, -1,  8, -1,  3,
+         0,  5,  1,  5,  0,  5,  1,  5,  0,  2, -1, -1, -1,  3,  8, -1,  8,  3,  0,  1,  5,  1,  0,  5,  5,  5,  0,
+         3,  4, -1,  4,  3, -1, -1, -1,  2,  6, -1, -1, -1,  7, -1, -1, -1,  6,  3,  8, -1,  8,  3, -1, -1, -1,  2,
+         7, -1, -1, -1,  6, -1, -1, -1,  6,  9, -1, -1, -1,  9, -1, -1, -1,  9,  7, -1, -1, -1,  6, -1, -1, -1,  6,
+         3,  8, -1,  8,  3, -1, -1, -1,  2,  6, -1, -1, -1,  7, -1, -1, -1,  6,  3,  4, -1,  4,  3, -1, -1, -1,  2,
+         0,  1,  5,  1,  0,  5,  5,  5,  0,  2, -1, -1, -1,  3,  8, -1,  8,  3,  0,  5,  1,  5,  0,  5,  1,  5,  0,
+         3, -1,  8, -1,  2, -1,  8, -1,  3,  6, -1, -1, -1,  6, -1, -1, -1,  7,  3, -1,  4, -1,  2, -1,  4, -1,  3,
+         0,  5,  5,  5,  0,  1,  5,  1,  0,  2, -1, -1, -1,  3,  4, -1,  4,  3,  0,  1,  1,  1,  0,  1,  1,  1,  0};
+    return t[i];
+}
+
+constexpr int kGridTX = 32, kGridTY = 8;                        // tile of groups per block (one warp per row)
+constexpr int kGridPX = kGridTX + 2, kGridPY = kGridTY + 2;     // with halo
+constexpr int kGridPlane = kGridPX * kGridPY * 3;               // staged values per plane (1020)
+constexpr int kGridLoads = (kGridPlane + 255) / 256;            // per thread (4)
+
+template <class AT>
+struct GridCoef {
+    AT v[81][3];           // interior pattern: entry k = 27 dz' + 9 dy' + 3 dx' + c (primes: offset + 1), row d
+    AT cls[kHexClasses];   // its class values when it has the hex structure (hex_class)
+};
+
+struct GridGeom {
+    int32_t lx, ly, lz;        // group box
+    int32_t ntx, nty, zc;      // tiles per plane in x and y, planes per z run
+    int32_t ntile;             // ntx * nty * ceil(lz / zc)
+    int32_t bound_blocks;      // blocks [0, bound_blocks) run the boundary list, the rest the tiles
+    int32_t hot, all_hot;      // interior pattern id; 1 when no interior group has another pattern
+    int64_t nbound;
+};
+
+// One term of a stencil row: the coefficient of entry k, row d.  HEX takes it from the ten class
+// values (zero entries skipped where SKIP0, i.e. wherever the result need not equal the sequential
+// sum over every stored entry bit for bit: NaN or infinite x and the sign of a zero sum are the
+// only differences), otherwise from the full table.
+template <class AT, bool FUSED, bool HEX, bool SKIP0>
+__device__ __forceinline__ AT grid_term(AT acc, const GridCoef<AT> &cf, int k, int d, AT v) {
+    if constexpr (HEX) {
+        const int c = hex_class(3 * k + d);
+        if (c >= 0) return madd_op<AT, FUSED>(acc, cf.cls[c], v);
+        if constexpr (SKIP0) return acc;
+        else return madd_op<AT, FUSED>(acc, AT(0), v);
+    } else {
+        return madd_op<AT, FUSED>(acc, cf.v[k][d], v);
+    }
+}
+
+// One staged plane applied to the three accumulated groups: below (DI: group p+1 takes the
+// plane as its dz = -1 neighbours), at (DM: group p, dz = 0) and above (DF: group p-1, dz = +1).
+template <class AT, bool FUSED, bool HEX, bool SKIP0, bool DI, bool DM, bool DF>
+__device__ __forceinline__ void grid_plane_step(const AT *__restrict__ pl, int tx, int ty, const GridCoef<AT> &cf,
+                                                AT (&a0)[3], AT (&a1)[3], AT (&a2)[3]) {
 #pragma unroll
-        for (int d = 0; d < G; ++d) s[d] = op.init(r0 + d);
-        uint32_t k = b;
-        for (; k + 4 <= e; k += 4) {
-            PatRec<AT> q[4];
+    for (int dy = 0; dy < 3; ++dy)
 #pragma unroll
-            for (int u = 0; u < 4; ++u) q[u] = rec[k + u];
-            if constexpr (SHIFT) {
-                AT x[4][G];
+        for (int dx = 0; dx < 3; ++dx)
 #pragma unroll
-                for (int u = 0; u < 4; ++u)
+            for (int c = 0; c < 3; ++c) {
+                const AT v = pl[((ty + dy) * kGridPX + tx + dx) * 3 + c];
+                const int k = 9 * dy + 3 * dx + c;
 #pragma unroll
-                    for (int d = 0; d < G; ++d) x[u][d] = g((uint32_t)(c0 + q[u].off + d));
+                for (int d = 0; d < 3; ++d) {
+                    if (DI) a2[d] = grid_term<AT, FUSED, HEX, SKIP0>(a2[d], cf, k, d, v);
+                    if (DM) a1[d] = grid_term<AT, FUSED, HEX, SKIP0>(a1[d], cf, 27 + k, d, v);
+                    if (DF) a0[d] = grid_term<AT, FUSED, HEX, SKIP0>(a0[d], cf, 54 + k, d, v);
+                }
+            }
+}
+
+template <class AT, class Gather, class Op, bool HEX>
+__global__ void __launch_bounds__(256, sizeof(AT) == 8 ? 2 : 3)
+    k_duvi_grid(GridGeom G, GridCoef<AT> cf, const uint16_t *__restrict__ pid, const uint32_t *__restrict__ pstart,
+                const PatRec<AT> *__restrict__ grec, const uint32_t *__restrict__ bnode, int32_t npat, int32_t nrec,
+                Gather g, Op op, const int *__restrict__ done, double *partials, unsigned *ticket) {
+    if (done && *(volatile const int *)done) return;
+    extern __shared__ uint4 grid_smem[];
+    constexpr bool FU = op_fused<Op>::value;
+    constexpr bool S0 = FU || sizeof(AT) == 4;   // FP64 parity epilogues multiply the zeros too
+    double red[Op::NRED > 0 ? Op::NRED : 1];
 #pragma unroll
-                for (int u = 0; u < 4; ++u)
+    for (int i = 0; i < (Op::NRED > 0 ? Op::NRED : 1); ++i) red[i] = 0.0;
+    if ((int32_t)blockIdx.x < G.bound_blocks) {
+        // boundary groups from their pattern records
+        const PatRec<AT> *rec = reinterpret_cast<const PatRec<AT> *>(grid_smem);
+        const uint32_t *st = reinterpret_cast<const uint32_t *>(rec + nrec);
+        stage_patterns<AT>(grid_smem, grec, pstart, npat, nrec);
+        __syncthreads();
+        for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < G.nbound;
+             i += (int64_t)G.bound_blocks * blockDim.x)
+            pattern_group<AT, Gather, Op, 3, false, false>((int64_t)__ldg(bnode + i), rec, st, pid, nullptr, g, op, red);
+    } else {
+        AT *plane = reinterpret_cast<AT *>(grid_smem);   // two staged planes
+        const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+        // this thread's staging slots: the same positions in every plane and tile
+        int sx[kGridLoads], sy[kGridLoads], sc[kGridLoads];
 #pragma unroll
-                    for (int d = 0; d < G; ++d) s[d] = madd_op<AT, op_fused<Op>::value>(s[d], q[u].v[d], x[u][d]);
-            } else {
-                AT x[4];
+        for (int j = 0; j < kGridLoads; ++j) {
+            const int k = threadIdx.x + 256 * j;
+            const int row = k / (kGridPX * 3), col = k - row * (kGridPX * 3);
+            sx[j] = col / 3 - 1;
+            sc[j] = col - 3 * (col / 3);
+            sy[j] = k < kGridPlane ? row - 1 : -1000000;   // slots past the plane never load or store
+        }
+        const int64_t lxy = (int64_t)G.lx * G.ly;
+        const int nblk = (int)gridDim.x - G.bound_blocks;
+        for (int t = (int)blockIdx.x - G.bound_blocks; t < G.ntile; t += nblk) {
+            const int txi = t % G.ntx, tyi = (t / G.ntx) % G.nty, tzi = t / (G.ntx * G.nty);
+            const int x0 = txi * kGridTX, y0 = tyi * kGridTY, z0 = tzi * G.zc, z1 = min(G.lz, z0 + G.zc);
+            const int ix = x0 + tx, iy = y0 + ty;
+            const bool inxy = ix >= 1 && ix <= G.lx - 2 && iy >= 1 && iy <= G.ly - 2;
+            const int64_t col_xy = (int64_t)ix + (int64_t)G.lx * iy;   // group index in its plane
+            AT pre[kGridLoads];
+            auto load = [&](int z) {
 #pragma unroll
-                for (int u = 0; u < 4; ++u) x[u] = g((uint32_t)(c0 + q[u].off));
+                for (int j = 0; j < kGridLoads; ++j) {
+                    const int xn = x0 + sx[j], yn = y0 + sy[j];
+                    AT v = AT(0);
+                    if (xn >= 0 && xn < G.lx && yn >= 0 && yn < G.ly && z >= 0 && z < G.lz)
+                        v = g((uint32_t)(3 * ((int64_t)xn + (int64_t)G.lx * yn + lxy * z) + sc[j]));
+                    pre[j] = v;
+                }
+            };
+            // a stencil group (off the faces, interior pattern) that this thread finishes
+            auto active = [&](int z) {
+                if (!inxy || z < 1 || z > G.lz - 2) return false;
+                return G.all_hot || (int)__ldg(pid + col_xy + lxy * z) == G.hot;
+            };
+            load(z0 - 1);
+            AT a0[3], a1[3], a2[3];
 #pragma unroll
-                for (int u = 0; u < 4; ++u)
+            for (int d = 0; d < 3; ++d) a0[d] = a1[d] = a2[d] = AT(0);
+            bool act0 = false, act1 = false, act2 = false;
+            int buf = 0;
+            for (int p = z0 - 1; p <= z1; ++p) {
+                AT *pl = plane + buf * kGridPlane;
 #pragma unroll
-                    for (int d = 0; d < G; ++d) s[d] = madd_op<AT, op_fused<Op>::value>(s[d], q[u].v[d], x[u]);
+                for (int j = 0; j < kGridLoads; ++j)
+                    if (sy[j] > -2) pl[threadIdx.x + 256 * j] = pre[j];
+                __syncthreads();
+                if (p + 1 <= z1) load(p + 1);
+                const bool di = p + 1 >= z0 && p + 1 < z1, dm = p >= z0 && p < z1, df = p - 1 >= z0 && p - 1 < z1;
+                if (di) {
+                    act2 = active(p + 1);
+                    const int32_t r = (int32_t)(3 * (col_xy + lxy * (p + 1)));
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) a2[d] = act2 ? op.init(r + d) : AT(0);
+                }
+                if (di && dm && df) grid_plane_step<AT, FU, HEX, S0, true, true, true>(pl, tx, ty, cf, a0, a1, a2);
+                else if (di && dm) grid_plane_step<AT, FU, HEX, S0, true, true, false>(pl, tx, ty, cf, a0, a1, a2);
+                else if (dm && df) grid_plane_step<AT, FU, HEX, S0, false, true, true>(pl, tx, ty, cf, a0, a1, a2);
+                else if (di) grid_plane_step<AT, FU, HEX, S0, true, false, false>(pl, tx, ty, cf, a0, a1, a2);
+                else if (dm) grid_plane_step<AT, FU, HEX, S0, false, true, false>(pl, tx, ty, cf, a0, a1, a2);
+                else if (df) grid_plane_step<AT, FU, HEX, S0, false, false, true>(pl, tx, ty, cf, a0, a1, a2);
+                if (df && act0) {
+                    const int32_t r = (int32_t)(3 * (col_xy + lxy * (p - 1)));
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) op.row(r + d, a0[d], red);
+                }
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    a0[d] = a1[d];
+                    a1[d] = a2[d];
+                }
+                act0 = act1;
+                act1 = act2;
+                act2 = false;
+                buf ^= 1;
             }
         }
-        for (; k < e; ++k) {
-            const PatRec<AT> q = rec[k];
-#pragma unroll
-            for (int d = 0; d < G; ++d) s[d] = madd_op<AT, op_fused<Op>::value>(s[d], q.v[d], g((uint32_t)(c0 + q.off + (SHIFT ? d : 0))));
-        }
-#pragma unroll
-        for (int d = 0; d < G; ++d) op.row(r0 + d, s[d], red);
     }
     if constexpr (Op::NRED > 0) {
         double tot[Op::NRED];
@@ -918,6 +1136,60 @@ void launch_duvi_pattern_gbs(const LaunchEnv &e, const dv_matrix *m, Gather g, O
                                           m->pat_count, m->pat_entries, ng, g, op, e.done, e.partials, e.ticket);
     DV_CUDA(cudaGetLastError());
     e.ctx->count();
+}
+
+// Grid-stencil launch: boundary blocks first (they run alongside the tiles), then tile blocks over
+// runs of zc planes; zc shrinks until the tiles fill at least four waves of resident blocks.
+template <class AT, class Gather, class Op, bool HEX>
+void launch_duvi_grid_h(const LaunchEnv &e, const dv_matrix *m, Gather g, Op op) {
+    auto kern = k_duvi_grid<AT, Gather, Op, HEX>;
+    const size_t smem = std::max(2 * sizeof(AT) * (size_t)kGridPlane,
+                                 sizeof(PatRec<AT>) * (size_t)m->pat_entries + 4 * ((size_t)m->pat_count + 1));
+    static SmemLimit limit;   // per instantiation and device
+    limit.raise(kern, smem, e.ctx->device);
+    static OccupancyCache occupancy;   // per instantiation
+    const int occ = occupancy.get(kern, 256, smem, e.ctx->device);
+    GridCoef<AT> cf;
+    for (int k = 0; k < 81; ++k)
+        for (int d = 0; d < 3; ++d) cf.v[k][d] = (AT)m->grid_coef[3 * k + d];
+    for (int c = 0; c < kHexClasses; ++c) cf.cls[c] = HEX ? (AT)m->grid_cls[c] : AT(0);
+    GridGeom G;
+    G.lx = m->grid_lx;
+    G.ly = m->grid_ly;
+    G.lz = m->grid_lz;
+    G.ntx = (G.lx + kGridTX - 1) / kGridTX;
+    G.nty = (G.ly + kGridTY - 1) / kGridTY;
+    G.hot = m->grid_hot;
+    G.all_hot = m->grid_all_hot;
+    G.nbound = m->grid_nb;
+    const int64_t wave = (int64_t)e.ctx->num_sms * occ;
+    G.bound_blocks = G.nbound == 0 ? 0
+                     : (int32_t)std::min<int64_t>((G.nbound + 255) / 256, std::max<int64_t>(1, e.max_blocks / 4));
+    const int64_t plane_tiles = (int64_t)G.ntx * G.nty;
+    int zc = 16;
+    while (zc > 4 && plane_tiles * ((G.lz + zc - 1) / zc) < 4 * wave) zc /= 2;
+    G.zc = zc;
+    G.ntile = (int32_t)(plane_tiles * ((G.lz + zc - 1) / zc));
+    const int64_t tile_blocks = std::min<int64_t>(G.ntile, std::max<int64_t>(1, e.max_blocks - G.bound_blocks));
+    const int blocks = (int)(G.bound_blocks + tile_blocks);
+    kern<<<blocks, 256, smem, e.stream>>>(G, cf, m->pat_id.as<uint16_t>(), m->pat_start.as<uint32_t>(),
+                                          static_cast<const PatRec<AT> *>(m->pat_rec.p), m->grid_bnode.as<uint32_t>(),
+                                          m->pat_count, m->pat_entries, g, op, e.done, e.partials, e.ticket);
+    DV_CUDA(cudaGetLastError());
+    e.ctx->count();
+}
+
+template <class AT, class Gather, class Op, int G>
+void launch_duvi_pattern_g(const LaunchEnv &e, const dv_matrix *m, Gather g, Op op);
+
+// The hex-structured stencil when the matrix has it; the general stencil (243 coefficients) in
+// FP32 otherwise.  FP64 matrices without the hex structure keep the node patterns (grid_ok is
+// not set for them); the fallback below only guards against a stale variant.
+template <class AT, class Gather, class Op>
+void launch_duvi_grid(const LaunchEnv &e, const dv_matrix *m, Gather g, Op op) {
+    if (m->grid_hex) launch_duvi_grid_h<AT, Gather, Op, true>(e, m, g, op);
+    else if constexpr (sizeof(AT) == 4) launch_duvi_grid_h<AT, Gather, Op, false>(e, m, g, op);
+    else launch_duvi_pattern_g<AT, Gather, Op, 3>(e, m, g, op);
 }
 
 template <class AT, class Gather, class Op, int G>
@@ -975,6 +1247,10 @@ void launch_csr_tpr(const LaunchEnv &e, const dv_matrix *m, Gather g, Op op) {
 // Runs op over every row of m with the accumulator type AT (= value precision).
 template <class AT, class Gather, class Op>
 void launch_rows(const LaunchEnv &e, const dv_matrix *m, Gather g, Op op) {
+    if (m->format == DV_FORMAT_DUVI && m->duvi_variant == 3) {
+        launch_duvi_grid<AT>(e, m, g, op);
+        return;
+    }
     if (m->format == DV_FORMAT_DUVI && m->duvi_variant == 2) {
         launch_duvi_pattern<AT>(e, m, g, op);
         return;

@@ -2,6 +2,7 @@
 #include "dv_kernels.cuh"
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 
@@ -209,6 +210,37 @@ static void finish_duvi_upload(dv_matrix *m, const DuviHost &h, cudaStream_t s) 
                 m->pat_count = (int32_t)P.start.size() - 1;
                 m->pat_entries = (int32_t)ne;
                 m->duvi_variant = 2;
+                const char *ge = getenv("DV_GRID");   // DV_GRID=0 keeps the node-pattern kernel (A/B comparisons)
+                DuviGridHost Gd;
+                if (!(ge && ge[0] == '0')) dv_build_duvi_grid(P, Gd);
+                if (Gd.ok) {
+                    m->grid_lx = Gd.lx;
+                    m->grid_ly = Gd.ly;
+                    m->grid_lz = Gd.lz;
+                    m->grid_hot = Gd.hot;
+                    m->grid_all_hot = Gd.all_hot;
+                    m->grid_coef.resize(Gd.vi.size());
+                    for (size_t i = 0; i < Gd.vi.size(); ++i) m->grid_coef[i] = h.values[Gd.vi[i]];
+                    // the hex stencil's structure: equal values within each class, zeros where expected
+                    bool hex = true, seen[dvk::kHexClasses] = {};
+                    for (int i = 0; i < 243 && hex; ++i) {
+                        const int c = dvk::hex_class(i);
+                        const double v = m->grid_coef[i];
+                        if (c < 0) hex = v == 0.0 && !std::signbit(v);
+                        else if (!seen[c]) { seen[c] = true; m->grid_cls[c] = v; }
+                        else hex = v == m->grid_cls[c] && std::signbit(v) == std::signbit(m->grid_cls[c]);
+                    }
+                    m->grid_hex = hex ? 1 : 0;
+                    // FP64 runs the stencil with the hex structure only (the general FP64 stencil would
+                    // hold 243 coefficients in registers); otherwise the node patterns stay
+                    m->grid_ok = m->grid_hex || m->precision == DV_F32;
+                    m->grid_nb = (int64_t)Gd.boundary.size();
+                    if (m->grid_ok) {
+                        upload(m->grid_bnode, Gd.boundary.data(), 4 * Gd.boundary.size(), s);
+                        DV_CUDA(cudaStreamSynchronize(s));
+                        m->duvi_variant = 3;
+                    }
+                }
             }
         }
     }
@@ -275,16 +307,19 @@ static void autotune(dv_matrix *m) {
     // CSR: threads per row; DuVi: 4 / 9 = staged kernel with that batch width, 100 = lane kernel
     std::vector<int> cand = m->format == DV_FORMAT_CSR ? std::vector<int>{8, 16, 32} : std::vector<int>{4, 9, 100};
     if (m->format == DV_FORMAT_DUVI && m->pat_ok) cand.push_back(200);
+    if (m->format == DV_FORMAT_DUVI && m->grid_ok) cand.push_back(300);
     cudaEvent_t e0, e1;
     DV_CUDA(cudaEventCreate(&e0));
     DV_CUDA(cudaEventCreate(&e1));
     float best = 1e30f;
     auto current = [&] {
         return m->format == DV_FORMAT_CSR ? m->csr_tpr
-                                          : (m->duvi_variant == 2 ? 200 : m->duvi_variant == 1 ? 100 : m->duvi_batch);
+                                          : (m->duvi_variant == 3 ? 300 : m->duvi_variant == 2 ? 200
+                                             : m->duvi_variant == 1 ? 100 : m->duvi_batch);
     };
     auto apply = [&](int v) {
         if (m->format == DV_FORMAT_CSR) m->csr_tpr = v;
+        else if (v == 300) m->duvi_variant = 3;
         else if (v == 200) m->duvi_variant = 2;
         else if (v == 100) m->duvi_variant = 1;
         else { m->duvi_variant = 0; m->duvi_batch = v; }
@@ -440,7 +475,8 @@ extern "C" DV_API int dv_matrix_get_info(const dv_matrix *m, dv_matrix_info *inf
         info->precision = m->precision;
         info->value_index_bits = m->format == DV_FORMAT_DUVI ? m->vi_bits : 0;
         info->kernel_variant = m->format == DV_FORMAT_CSR ? m->csr_tpr
-                               : (m->duvi_variant == 2 ? 200 + m->lanes_group
+                               : (m->duvi_variant == 3 ? 300 + m->lanes_group
+                                  : m->duvi_variant == 2 ? 200 + m->lanes_group
                                   : m->duvi_variant == 1 ? 100 + m->lanes_group : m->duvi_batch);
         info->device_bytes = m->device_bytes;
         info->row_group = m->row_group;

@@ -287,26 +287,113 @@ def test_lane_kernel_node_tuples_and_fallback(ctx, native, oracle, rng, pool, mo
 
 
 
+LAYOUTS = {"grid": ("1", "1", 303), "patterns": ("1", "0", 203), "lanes": ("0", "0", 103)}
+
+
 @pytest.mark.parametrize("ne", [(8, 8, 8), (16, 4, 4), (7, 5, 9), (40, 21, 13)])
-@pytest.mark.parametrize("patterns", ["1", "0"])
-def test_hex_operator_pattern_and_lane_kernels_bit_exact(ctx, native, oracle, rng, ne, patterns, monkeypatch):
+@pytest.mark.parametrize("layout", ["grid", "patterns", "lanes"])
+def test_hex_operator_grid_pattern_and_lane_kernels_bit_exact(ctx, native, oracle, rng, ne, layout, monkeypatch):
     # The hex stiffness repeats one entry list per node class (interior, faces, edges,
-    # corners): with patterns on, one pattern id per node and a shared-memory pattern
-    # table (variant 203); with them off, the lane layout with stencil offsets and node
-    # tuples (variant 103).  Both sum every row in storage order: bit-exact in FP64.
-    # (40, 21, 13) spans many blocks of the grid-stride loop.
+    # corners).  grid (variant 303): interior nodes by the plane-streaming stencil with the
+    # interior pattern's values as kernel parameters, the others from their records;
+    # patterns (203): one pattern id per node and a shared-memory pattern table; lanes
+    # (103): the lane layout with stencil offsets and node tuples.  All sum every row in
+    # storage order: bit-exact in FP64.  (40, 21, 13) spans two x tiles (one partial), three
+    # y tiles and several z runs.
+    patterns, grid, variant = LAYOUTS[layout]
     monkeypatch.setenv("DV_PATTERNS", patterns)
+    monkeypatch.setenv("DV_GRID", grid)
     A = native.hex_stiffness(ne)
     x = rng.standard_normal(A.shape[1])
     ref = oracle.DuVi(oracle.Csr.from_scipy(A)).spmv(x)
     M = native.SparseMatrix(ctx, A, "duvi", "f64")
-    assert M.info()["kernel_variant"] == (203 if patterns == "1" else 103)
+    assert M.info()["kernel_variant"] == variant
     np.testing.assert_array_equal(M.Multiply(x), ref)
     y0 = rng.standard_normal(A.shape[0])
     np.testing.assert_array_equal(M.Multiply(x, y0.copy(), clear=False),
                                   oracle.DuVi(oracle.Csr.from_scipy(A)).spmv(x, y0.copy(), clear=False))
     F = native.SparseMatrix(ctx, A, "duvi", "f32")
+    assert F.info()["kernel_variant"] == variant
     assert rowwise_rel(F.Multiply(x), A @ x, A, x) <= REL32
+
+
+def _device_product(ctx, M, x, dtype):
+    import torch
+    dx = torch.from_numpy(np.ascontiguousarray(x, dtype)).cuda()
+    dy = torch.zeros(M.shape[0], dtype=dx.dtype, device="cuda")
+    torch.cuda.synchronize()
+    M.multiply_device(dx.data_ptr(), dy.data_ptr(), "f32" if dtype == np.float32 else "f64")
+    ctx.synchronize()
+    return dy.cpu().numpy()
+
+
+def _grid_vs_patterns(native, ctx, A, x, prec, monkeypatch, expect_grid=303):
+    monkeypatch.setenv("DV_GRID", "1")
+    G = native.SparseMatrix(ctx, A, "duvi", prec)
+    assert G.info()["kernel_variant"] == expect_grid
+    monkeypatch.setenv("DV_GRID", "0")
+    Pm = native.SparseMatrix(ctx, A, "duvi", prec)
+    assert Pm.info()["kernel_variant"] == 203
+    dt = np.float32 if prec == "f32" else np.float64
+    return _device_product(ctx, G, x, dt), _device_product(ctx, Pm, x, dt)
+
+
+@pytest.mark.parametrize("ne", [(8, 8, 8), (33, 9, 20), (64, 17, 10)])
+def test_grid_stencil_f32_equals_pattern_kernel(ctx, native, rng, ne, monkeypatch):
+    # FP32 products on device vectors: the grid stencil (hex value classes, structural zeros
+    # skipped) and the node-pattern kernel give the same floats (the same fused multiply-adds in
+    # the same order; the skipped terms add exact zeros).
+    monkeypatch.setenv("DV_AUTOTUNE", "0")
+    A = native.hex_stiffness(ne, scale=2.0)
+    x = rng.standard_normal(A.shape[1])
+    yg, yp = _grid_vs_patterns(native, ctx, A, x, "f32", monkeypatch)
+    np.testing.assert_array_equal(yg, yp)
+
+
+def test_grid_stencil_general_coefficients(ctx, native, oracle, rng, monkeypatch):
+    # An operator with the 27-neighbour interior pattern but without the hex value classes (one
+    # coupling changed by the same amount in every row of dof 0 with a +x neighbour): FP32 runs
+    # the general stencil (all 243 coefficients) and equals the pattern kernel; FP64 keeps the
+    # node patterns (variant 203) and equals the oracle's walk.
+    ne = (20, 11, 9)
+    A = native.hex_stiffness(ne).tolil()
+    lx = ne[0]
+    for i in range(A.shape[0] // 3):
+        if (i % lx) < lx - 1:
+            A[3 * i, 3 * (i + 1)] += 1e-3
+    A = A.tocsr()
+    A.sort_indices()
+    x = rng.standard_normal(A.shape[1])
+    yg, yp = _grid_vs_patterns(native, ctx, A, x, "f32", monkeypatch)
+    np.testing.assert_array_equal(yg, yp)
+    monkeypatch.setenv("DV_GRID", "1")
+    M = native.SparseMatrix(ctx, A, "duvi", "f64")
+    assert M.info()["kernel_variant"] == 203
+    np.testing.assert_array_equal(M.Multiply(x), oracle.DuVi(oracle.Csr.from_scipy(A)).spmv(x))
+
+
+def test_grid_stencil_interior_nodes_of_other_patterns(ctx, native, oracle, rng, monkeypatch):
+    # A few elements with other moduli: the interior nodes around them get their own patterns
+    # and run from their records inside the grid launch; FP64 stays bit-exact with the oracle,
+    # the residual r = b - A x too.
+    import torch
+    monkeypatch.setenv("DV_GRID", "1")
+    ne = (24, 10, 12)
+    E = np.ones(int(np.prod(ne)))
+    E[rng.choice(E.size, 7, replace=False)] = 2.0
+    A = native.hex_stiffness(ne, E)
+    x = rng.standard_normal(A.shape[1])
+    M = native.SparseMatrix(ctx, A, "duvi", "f64")
+    assert M.info()["kernel_variant"] == 303
+    ref = oracle.DuVi(oracle.Csr.from_scipy(A)).spmv(x)
+    np.testing.assert_array_equal(M.Multiply(x), ref)
+    b = rng.standard_normal(A.shape[0])
+    db, dx = torch.from_numpy(b).cuda(), torch.from_numpy(x).cuda()
+    dr = torch.empty_like(db)
+    torch.cuda.synchronize()
+    M.residual_device(db.data_ptr(), dx.data_ptr(), dr.data_ptr(), "f64")
+    ctx.synchronize()
+    np.testing.assert_array_equal(dr.cpu().numpy(), b - ref)
 
 
 @pytest.mark.parametrize("k", [5, 40, 130])
