@@ -12,14 +12,15 @@ from .adjoint import AdjointCantilever, cantilever_solve_function, element_gradi
 from .solvers import (CudaCsrGeometricMultigridSolver, CudaCsrPcgSolver, CudaDuViGeometricMultigridSolver,
                       BatchedMultigridSolver, IterativeStatistics, MultigridPcgSolver, make_path)
 from .cantilever import (FemCantilever3D, cantilever_batch, cartesian_transfer, duvi_encode, galerkin,
-                         galerkin_hierarchy, hex_hierarchy, hex_stiffness, hex_trilinear, random_face_loads,
+                         galerkin_hierarchy, hex_assemble_device, hex_csr_size, hex_hierarchy, hex_stiffness,
+                         hex_trilinear, random_face_loads,
                          traction_rhs, units_decode, units_encode)
 
 __all__ = [
     "AdjointCantilever", "cantilever_solve_function", "element_gradient_device",
     "CudaContext", "SparseMatrix", "CudaCsrGeometricMultigridSolver", "CudaDuViGeometricMultigridSolver",
     "CudaCsrPcgSolver", "MultigridPcgSolver", "BatchedMultigridSolver", "cantilever_batch", "IterativeStatistics", "FemCantilever3D", "hex_hierarchy",
-    "hex_stiffness", "hex_trilinear", "duvi_encode", "units_encode", "units_decode", "galerkin", "galerkin_hierarchy", "traction_rhs", "random_face_loads", "cartesian_transfer", "make_path", "DuviError",
+    "hex_stiffness", "hex_assemble_device", "hex_csr_size", "hex_trilinear", "duvi_encode", "units_encode", "units_decode", "galerkin", "galerkin_hierarchy", "traction_rhs", "random_face_loads", "cartesian_transfer", "make_path", "DuviError",
     "NotImplementedFeatureError", "NotInitializedError", "NoDeviceError",
 ]
 

@@ -33,6 +33,21 @@ def hex_stiffness(ne, elem_E=None, scale=1.0, E=1.0, nu=0.3):
     return sp.csr_matrix((va, ci, rp), shape=(nr.value, nr.value))
 
 
+def hex_assemble_device(ctx, ne, d_rowptr, d_col, d_val, d_elem_E=None, scale=1.0, E=1.0, nu=0.3):
+    """The same free-dof stiffness assembled on the device into caller-owned device arrays
+    (pointers; sizes from hex_csr_size), bit for bit equal to hex_stiffness."""
+    ne = np.ascontiguousarray(ne, np.int32)
+    N.check(N.lib().dv_hex_assemble_device(ctx.h, N.ptr(ne), d_elem_E, scale, E, nu, d_rowptr, d_col, d_val))
+
+
+def hex_csr_size(ne):
+    """(rows, stored entries) of the free-dof hexa stiffness."""
+    ne = np.ascontiguousarray(ne, np.int32)
+    nr, nnz = C.c_int32(), C.c_int64()
+    N.check(N.lib().dv_hex_csr_size(N.ptr(ne), C.byref(nr), C.byref(nnz)))
+    return nr.value, nnz.value
+
+
 def hex_trilinear(ne_fine):
     """Trilinear prolongation of the factor-2 vertex coarsening (coarse nodes at the even
     fine nodes and the last one, so odd element counts coarsen to ceil(n/2))."""

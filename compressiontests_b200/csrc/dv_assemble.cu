@@ -1,0 +1,132 @@
+// On-device assembly of the structured hexahedral stiffness (free dofs, sorted CSR).
+//
+// The reference assembles element by element into a dictionary-of-keys builder
+// (FemCantileverBase.AssembleGlobalMatrix, FemCantileverBase.cs:87-104, through
+// DokRowMajor.AddSubmatrix, DokRowMajor.cs:182-207) and converts it to CSR
+// (DokRowMajor.BuildCsrArrays, :286-324).  Every stored entry (i, j) is therefore
+// the sum, in increasing element id, of (scale * E_e) * Ke(a_i, a_j) over the
+// elements that contain both dofs, the first term added to +0.0; rows are sorted
+// by column and structural zeros are kept.  Here one thread owns one free node
+// (its three rows) and writes its entries straight into the CSR arrays, with
+// separately rounded products and sums in exactly that order, so the arrays equal
+// the host assembler's (dv_hex_assemble) bit for bit.  Row offsets are closed-form:
+// the number of stored columns of a node is a product of per-axis neighbour
+// counts, so the entries before a node are sums of per-axis prefix counts.
+#include "dv_kernels.cuh"
+
+#include <algorithm>
+#include <vector>
+
+using namespace dvk;
+
+namespace {
+
+struct HexAxes {
+    int32_t nx, ny, nz;            // node counts per axis (x: node 0 is clamped)
+    int32_t ne0, ne1, ne2;         // element counts per axis
+    int64_t sx, sy;                // sums of the x (free nodes) and y neighbour counts
+};
+
+// neighbours of a node along one axis (itself included); x counts free nodes 1..nx-1 only
+__device__ __forceinline__ int nbr_x(int32_t i, int32_t nx) { return (i > 1 ? 1 : 0) + 1 + (i + 1 < nx ? 1 : 0); }
+__device__ __forceinline__ int nbr_yz(int32_t j, int32_t n) { return (j > 0 ? 1 : 0) + 1 + (j + 1 < n ? 1 : 0); }
+// sums of those counts over the nodes before i: free x nodes 1..i-1 (3 each, minus node 1's
+// missing -x neighbour); y or z nodes 0..j-1 (3 each, minus node 0's missing -y neighbour)
+__device__ __forceinline__ int64_t pre_x(int32_t i) { return i <= 1 ? 0 : 3 * (int64_t)(i - 1) - 1; }
+__device__ __forceinline__ int64_t pre_yz(int32_t j) { return j <= 0 ? 0 : 3 * (int64_t)j - 1; }
+
+__global__ void k_hex_assemble(HexAxes H, const double *__restrict__ ke_g, const double *__restrict__ elem_E,
+                               double scale, int32_t *__restrict__ rowptr, int32_t *__restrict__ col,
+                               double *__restrict__ val) {
+    __shared__ double ke[576];
+    __shared__ int vtk[8];
+    for (int t = threadIdx.x; t < 576; t += blockDim.x) ke[t] = ke_g[t];
+    if (threadIdx.x < 8) {
+        const int v[8] = {0, 1, 3, 2, 4, 5, 7, 6};   // lexicographic corner (dx + 2 dy + 4 dz) -> VTK hexa order
+        vtk[threadIdx.x] = v[threadIdx.x];
+    }
+    __syncthreads();
+    const int32_t fx = H.nx - 1;   // free nodes per x line
+    const int64_t nodes = (int64_t)fx * H.ny * H.nz;
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < nodes; q += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t i = (int32_t)(q % fx) + 1, j = (int32_t)((q / fx) % H.ny), k = (int32_t)(q / ((int64_t)fx * H.ny));
+        const int cx = nbr_x(i, H.nx), cy = nbr_yz(j, H.ny), cz = nbr_yz(k, H.nz);
+        // stored entries before this node: 9 per pair of neighbouring nodes (3 rows x 3 columns)
+        const int64_t before = 9 * (pre_yz(k) * H.sy * H.sx + (int64_t)cz * pre_yz(j) * H.sx + (int64_t)cz * cy * pre_x(i));
+        const int32_t per_row = 3 * cx * cy * cz;
+        const int32_t r0 = (int32_t)(3 * q);
+        for (int d = 0; d < 3; ++d) {
+            int64_t p = before + (int64_t)d * per_row;
+            rowptr[r0 + d] = (int32_t)p;
+            if (q == nodes - 1 && d == 2) rowptr[r0 + 3] = (int32_t)(p + per_row);
+            for (int dk = -1; dk <= 1; ++dk)
+                for (int dj = -1; dj <= 1; ++dj)
+                    for (int di = -1; di <= 1; ++di) {
+                        const int32_t ii = i + di, jj = j + dj, kk = k + dk;
+                        if (ii < 1 || ii >= H.nx || jj < 0 || jj >= H.ny || kk < 0 || kk >= H.nz) continue;
+                        const int32_t c0 = max(max(k, kk) - 1, 0), c1 = min(min(k, kk), H.ne2 - 1);
+                        const int32_t b0 = max(max(j, jj) - 1, 0), b1 = min(min(j, jj), H.ne1 - 1);
+                        const int32_t a0 = max(max(i, ii) - 1, 0), a1 = min(min(i, ii), H.ne0 - 1);
+                        const int32_t cbase = 3 * ((ii - 1) + fx * (jj + H.ny * kk));
+                        for (int d2 = 0; d2 < 3; ++d2) {
+                            double s = 0.0;
+                            bool first = true;
+                            for (int32_t c = c0; c <= c1; ++c)
+                                for (int32_t b = b0; b <= b1; ++b)
+                                    for (int32_t a = a0; a <= a1; ++a) {
+                                        const int64_t e = a + (int64_t)H.ne0 * (b + (int64_t)H.ne1 * c);
+                                        const int la = vtk[(i - a) + 2 * (j - b) + 4 * (k - c)];
+                                        const int lb = vtk[(ii - a) + 2 * (jj - b) + 4 * (kk - c)];
+                                        const double ce = elem_E ? __dmul_rn(scale, __ldg(elem_E + e)) : scale;
+                                        const double t = __dmul_rn(ce, ke[(3 * la + d) * 24 + 3 * lb + d2]);
+                                        s = first ? __dadd_rn(t, 0.0) : __dadd_rn(t, s);
+                                        first = false;
+                                    }
+                            col[p] = cbase + d2;
+                            val[p] = s;
+                            ++p;
+                        }
+                    }
+        }
+    }
+}
+
+}  // namespace
+
+extern "C" DV_API int dv_hex_assemble_device(dv_context *ctx, const int32_t *ne, const double *d_elem_E, double scale,
+                                             double E, double nu, int32_t *d_rowptr, int32_t *d_col, double *d_val) {
+    return dv_guard([&] {
+        dv_ctx_check(ctx);
+        int32_t nrows;
+        int64_t nnz;
+        const int st = dv_hex_csr_size(ne, &nrows, &nnz);
+        DV_REQUIRE(st == DV_OK, st, "bad mesh");
+        DV_REQUIRE(d_rowptr && d_col && d_val, DV_ERR_ARG, "null output array");
+        DV_REQUIRE(nnz < INT32_MAX, DV_ERR_ARG, "more stored entries than int32 row offsets hold");
+        std::vector<double> ke(576);
+        dv_hex_ke(E, nu, ke.data());
+        cudaStream_t s = ctx->stream;
+        DevMem dke(sizeof(double) * 576);
+        DV_CUDA(cudaMemcpyAsync(dke.p, ke.data(), sizeof(double) * 576, cudaMemcpyHostToDevice, s));
+        HexAxes H;
+        H.nx = ne[0] + 1;
+        H.ny = ne[1] + 1;
+        H.nz = ne[2] + 1;
+        H.ne0 = ne[0];
+        H.ne1 = ne[1];
+        H.ne2 = ne[2];
+        auto total = [](int32_t n, bool clamp) {   // sum of the neighbour counts along one axis
+            int64_t t = 0;
+            for (int32_t i = clamp ? 1 : 0; i < n; ++i) t += (clamp ? (i > 1) : (i > 0)) + 1 + (i + 1 < n);
+            return t;
+        };
+        H.sx = total(H.nx, true);
+        H.sy = total(H.ny, false);
+        const int64_t nodes = (int64_t)nrows / 3;
+        const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((nodes + 127) / 128, (int64_t)ctx->num_sms * 16));
+        k_hex_assemble<<<blocks, 128, 0, s>>>(H, dke.as<double>(), d_elem_E, scale, d_rowptr, d_col, d_val);
+        DV_CUDA(cudaGetLastError());
+        ctx->count();
+        DV_CUDA(cudaStreamSynchronize(s));   // dke is released on return
+    });
+}

@@ -366,6 +366,15 @@ DV_API int dv_hex_element_gradient(dv_context *ctx, const int32_t *ne, const dou
 DV_API int dv_hex_csr_size(const int32_t *ne, int32_t *n_rows, int64_t *nnz);
 DV_API int dv_hex_assemble(const int32_t *ne, const double *elem_E, double scale, double E, double nu,
                            int32_t *rowptr, int32_t *col, double *val);
+/* The same assembly on the device, bit for bit (one thread per node writes its three
+ * rows in the summation order above): d_rowptr, d_col, d_val are device arrays of
+ * n_rows + 1, nnz and nnz elements (sizes from dv_hex_csr_size, nnz < 2^31); d_elem_E
+ * is a device array of ne[0] ne[1] ne[2] moduli, or NULL for a uniform modulus.
+ * Replaces the element loop of FemCantileverBase.AssembleGlobalMatrix
+ * (FemCantileverBase.cs:87-104) into DokRowMajor (DokRowMajor.cs:182-207, 286-324).
+ * Context stream; returns when the arrays are written. */
+DV_API int dv_hex_assemble_device(dv_context *ctx, const int32_t *ne, const double *d_elem_E, double scale, double E,
+                                  double nu, int32_t *d_rowptr, int32_t *d_col, double *d_val);
 /* Trilinear prolongation of the factor-2 vertex coarsening (fine free x coarse
  * free).  Per axis with n elements the coarse nodes are the even fine nodes
  * and the last one, so odd n coarsens to (n+1)/2 elements (the last of length
