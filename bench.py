@@ -54,7 +54,8 @@ METRIC = "MG-PCG time to 1e-8 rel. residual (mixed FP32/FP64, 128^3 hex elastici
 # dv_matrix_info.kernel_variant -> kernel (DuVi: 100 + g lane layout, 200 + g node patterns,
 # 300 + g grid stencil; CSR: threads per row; DuVi 4 / 9: staged row bundles)
 KERNEL_NAMES = {101: "k_duvi_lanes", 102: "k_duvi_lanes", 103: "k_duvi_lanes", 201: "k_duvi_pattern",
-                202: "k_duvi_pattern", 203: "k_duvi_pattern", 303: "k_duvi_grid", 4: "k_duvi", 9: "k_duvi"}
+                202: "k_duvi_pattern", 203: "k_duvi_pattern", 303: "k_duvi_grid", 400: "k_hex_elem", 4: "k_duvi",
+                9: "k_duvi"}
 # derived layouts whose matrix costs ~2 bytes per node group: their algorithmic bytes are the vectors
 DERIVED_SHAPES = {201, 202, 203, 303}
 OMEGA_EFF = (2.0 / 3.0) * 2.0 / (1.1 * 3.09)   # 2/3 of the spectrally normalised Jacobi weight (lambda ~ 3.09)
@@ -306,8 +307,39 @@ def spmv_log_uniform(cb, ctx, n, reps, peak):
     A0 = cb.hex_stiffness((n, n, n), E)
     t_asm = time.time() - t
     out, _ = spmv_table(cb, ctx, A0, reps, peak, (("csr", "f64"), ("duvi", "f64")))
+    del A0
+    out.update(hex_operator_spmv(cb, ctx, (n, n, n), E, reps, peak))
     return {"size": f"{n}^3", "elem_E": "10^U(-2,0) per element, seed 20261203", "assembly_s": round(t_asm, 1),
             **out}
+
+
+def hex_operator_spmv(cb, ctx, ne, E, reps, peak):
+    """The same operator applied matrix-free (element kernel): one factor per element, x and y."""
+    import torch
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    out = {}
+    for prec in ("f64", "f32"):
+        H = cb.SparseMatrix.hex_operator(ctx, ne, E, precision=prec)
+        n = H.shape[0]
+        dt = torch.float32 if prec == "f32" else torch.float64
+        x = torch.randn(n, dtype=dt, device="cuda", generator=torch.Generator(device="cuda").manual_seed(20261203))
+        y = torch.zeros_like(x)
+        torch.cuda.synchronize()
+        fn = lambda: H.multiply_device(x.data_ptr(), y.data_ptr(), prec)
+        for _ in range(3):
+            fn()
+        ctx.synchronize()
+        ms = time_launches(stream, fn, reps)
+        vs = 4 if prec == "f32" else 8
+        alg = H.info()["device_bytes"] + 2 * vs * n
+        out[f"hex_{prec}"] = {"ms": round(ms, 4), "algorithmic_bytes": int(alg), "GBps": round(alg / ms / 1e6, 1),
+                              "frac_of_peak": round(alg / ms / 1e6 / peak, 3), "launch_shape": 400,
+                              "kernel": "k_hex_elem", "format_bytes": int(alg),
+                              "format_GBps": round(alg / ms / 1e6, 1)}
+        H.release()
+        del x, y
+        torch.cuda.empty_cache()
+    return out
 
 
 def cpu_solve(A, P, b, threads, tol):

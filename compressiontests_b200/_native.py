@@ -24,7 +24,7 @@ DV_ERR_FORMAT = -6
 DV_ERR_NO_DEVICE = -7
 DV_ERR_SINGULAR = -8
 
-FORMAT_CSR, FORMAT_DUVI = 0, 1
+FORMAT_CSR, FORMAT_DUVI, FORMAT_HEX = 0, 1, 2
 F64, F32, MIXED = 0, 1, 2
 SMOOTHER_JACOBI, SMOOTHER_GS_LEX, SMOOTHER_GS_COLOR = 0, 1, 2
 OMEGA_ABSOLUTE, OMEGA_SPECTRAL = 0, 1
@@ -136,6 +136,7 @@ _SIGNATURES = {
     "dv_hex_element_gradient": (C.c_int, [_vp, _vp, _vp, C.c_double, C.c_double, C.c_double, _vp, _vp, _vp]),
     "dv_hex_csr_size": (C.c_int, [_vp, _P(C.c_int32), _P(C.c_int64)]),
     "dv_hex_assemble": (C.c_int, [_vp, _vp, C.c_double, C.c_double, C.c_double, _vp, _vp, _vp]),
+    "dv_matrix_create_hex": (C.c_int, [_vp, _vp, _vp, C.c_double, C.c_double, C.c_double, C.c_int32, _P(_vp)]),
     "dv_hex_assemble_device": (C.c_int, [_vp, _vp, _vp, C.c_double, C.c_double, C.c_double, _vp, _vp, _vp]),
     "dv_hex_trilinear_size": (C.c_int, [_vp, _P(C.c_int32), _P(C.c_int32), _P(C.c_int64)]),
     "dv_hex_trilinear": (C.c_int, [_vp, _vp, _vp, _vp]),

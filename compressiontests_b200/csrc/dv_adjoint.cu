@@ -16,6 +16,7 @@
 #include "dv_mgpcg.cuh"
 
 #include <cmath>
+#include <cstdlib>
 #include <vector>
 
 namespace {
@@ -103,6 +104,7 @@ struct dv_adjoint {
     dv_mgpcg *solver = nullptr;
     DevMem rho, ke, u, lam, grad, f;
     bool have_u = false;
+    bool matrix_free = false;   // finest operator applied element by element (DV_FORMAT_HEX)
     ~dv_adjoint() {
         if (solver) dv_mgpcg_destroy(solver);
     }
@@ -200,6 +202,30 @@ extern "C" DV_API int dv_adjoint_create(dv_context *ctx, const int32_t *ne, cons
         for (auto &p : P) pv.push_back(p.view());
         int st = dv_mgpcg_create(ctx, (int32_t)av.size(), av.data(), pv.data(), cfg, &s->solver);
         DV_REQUIRE(st == DV_OK, st, dv_last_error());
+        // The finest operator K(rho) has a factor per element and no repeating rows: the solver
+        // applies it matrix-free (element kernel) in the outer FP64 loop and in the finest level
+        // of the Jacobi V-cycle; the coarse Galerkin levels stay assembled.  DV_MATRIX_FREE=0
+        // keeps the assembled operator (A/B comparisons).
+        const char *mf = getenv("DV_MATRIX_FREE");
+        if (!(mf && mf[0] == '0') && cfg->smoother == DV_SMOOTHER_JACOBI) {
+            dv_mgpcg *m = s->solver;
+            dv_matrix *h64 = nullptr;
+            st = dv_matrix_create_hex(ctx, ne, scale_e.data(), 1.0, E0, nu, DV_F64, &h64);
+            DV_REQUIRE(st == DV_OK, st, dv_last_error());
+            m->Aout.reset(h64);
+            if (m->v32) {
+                dv_matrix *h32 = nullptr;
+                st = dv_matrix_create_hex(ctx, ne, scale_e.data(), 1.0, E0, nu, DV_F32, &h32);
+                DV_REQUIRE(st == DV_OK, st, dv_last_error());
+                m->v32->lv[0].A.reset(h32);
+            } else {
+                dv_matrix *h = nullptr;
+                st = dv_matrix_create_hex(ctx, ne, scale_e.data(), 1.0, E0, nu, DV_F64, &h);
+                DV_REQUIRE(st == DV_OK, st, dv_last_error());
+                m->v64->lv[0].A.reset(h);
+            }
+            s->matrix_free = true;
+        }
         // device copies
         cudaStream_t stream = ctx->stream;
         std::vector<double> ke(576);

@@ -12,6 +12,11 @@
 // the host assembler's (dv_hex_assemble) bit for bit.  Row offsets are closed-form:
 // the number of stored columns of a node is a product of per-axis neighbour
 // counts, so the entries before a node are sums of per-axis prefix counts.
+//
+// dv_matrix_create_hex builds the matrix-free form of the same operator (the element
+// kernel k_hex_elem): the per-element factors on the device, the value classes of Ke,
+// and the diagonal for Jacobi weights (summed on the host in the assembly's order, so it
+// equals the assembled matrix's diagonal bit for bit).
 #include "dv_kernels.cuh"
 
 #include <algorithm>
@@ -128,5 +133,80 @@ extern "C" DV_API int dv_hex_assemble_device(dv_context *ctx, const int32_t *ne,
         DV_CUDA(cudaGetLastError());
         ctx->count();
         DV_CUDA(cudaStreamSynchronize(s));   // dke is released on return
+    });
+}
+
+extern "C" DV_API int dv_matrix_create_hex(dv_context *ctx, const int32_t *ne, const double *elem_E, double scale,
+                                           double E, double nu, int32_t precision, dv_matrix **out) {
+    return dv_guard([&] {
+        DV_REQUIRE(ne && out, DV_ERR_ARG, "null argument");
+        DV_REQUIRE(precision == DV_F64 || precision == DV_F32, DV_ERR_ARG, "precision must be DV_F64 or DV_F32");
+        dv_ctx_check(ctx);
+        int32_t nrows;
+        int64_t nnz;
+        const int st = dv_hex_csr_size(ne, &nrows, &nnz);
+        DV_REQUIRE(st == DV_OK, st, "bad mesh");
+        std::vector<double> ke(576);
+        dv_hex_ke(E, nu, ke.data());
+        auto m = std::make_unique<dv_matrix>();
+        bool seen[kKeClasses] = {};
+        for (int i = 0; i < 576; ++i) {
+            const int c = ke_class(i);
+            if (!seen[c]) {
+                seen[c] = true;
+                m->hex_cls[c] = ke[i];
+            } else {
+                DV_REQUIRE(ke[i] == m->hex_cls[c], DV_ERR_UNSUPPORTED, "element stiffness without the hexahedron's symmetries");
+            }
+        }
+        const int64_t nel = (int64_t)ne[0] * ne[1] * ne[2];
+        std::vector<double> f(nel);
+        for (int64_t e = 0; e < nel; ++e) f[e] = elem_E ? scale * elem_E[e] : scale;
+        m->ctx = ctx;
+        m->n_rows = m->n_cols = nrows;
+        m->nnz = nnz;
+        m->format = DV_FORMAT_HEX;
+        m->precision = precision;
+        for (int d = 0; d < 3; ++d) m->hex_ne[d] = ne[d];
+        cudaStream_t s = ctx->stream;
+        if (precision == DV_F64) {
+            m->hex_factor.alloc(8 * (size_t)nel);
+            DV_CUDA(cudaMemcpyAsync(m->hex_factor.p, f.data(), 8 * (size_t)nel, cudaMemcpyHostToDevice, s));
+        } else {
+            std::vector<float> f32(f.begin(), f.end());
+            m->hex_factor.alloc(4 * (size_t)nel);
+            DV_CUDA(cudaMemcpyAsync(m->hex_factor.p, f32.data(), 4 * (size_t)nel, cudaMemcpyHostToDevice, s));
+            DV_CUDA(cudaStreamSynchronize(s));
+        }
+        // diagonal: sum over the node's elements in increasing id of (scale E_e) Ke(a, a), as assembled
+        const int32_t nx = ne[0] + 1, ny = ne[1] + 1, nz = ne[2] + 1;
+        static const int vtk[8] = {0, 1, 3, 2, 4, 5, 7, 6};
+        m->host_diag.assign(nrows, 0.0);
+#pragma omp parallel for collapse(2) schedule(static)
+        for (int32_t k = 0; k < nz; ++k)
+            for (int32_t j = 0; j < ny; ++j)
+                for (int32_t i = 1; i < nx; ++i) {
+                    const int32_t r0 = 3 * ((i - 1) + (nx - 1) * (j + ny * k));
+                    for (int d = 0; d < 3; ++d) {
+                        double s2 = 0.0;
+                        bool first = true;
+                        for (int32_t c = std::max(k - 1, 0); c <= std::min(k, ne[2] - 1); ++c)
+                            for (int32_t b = std::max(j - 1, 0); b <= std::min(j, ne[1] - 1); ++b)
+                                for (int32_t a = std::max(i - 1, 0); a <= std::min(i, ne[0] - 1); ++a) {
+                                    const int64_t e = a + (int64_t)ne[0] * (b + (int64_t)ne[1] * c);
+                                    const int la = vtk[(i - a) + 2 * (j - b) + 4 * (k - c)];
+                                    const double t = f[e] * ke[(3 * la + d) * 24 + 3 * la + d];
+                                    s2 = first ? t + 0.0 : t + s2;
+                                    first = false;
+                                }
+                        m->host_diag[r0 + d] = s2;
+                    }
+                }
+        m->zero_diag = std::any_of(m->host_diag.begin(), m->host_diag.end(), [](double d) { return d == 0.0; });
+        m->diag.alloc(8 * (size_t)nrows);
+        DV_CUDA(cudaMemcpyAsync(m->diag.p, m->host_diag.data(), 8 * (size_t)nrows, cudaMemcpyHostToDevice, s));
+        DV_CUDA(cudaStreamSynchronize(s));
+        m->device_bytes = (int64_t)(precision == DV_F64 ? 8 : 4) * nel;
+        *out = m.release();
     });
 }

@@ -229,6 +229,9 @@ struct dv_matrix {
     double grid_cls[10] = {};            // its class values
     DevMem grid_bnode;                   // u32 boundary groups
     int64_t grid_nb = 0;
+    int32_t hex_ne[3] = {0, 0, 0};       // DV_FORMAT_HEX: elements per axis
+    DevMem hex_factor;                   // per-element factor scale * E_e, matrix precision
+    double hex_cls[14] = {};             // value classes of Ke (dvk::ke_class)
     int lanes_stencil = 0;     // stencil mode: lanes_off holds the column offsets (int32)
     DevMem lanes_off;
     int32_t lanes_noff = 0;

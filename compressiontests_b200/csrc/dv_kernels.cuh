@@ -1244,9 +1244,268 @@ void launch_csr_tpr(const LaunchEnv &e, const dv_matrix *m, Gather g, Op op) {
     e.ctx->count();
 }
 
+// ---------------------------------------------------------------------------
+// Matrix-free hexahedral operator (DV_FORMAT_HEX): y = K(E) x with K = sum_e f_e Ke on a
+// structured grid of unit-cube trilinear hexahedra, f_e = scale * E_e per element, the
+// nodes of the x = 0 face clamped (FemCantileverBase.cs:87-158, FemCantilever3D.cs:27-132).
+//
+// Nothing of the matrix is stored: a product reads the element factors (one value per
+// element), x and writes y.  A block owns a tile of 32 x 8 free nodes of the xy plane and a
+// run of zc planes and streams node planes of x and layers of element factors through
+// shared memory (x planes double buffered, factor layers triple buffered because each layer
+// is read in two consecutive steps).  At plane p every thread loads its 3 x 3 x 3
+// neighbourhood of x once and forms, for the 8 elements around its node column, the
+// element rows Ke(a, b) x_b of the corners b in plane p, scaled by the element factor, into
+// the three nodes it accumulates (planes p + 1, p, p - 1).  Elements outside the mesh have
+// factor 0 and clamped or outside nodes have x = 0, so face and edge nodes need no special
+// case.  Ke enters through its 14 value classes (ke_class): equal entries share one
+// register-resident value.  The sum order differs from the assembled operator's, so FP64
+// products agree with the assembled matrix to rounding (not bit for bit).
+// ---------------------------------------------------------------------------
+
+// Value classes of the 24 x 24 unit-cube hexahedron stiffness (VTK corner order, 3 dofs per
+// corner, entry (3 a + d, 3 b + c) at 24 (3 a + d) + 3 b + c): entries of one class are equal
+// for every modulus and Poisson ratio (the element's symmetries; no entry is structurally
+// zero).  Checked against Ke when an operator is created.
+constexpr int kKeClasses = 14;
+__host__ __device__ constexpr int ke_class(int i) {
+    constexpr signed char t[576] = {
+         0,  1,  1,  2,  3,  3,  4,  5,  6,  7,  8,  9,  7,  9,  8,  4,  6,  5, 10, 11, 11, 12, 13, 13,
+         1,  0,  1,  8,  7,  9,  5,  4,  6,  3,  2,  3,  9,  7,  8, 13, 12, 13, 11, 10, 11,  6,  4,  5,
+         1,  1,  0,  8,  9,  7, 13, 13, 12,  9,  8,  7,  3,  3,  2,  5,  6,  4, 11, 11, 10,  6,  5,  4,
+         2,  8,  8,  0,  5,  5,  7,  3, 11,  4,  1, 13,  4, 13,  1,  7, 11,  3, 12,  6,  6, 10,  9,  9,
+         3,  7,  9,  5,  0,  1,  8,  2,  3,  1,  4,  6,  6, 12, 13, 11,  7,  8, 13,  4,  5,  9, 10, 11,
+         3,  9,  7,  5,  1,  0, 11,  8,  7,  6, 13, 12,  1,  6,  4,  8,  3,  2, 13,  5,  4,  9, 11, 10,
+         4,  5, 13,  7,  8, 11,  0,  1,  5,  2,  3,  8, 10, 11,  9, 12, 13,  6,  7,  9,  3,  4,  6,  1,
+         5,  4, 13,  3,  2,  8,  1,  0,  5,  8,  7, 11, 11, 10,  9,  6,  4,  1,  9,  7,  3, 13, 12,  6,
+         6,  6, 12, 11,  3,  7,  5,  5,  0,  3, 11,  7,  9,  9, 10, 13,  1,  4,  8,  8,  2,  1, 13,  4,
+         7,  3,  9,  4,  1,  6,  2,  8,  3,  0,  5,  1, 12,  6, 13, 10,  9, 11,  4, 13,  5,  7, 11,  8,
+         8,  2,  8,  1,  4, 13,  3,  7, 11,  5,  0,  5, 13,  4,  1,  9, 10,  9,  6, 12,  6, 11,  7,  3,
+         9,  3,  7, 13,  6, 12,  8, 11,  7,  1,  5,  0,  6,  1,  4, 11,  9, 10,  5, 13,  4,  3,  8,  2,
+         7,  9,  3,  4,  6,  1, 10, 11,  9, 12, 13,  6,  0,  1,  5,  2,  3,  8,  4,  5, 13,  7,  8, 11,
+         9,  7,  3, 13, 12,  6, 11, 10,  9,  6,  4,  1,  1,  0,  5,  8,  7, 11,  5,  4, 13,  3,  2,  8,
+         8,  8,  2,  1, 13,  4,  9,  9, 10, 13,  1,  4,  5,  5,  0,  3, 11,  7,  6,  6, 12, 11,  3,  7,
+         4, 13,  5,  7, 11,  8, 12,  6, 13, 10,  9, 11,  2,  8,  3,  0,  5,  1,  7,  3,  9,  4,  1,  6,
+         6, 12,  6, 11,  7,  3, 13,  4,  1,  9, 10,  9,  3,  7, 11,  5,  0,  5,  8,  2,  8,  1,  4, 13,
+         5, 13,  4,  3,  8,  2,  6,  1,  4, 11,  9, 10,  8, 11,  7,  1,  5,  0,  9,  3,  7, 13,  6, 12,
+        10, 11, 11, 12, 13, 13,  7,  9,  8,  4,  6,  5,  4,  5,  6,  7,  8,  9,  0,  1,  1,  2,  3,  3,
+        11, 10, 11,  6,  4,  5,  9,  7,  8, 13, 12, 13,  5,  4,  6,  3,  2,  3,  1,  0,  1,  8,  7,  9,
+        11, 11, 10,  6,  5,  4,  3,  3,  2,  5,  6,  4, 13, 13, 12,  9,  8,  7,  1,  1,  0,  8,  9,  7,
+        12,  6,  6, 10,  9,  9,  4, 13,  1,  7, 11,  3,  7,  3, 11,  4,  1, 13,  2,  8,  8,  0,  5,  5,
+        13,  4,  5,  9, 10, 11,  6, 12, 13, 11,  7,  8,  8,  2,  3,  1,  4,  6,  3,  7,  9,  5,  0,  1,
+        13,  5,  4,  9, 11, 10,  1,  6,  4,  8,  3,  2, 11,  8,  7,  6, 13, 12,  3,  9,  7,  5,  1,  0};
+    return t[i];
+}
+
+template <class AT>
+struct KeCoef {
+    AT cls[kKeClasses];
+};
+
+struct HexOpGeom {
+    int32_t ne0, ne1, ne2;     // elements per axis
+    int32_t lx, ly, lz;        // free-node box: lx = ne0 (x index 1..ne0), ly = ne1 + 1, lz = ne2 + 1
+    int32_t ntx, nty, zc, ntile;
+};
+
+constexpr int kHexEX = kGridTX + 1, kHexEY = kGridTY + 1;   // element tile per layer (33 x 9)
+constexpr int kHexLayer = kHexEX * kHexEY;                  // 297 factors
+constexpr int kHexLayerLoads = (kHexLayer + 255) / 256;     // per thread (2)
+
+// Contributions of one element layer to the two accumulated nodes of the thread's column that
+// its elements contain.  L = 0: the layer above plane p (elements between p and p + 1; their
+// corners in plane p are lower corners), which holds node p + 1 as an upper corner (UP, into
+// au) and node p as a lower corner (DN, into ad).  L = 1: the layer below (p - 1 .. p; corners
+// in plane p are upper corners), holding node p as an upper corner and node p - 1 as a lower
+// one.  Each staged x value is scaled by the element factor once and applied to both nodes.
+template <class AT, bool FUSED, int L, bool UP, bool DN>
+__device__ __forceinline__ void hex_layer_terms(const AT (&xv)[27], const AT *__restrict__ el, int tx, int ty,
+                                                const KeCoef<AT> &kc, AT (&au)[3], AT (&ad)[3]) {
+    constexpr int vtk[8] = {0, 1, 3, 2, 4, 5, 7, 6};
+    constexpr int bz = L == 0 ? 0 : 1;
+#pragma unroll
+    for (int eyo = 0; eyo < 2; ++eyo)
+#pragma unroll
+        for (int exo = 0; exo < 2; ++exo) {
+            const AT f = el[(tx + exo) + kHexEX * (ty + eyo)];
+            const int a_up = vtk[(1 - exo) + 2 * (1 - eyo) + 4];   // the node as the element's upper corner
+            const int a_dn = vtk[(1 - exo) + 2 * (1 - eyo)];       // and as its lower corner
+#pragma unroll
+            for (int by = 0; by < 2; ++by)
+#pragma unroll
+                for (int bx = 0; bx < 2; ++bx) {
+                    const int b = vtk[bx + 2 * by + 4 * bz];
+                    const int dxs = exo + bx - 1, dys = eyo + by - 1;   // source node offset in the plane
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        const AT w = f * xv[9 * (dys + 1) + 3 * (dxs + 1) + c];
+#pragma unroll
+                        for (int d = 0; d < 3; ++d) {
+                            if (UP) au[d] = madd_op<AT, FUSED>(au[d], kc.cls[ke_class(24 * (3 * a_up + d) + 3 * b + c)], w);
+                            if (DN) ad[d] = madd_op<AT, FUSED>(ad[d], kc.cls[ke_class(24 * (3 * a_dn + d) + 3 * b + c)], w);
+                        }
+                    }
+                }
+        }
+}
+
+// One plane step: layer p feeds nodes p + 1 (DI) and p (DM), layer p - 1 nodes p (DM) and p - 1 (DF).
+template <class AT, bool FUSED, bool DI, bool DM, bool DF>
+__device__ __forceinline__ void hex_plane_step(const AT (&xv)[27], const AT *lay_up, const AT *lay_dn, int tx, int ty,
+                                               const KeCoef<AT> &kc, AT (&a0)[3], AT (&a1)[3], AT (&a2)[3]) {
+    if constexpr (DI || DM) hex_layer_terms<AT, FUSED, 0, DI, DM>(xv, lay_up, tx, ty, kc, a2, a1);
+    if constexpr (DM || DF) hex_layer_terms<AT, FUSED, 1, DM, DF>(xv, lay_dn, tx, ty, kc, a1, a0);
+}
+
+template <class AT, class Gather, class Op>
+__global__ void __launch_bounds__(256, sizeof(AT) == 8 ? 1 : 3)
+    k_hex_elem(HexOpGeom G, KeCoef<AT> kc, const AT *__restrict__ ef, Gather g, Op op, const int *__restrict__ done,
+               double *partials, unsigned *ticket) {
+    if (done && *(volatile const int *)done) return;
+    extern __shared__ uint4 hex_smem[];
+    constexpr bool FU = op_fused<Op>::value;
+    AT *plane = reinterpret_cast<AT *>(hex_smem);    // 2 x kGridPlane node values
+    AT *layer = plane + 2 * kGridPlane;              // 3 x kHexLayer element factors
+    double red[Op::NRED > 0 ? Op::NRED : 1];
+#pragma unroll
+    for (int i = 0; i < (Op::NRED > 0 ? Op::NRED : 1); ++i) red[i] = 0.0;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    int sx[kGridLoads], sy[kGridLoads], sc[kGridLoads];
+#pragma unroll
+    for (int j = 0; j < kGridLoads; ++j) {
+        const int k = threadIdx.x + 256 * j;
+        const int row = k / (kGridPX * 3), col = k - row * (kGridPX * 3);
+        sx[j] = col / 3 - 1;
+        sc[j] = col - 3 * (col / 3);
+        sy[j] = k < kGridPlane ? row - 1 : -1000000;
+    }
+    int ex_[kHexLayerLoads], ey_[kHexLayerLoads];
+#pragma unroll
+    for (int j = 0; j < kHexLayerLoads; ++j) {
+        const int k = threadIdx.x + 256 * j;
+        ey_[j] = k < kHexLayer ? k / kHexEX : -1000000;
+        ex_[j] = k - (k / kHexEX) * kHexEX;
+    }
+    const int64_t lxy = (int64_t)G.lx * G.ly;
+    for (int t = blockIdx.x; t < G.ntile; t += gridDim.x) {
+        const int txi = t % G.ntx, tyi = (t / G.ntx) % G.nty, tzi = t / (G.ntx * G.nty);
+        const int x0 = txi * kGridTX, y0 = tyi * kGridTY, z0 = tzi * G.zc, z1 = min(G.lz, z0 + G.zc);
+        const int ix = x0 + tx, iy = y0 + ty;
+        const bool inxy = ix < G.lx && iy < G.ly;
+        const int64_t col_xy = (int64_t)ix + (int64_t)G.lx * iy;
+        AT pre[kGridLoads], pe[kHexLayerLoads];
+        auto load = [&](int z) {   // node plane z and element layer z (elements between planes z and z + 1)
+#pragma unroll
+            for (int j = 0; j < kGridLoads; ++j) {
+                const int xn = x0 + sx[j], yn = y0 + sy[j];
+                AT v = AT(0);
+                if (xn >= 0 && xn < G.lx && yn >= 0 && yn < G.ly && z >= 0 && z < G.lz)
+                    v = g((uint32_t)(3 * ((int64_t)xn + (int64_t)G.lx * yn + lxy * z) + sc[j]));
+                pre[j] = v;
+            }
+#pragma unroll
+            for (int j = 0; j < kHexLayerLoads; ++j) {
+                const int ex = x0 + ex_[j], ey = y0 - 1 + ey_[j];   // element (ex, ey, z): nodes x ex..ex+1 (x index 0 clamped)
+                AT v = AT(0);
+                if (ex < G.ne0 && ey >= 0 && ey < G.ne1 && z >= 0 && z < G.ne2)
+                    v = __ldg(ef + (ex + (int64_t)G.ne0 * (ey + (int64_t)G.ne1 * z)));
+                pe[j] = v;
+            }
+        };
+        load(z0 - 1);
+        AT a0[3], a1[3], a2[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) a0[d] = a1[d] = a2[d] = AT(0);
+        for (int p = z0 - 1; p <= z1; ++p) {
+            AT *pl = plane + (p & 1) * kGridPlane;
+            AT *lay_up = layer + ((p + 3) % 3) * kHexLayer;       // layer p: elements between planes p and p + 1
+            const AT *lay_dn = layer + ((p + 2) % 3) * kHexLayer; // layer p - 1
+#pragma unroll
+            for (int j = 0; j < kGridLoads; ++j)
+                if (sy[j] > -2) pl[threadIdx.x + 256 * j] = pre[j];
+#pragma unroll
+            for (int j = 0; j < kHexLayerLoads; ++j)
+                if (ey_[j] >= 0) lay_up[threadIdx.x + 256 * j] = pe[j];
+            __syncthreads();
+            if (p + 1 <= z1) load(p + 1);
+            const bool di = p + 1 >= z0 && p + 1 < z1, dm = p >= z0 && p < z1, df = p - 1 >= z0 && p - 1 < z1;
+            if (di) {
+                const int32_t r = (int32_t)(3 * (col_xy + lxy * (p + 1)));
+#pragma unroll
+                for (int d = 0; d < 3; ++d) a2[d] = inxy ? op.init(r + d) : AT(0);
+            }
+            AT xv[27];
+#pragma unroll
+            for (int dy = 0; dy < 3; ++dy)
+#pragma unroll
+                for (int dx = 0; dx < 3; ++dx)
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) xv[9 * dy + 3 * dx + c] = pl[((ty + dy) * kGridPX + tx + dx) * 3 + c];
+            if (di && dm && df) hex_plane_step<AT, FU, true, true, true>(xv, lay_up, lay_dn, tx, ty, kc, a0, a1, a2);
+            else if (di && dm) hex_plane_step<AT, FU, true, true, false>(xv, lay_up, lay_dn, tx, ty, kc, a0, a1, a2);
+            else if (dm && df) hex_plane_step<AT, FU, false, true, true>(xv, lay_up, lay_dn, tx, ty, kc, a0, a1, a2);
+            else if (di) hex_plane_step<AT, FU, true, false, false>(xv, lay_up, lay_dn, tx, ty, kc, a0, a1, a2);
+            else if (dm) hex_plane_step<AT, FU, false, true, false>(xv, lay_up, lay_dn, tx, ty, kc, a0, a1, a2);
+            else if (df) hex_plane_step<AT, FU, false, false, true>(xv, lay_up, lay_dn, tx, ty, kc, a0, a1, a2);
+            if (df) {
+                if (inxy) {
+                    const int32_t r = (int32_t)(3 * (col_xy + lxy * (p - 1)));
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) op.row(r + d, a0[d], red);
+                }
+            }
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                a0[d] = a1[d];
+                a1[d] = a2[d];
+            }
+        }
+        __syncthreads();   // the next tile restarts the buffer rotation
+    }
+    if constexpr (Op::NRED > 0) {
+        double tot[Op::NRED];
+        if (grid_reduce<Op::NRED, Op::MAXMASK>(red, partials, ticket, tot)) op.finish(tot);
+    }
+}
+
+template <class AT, class Gather, class Op>
+void launch_hex_elem(const LaunchEnv &e, const dv_matrix *m, Gather g, Op op) {
+    auto kern = k_hex_elem<AT, Gather, Op>;
+    const size_t smem = sizeof(AT) * (2 * (size_t)kGridPlane + 3 * (size_t)kHexLayer);
+    static SmemLimit limit;   // per instantiation and device
+    limit.raise(kern, smem, e.ctx->device);
+    static OccupancyCache occupancy;   // per instantiation
+    const int occ = occupancy.get(kern, 256, smem, e.ctx->device);
+    KeCoef<AT> kc;
+    for (int c = 0; c < kKeClasses; ++c) kc.cls[c] = (AT)m->hex_cls[c];
+    HexOpGeom G;
+    G.ne0 = m->hex_ne[0];
+    G.ne1 = m->hex_ne[1];
+    G.ne2 = m->hex_ne[2];
+    G.lx = G.ne0;
+    G.ly = G.ne1 + 1;
+    G.lz = G.ne2 + 1;
+    G.ntx = (G.lx + kGridTX - 1) / kGridTX;
+    G.nty = (G.ly + kGridTY - 1) / kGridTY;
+    const int64_t wave = (int64_t)e.ctx->num_sms * occ, plane_tiles = (int64_t)G.ntx * G.nty;
+    int zc = 16;
+    while (zc > 4 && plane_tiles * ((G.lz + zc - 1) / zc) < 4 * wave) zc /= 2;
+    G.zc = zc;
+    G.ntile = (int32_t)(plane_tiles * ((G.lz + zc - 1) / zc));
+    const int blocks = (int)std::min<int64_t>(G.ntile, e.max_blocks);
+    kern<<<blocks, 256, smem, e.stream>>>(G, kc, static_cast<const AT *>(m->hex_factor.p), g, op, e.done, e.partials,
+                                          e.ticket);
+    DV_CUDA(cudaGetLastError());
+    e.ctx->count();
+}
+
 // Runs op over every row of m with the accumulator type AT (= value precision).
 template <class AT, class Gather, class Op>
 void launch_rows(const LaunchEnv &e, const dv_matrix *m, Gather g, Op op) {
+    if (m->format == DV_FORMAT_HEX) {
+        launch_hex_elem<AT>(e, m, g, op);
+        return;
+    }
     if (m->format == DV_FORMAT_DUVI && m->duvi_variant == 3) {
         launch_duvi_grid<AT>(e, m, g, op);
         return;

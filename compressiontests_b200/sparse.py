@@ -89,6 +89,22 @@ class SparseMatrix:
         self.precision = precision
 
     @classmethod
+    def hex_operator(cls, ctx, ne, elem_E=None, scale=1.0, E=1.0, nu=0.3, precision="f64"):
+        """Matrix-free structured hexahedral stiffness (format "hex"): the operator of
+        hex_stiffness(ne, elem_E, scale, E, nu) applied element by element, nothing stored
+        but one factor per element."""
+        self = cls.__new__(cls)
+        nea = np.ascontiguousarray(ne, np.int32)
+        e = None if elem_E is None else np.ascontiguousarray(elem_E, np.float64)
+        h = C.c_void_p()
+        N.check(N.lib().dv_matrix_create_hex(ctx.h, N.ptr(nea), N.ptr(e), scale, E, nu,
+                                             {"f64": N.F64, "f32": N.F32}[precision], C.byref(h)))
+        n = 3 * int(nea[0]) * (int(nea[1]) + 1) * (int(nea[2]) + 1)
+        self.ctx, self.h, self.shape, self.format, self.precision = ctx, h, (n, n), "hex", precision
+        ctx.register(self)
+        return self
+
+    @classmethod
     def from_duvi_soa(cls, ctx, n_rows, n_cols, arrays, precision="f64"):
         """Upload pre-encoded DuVi arrays (row_to_col, row_to_dist, col_idx, dist, vidx, values, vi_bits)."""
         self = cls.__new__(cls)

@@ -52,7 +52,7 @@ enum {
     DV_ERR_SINGULAR = -8
 };
 
-enum { DV_FORMAT_CSR = 0, DV_FORMAT_DUVI = 1 };
+enum { DV_FORMAT_CSR = 0, DV_FORMAT_DUVI = 1, DV_FORMAT_HEX = 2 };
 enum { DV_F64 = 0, DV_F32 = 1, DV_MIXED = 2 };
 enum { DV_SMOOTHER_JACOBI = 0, DV_SMOOTHER_GS_LEX = 1, DV_SMOOTHER_GS_COLOR = 2 };
 enum { DV_TOL_ABS_MAX = 0, DV_TOL_REL_L2 = 1 };
@@ -171,6 +171,17 @@ DV_API int dv_matrix_create_duvi_soa(dv_context *ctx, int32_t n_rows, int32_t n_
                                      int64_t nnz, const void *value_indices, int32_t value_index_bits,
                                      const double *values, int64_t nuniq, int32_t precision,
                                      dv_matrix **out);
+/* Matrix-free operator of the structured hexahedral stiffness (format DV_FORMAT_HEX): the
+ * same operator as dv_hex_assemble(ne, elem_E, scale, E, nu), applied element by element
+ * from one factor scale * E_e per element (elem_E NULL: uniform) and the 24 x 24 element
+ * stiffness, without storing the matrix.  A product reads the factors, x and y only.
+ * Usable wherever an operator is applied (dv_spmv, dv_spmv_device, dv_residual_device, the
+ * diagonal for Jacobi weights); not for dv_spmm_device or DuVi export (DV_ERR_UNSUPPORTED).
+ * FP64 products equal the assembled matrix's to rounding (another summation order), not bit
+ * for bit.  The reference assembles the matrix (FemCantileverBase.cs:87-104); it has no
+ * matrix-free counterpart. */
+DV_API int dv_matrix_create_hex(dv_context *ctx, const int32_t *ne, const double *elem_E, double scale, double E,
+                                double nu, int32_t precision, dv_matrix **out);
 DV_API int dv_matrix_get_info(const dv_matrix *m, dv_matrix_info *info);
 /* Copy the DuVi arrays back (value indices widened to uint32). */
 DV_API int dv_matrix_export_duvi(const dv_matrix *m, uint32_t *row_to_col, uint32_t *row_to_dist,
@@ -343,7 +354,10 @@ DV_API int dv_batch_destroy(dv_batch *b);
  * path; the elements, dof numbering and load follow FemCantilever3D
  * (FemCantileverBase.cs:87-158).  create builds K(rho) and a Galerkin
  * hierarchy (vertex factor-2 coarsening, trilinear P) down to at most
- * max_coarse_dofs dofs, then the MG-PCG solver of cfg. */
+ * max_coarse_dofs dofs, then the MG-PCG solver of cfg.  With the Jacobi smoother
+ * the finest K(rho) is applied matrix-free (as dv_matrix_create_hex) in the outer
+ * loop and the finest V-cycle level; the environment variable DV_MATRIX_FREE=0
+ * keeps the assembled operator there. */
 DV_API int dv_adjoint_create(dv_context *ctx, const int32_t *ne, const double *rho, double penal, double E0, double nu,
                              int32_t max_coarse_dofs, const dv_mgpcg_config *cfg, dv_adjoint **out);
 DV_API int dv_adjoint_info(const dv_adjoint *a, int32_t *n_dofs, int64_t *n_elements);

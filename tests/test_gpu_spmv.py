@@ -410,3 +410,32 @@ def test_spmm_transfers_bit_exact(ctx, native, oracle, rng, k):
         ref = oracle.DuVi(oracle.Csr.from_scipy(M0))
         for j in (0, k // 2, k - 1):
             np.testing.assert_array_equal(Y[:, j], ref.spmv(X[:, j]))
+
+
+@pytest.mark.parametrize("ne", [(1, 1, 1), (8, 8, 8), (40, 21, 13), (33, 9, 20)])
+@pytest.mark.parametrize("moduli", ["uniform", "log_uniform"])
+def test_matrix_free_hex_operator(ctx, native, rng, ne, moduli):
+    # The element kernel (format "hex") applies K = sum_e (scale E_e) Ke without storing it:
+    # FP64 products within 1e-12 relative per row of the assembled matrix (another summation
+    # order), FP32 within 1e-5; y += A x and r = b - A x through the same kernel.
+    import torch
+    E = None if moduli == "uniform" else 10.0 ** rng.uniform(-2.0, 0.0, int(np.prod(ne)))
+    A = native.hex_stiffness(ne, E, scale=2.0)
+    x = rng.standard_normal(A.shape[1])
+    ref = A @ x
+    H = native.SparseMatrix.hex_operator(ctx, ne, E, scale=2.0)
+    assert H.info()["kernel_variant"] == 400 and H.info()["format"] == 2
+    assert rowwise_rel(H.Multiply(x), ref, A, x) <= REL64
+    y0 = rng.standard_normal(A.shape[0])
+    assert rowwise_rel(H.Multiply(x, y0.copy(), clear=False), y0 + ref, A, x) <= REL64
+    b = rng.standard_normal(A.shape[0])
+    db, dx = torch.from_numpy(b).cuda(), torch.from_numpy(x).cuda()
+    dr = torch.empty_like(db)
+    torch.cuda.synchronize()
+    H.residual_device(db.data_ptr(), dx.data_ptr(), dr.data_ptr(), "f64")
+    ctx.synchronize()
+    assert rowwise_rel(dr.cpu().numpy(), b - ref, A, x) <= REL64
+    F = native.SparseMatrix.hex_operator(ctx, ne, E, scale=2.0, precision="f32")
+    assert rowwise_rel(_device_product(ctx, F, x, np.float32).astype(np.float64), ref, A, x) <= REL32
+    with pytest.raises(native.DuviError):
+        H.multiply_many_device(2, dx.data_ptr(), dr.data_ptr(), "f64")
