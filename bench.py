@@ -83,8 +83,8 @@ def parse():
     p.add_argument("--batch-k", type=int, default=64, help="load cases of the multi-load-case section")
     p.add_argument("--batch-meshes", type=int, default=32, help="meshes of the batched-mesh section")
     p.add_argument("--spmv-only", default=None, metavar="FMT_PREC",
-                   help="only time the SpMV of the finest operator (duvi_f32, duvi_f64, csr_f32, csr_f64): "
-                        "the small case used for ncu captures")
+                   help="only time the SpMV of the finest operator (duvi_f32, duvi_f64, csr_f32, csr_f64, or the "
+                        "matrix-free hex_f32, hex_f64 with E = 10^U(-2,0)): the case used for ncu captures")
     return p.parse_args()
 
 
@@ -822,13 +822,16 @@ def run_spmv_only(args):
     import compressiontests_b200 as cb
     fmt, prec = args.spmv_only.split("_")
     n = args.size
-    A0 = cb.hex_stiffness((n, n, n))
     ctx = cb.CudaContext(0)
-    M = cb.SparseMatrix(ctx, A0, fmt, prec)
+    if fmt == "hex":   # matrix-free operator, per-element E = 10^U(-2,0)
+        E = 10.0 ** np.random.default_rng(20261203).uniform(-2.0, 0.0, n ** 3)
+        M = cb.SparseMatrix.hex_operator(ctx, (n, n, n), E, precision=prec)
+    else:
+        M = cb.SparseMatrix(ctx, cb.hex_stiffness((n, n, n)), fmt, prec)
     info = M.info()
     dt = torch.float32 if prec == "f32" else torch.float64
     g = torch.Generator(device="cuda").manual_seed(20261203)
-    x = torch.randn(A0.shape[0], dtype=dt, device="cuda", generator=g)
+    x = torch.randn(M.shape[0], dtype=dt, device="cuda", generator=g)
     y = torch.zeros_like(x)
     torch.cuda.synchronize()
     fn = lambda: M.multiply_device(x.data_ptr(), y.data_ptr(), prec)
@@ -836,7 +839,7 @@ def run_spmv_only(args):
         fn()
     ctx.synchronize()
     ms = time_events(torch.cuda.ExternalStream(ctx.stream), fn, args.steps)
-    alg = info["device_bytes"] + 2 * (4 if prec == "f32" else 8) * A0.shape[0]
+    alg = info["device_bytes"] + 2 * (4 if prec == "f32" else 8) * M.shape[0]
     print(json.dumps({"spmv": args.spmv_only, "size": n, "ms": ms, "algorithmic_bytes": int(alg),
                       "GBps": alg / ms / 1e6, "launch_shape": info["kernel_variant"]}), flush=True)
     M.release()

@@ -76,6 +76,53 @@ __global__ void k_gs_duvi(DuviArgs A, const T *__restrict__ b, T *x, const int32
     }
 }
 
+// Multicolor node-block update on the node-pattern layout: one thread per node of the color,
+// its pattern's records from shared memory.  One pass over the records gathers every column
+// of another node once and subtracts it from all three rows (fused multiply-adds); the node's
+// own 3 x 3 block is then solved row by row in order, each row using the rows of the node
+// already updated in this sweep and the old values of the later ones (the block Gauss-Seidel
+// step of the raw kernels above, with the neighbour sum taken first).
+template <class T>
+__global__ void __launch_bounds__(256) k_gs_pattern(const uint16_t *__restrict__ pid, const uint32_t *__restrict__ pstart,
+                                                    const PatRec<T> *__restrict__ grec, int32_t npat, int32_t nrec,
+                                                    const T *__restrict__ b, T *x, const int32_t *__restrict__ rows,
+                                                    int32_t count, const int *__restrict__ done) {
+    if (done && *(volatile const int *)done) return;
+    extern __shared__ uint4 gs_smem[];
+    const PatRec<T> *rec = reinterpret_cast<const PatRec<T> *>(gs_smem);
+    const uint32_t *st = reinterpret_cast<const uint32_t *>(rec + nrec);
+    stage_patterns<T>(gs_smem, grec, pstart, npat, nrec);
+    __syncthreads();
+    for (int32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < count; t += gridDim.x * blockDim.x) {
+        const int32_t r0 = rows[t];
+        const uint32_t p = __ldg(pid + r0 / 3);
+        const uint32_t kb = st[p], ke = st[p + 1];
+        T s0 = b[r0], s1 = b[r0 + 1], s2 = b[r0 + 2];
+        T a[3][3] = {{T(0), T(0), T(0)}, {T(0), T(0), T(0)}, {T(0), T(0), T(0)}};
+#pragma unroll 4
+        for (uint32_t k = kb; k < ke; ++k) {
+            const PatRec<T> q = rec[k];
+            if (q.off >= 0 && q.off < 3) {   // the node's own block, column q.off
+                if (q.off == 0) { a[0][0] = q.v[0]; a[1][0] = q.v[1]; a[2][0] = q.v[2]; }
+                else if (q.off == 1) { a[0][1] = q.v[0]; a[1][1] = q.v[1]; a[2][1] = q.v[2]; }
+                else { a[0][2] = q.v[0]; a[1][2] = q.v[1]; a[2][2] = q.v[2]; }
+                continue;
+            }
+            const T xv = __ldg(x + (r0 + q.off));
+            s0 = fma(-q.v[0], xv, s0);
+            s1 = fma(-q.v[1], xv, s1);
+            s2 = fma(-q.v[2], xv, s2);
+        }
+        const T x1o = x[r0 + 1], x2o = x[r0 + 2];
+        const T x0 = (s0 - a[0][1] * x1o - a[0][2] * x2o) / a[0][0];
+        const T x1 = (s1 - a[1][0] * x0 - a[1][2] * x2o) / a[1][1];
+        const T x2 = (s2 - a[2][0] * x0 - a[2][1] * x1) / a[2][2];
+        x[r0] = x0;
+        x[r0 + 1] = x1;
+        x[r0 + 2] = x2;
+    }
+}
+
 inline DuviArgs gs_duvi_args(const dv_matrix *m) {
     DuviArgs a;
     a.row_to_col = m->row_to_col.as<uint32_t>();
@@ -129,7 +176,16 @@ void gs_sweep(const LaunchEnv &e, const dv_matrix *A, const GsOrder &o, const T 
         const int32_t cnt = o.off[q + 1] - o.off[q];
         const int32_t *rows = o.rows.as<int32_t>() + o.off[q];
         const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((cnt + kThreads - 1) / kThreads, ctx->num_sms * 8));
-        if (A->format == DV_FORMAT_CSR) {
+        if (o.bs == 3 && A->format == DV_FORMAT_DUVI && A->pat_ok && A->lanes_group == 3 && !A->pat_based &&
+            sizeof(T) == (A->precision == DV_F64 ? 8 : 4)) {
+            // node blocks of one color on the pattern layout
+            const size_t smem = sizeof(PatRec<T>) * (size_t)A->pat_entries + 4 * ((size_t)A->pat_count + 1);
+            static SmemLimit limit;   // per instantiation and device
+            limit.raise(k_gs_pattern<T>, smem, ctx->device);
+            k_gs_pattern<T><<<grid, kThreads, smem, e.stream>>>(A->pat_id.as<uint16_t>(), A->pat_start.as<uint32_t>(),
+                                                               static_cast<const PatRec<T> *>(A->pat_rec.p),
+                                                               A->pat_count, A->pat_entries, b, x, rows, cnt, e.done);
+        } else if (A->format == DV_FORMAT_CSR) {
             k_gs_csr<T><<<grid, kThreads, 0, e.stream>>>(A->rowptr.as<int32_t>(), A->col.as<int32_t>(),
                                                          static_cast<const T *>(A->val.p), b, x, rows, cnt, o.bs, e.done);
         } else if (A->vi_bits == 8) {
