@@ -10,6 +10,8 @@
 
 #include <cstddef>
 #include <mutex>
+#include <type_traits>
+#include <utility>
 
 #include "dv_internal.cuh"
 
@@ -199,13 +201,28 @@ __device__ __forceinline__ AT madd_op(AT acc, AT a, AT b) {
 }
 
 // ---------------------------------------------------------------------------
-// epilogues (row operators).  Each has NRED reduction slots and MAXMASK.
+// epilogues (row operators).  Each has NRED reduction slots and MAXMASK.  An
+// epilogue may define touch(r): a prefetch of what row() will read at rows r .. r+2,
+// issued by the streaming kernels one step before they finish those rows.
 // ---------------------------------------------------------------------------
 struct NoRed {
     static constexpr int NRED = 0;
     static constexpr unsigned MAXMASK = 0;
     __device__ void finish(const double *) const {}
 };
+
+template <class T>
+__device__ __forceinline__ void prefetch_l1(const T *p) {
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
+template <class Op, class = void>
+struct op_touch : std::false_type {};
+template <class Op>
+struct op_touch<Op, std::void_t<decltype(std::declval<const Op &>().touch(0))>> : std::true_type {};
+template <class Op>
+__device__ __forceinline__ void touch_rows(const Op &op, int32_t r) {
+    if constexpr (op_touch<Op>::value) op.touch(r);
+}
 
 // y = A x (clear) or y += A x, accumulating onto the old y in entry order.
 template <class YT, class AT>
@@ -214,6 +231,7 @@ struct OpSpmv : NoRed {
     int clear;
     __device__ __forceinline__ AT init(int32_t r) const { return clear ? AT(0) : (AT)y[r]; }
     __device__ __forceinline__ void row(int32_t r, AT s, double *) const { y[r] = (YT)s; }
+    __device__ __forceinline__ void touch(int32_t) const {}
 };
 
 // r = b - A x
@@ -223,6 +241,7 @@ struct OpResid : NoRed {
     T *__restrict__ r;
     __device__ __forceinline__ T init(int32_t) const { return T(0); }
     __device__ __forceinline__ void row(int32_t i, T s, double *) const { r[i] = b[i] - s; }
+    __device__ __forceinline__ void touch(int32_t i) const { prefetch_l1(b + i); }
 };
 
 // y = x + w .* (b - A x)  (jacobi_iteration, CsrGeometricMultigrid.cl:176-194)
@@ -234,6 +253,11 @@ struct OpJacobi : NoRed {
     T *__restrict__ y;
     __device__ __forceinline__ T init(int32_t) const { return T(0); }
     __device__ __forceinline__ void row(int32_t i, T s, double *) const { y[i] = x[i] + w[i] * (b[i] - s); }
+    __device__ __forceinline__ void touch(int32_t i) const {
+        prefetch_l1(x + i);
+        prefetch_l1(w + i);
+        prefetch_l1(b + i);
+    }
 };
 // Second sweep from a zero guess: x1 = w .* b, y = x1 + w .* (b - A x1).
 template <class T>
@@ -245,6 +269,10 @@ struct OpJacobiFromZero : NoRed {
     __device__ __forceinline__ void row(int32_t i, T s, double *) const {
         T wi = w[i], bi = b[i];
         y[i] = wi * bi + wi * (bi - s);
+    }
+    __device__ __forceinline__ void touch(int32_t i) const {
+        prefetch_l1(w + i);
+        prefetch_l1(b + i);
     }
 };
 
@@ -275,6 +303,13 @@ struct OpJacobiFcgRed {
         y[i] = z;
         red[0] += (double)z * q[i];
         red[1] += (double)z * r[i];
+    }
+    __device__ __forceinline__ void touch(int32_t i) const {
+        prefetch_l1(x + i);
+        prefetch_l1(w + i);
+        prefetch_l1(b + i);
+        prefetch_l1(q + i);
+        prefetch_l1(r + i);
     }
     __device__ void finish(const double *t) const {
         sc->zq = t[0];
@@ -321,6 +356,11 @@ struct OpFcg {
         q[i] = qi;
         p[i] = pi;
         red[0] += pi * qi;
+    }
+    __device__ __forceinline__ void touch(int32_t i) const {
+        prefetch_l1(z + i);
+        prefetch_l1(p + i);
+        prefetch_l1(q + i);
     }
     __device__ void finish(const double *t) const {
         sc->pq = t[0];
@@ -936,18 +976,27 @@ __global__ void __launch_bounds__(256) k_duvi_pattern(const uint16_t *__restrict
 // values then describe the whole stencil.  A matrix is checked against this table when its
 // grid layout is built and uses it only if every equality and zero holds exactly.
 constexpr int kHexClasses = 10;
-__host__ __device__ constexpr int hex_class(int i) {
-    constexpr signed char t[243] = {
-         0,  1,  1,  1,  0,  1,  1,  1,  0,  2, -1, -1, -1,  3,  4, -1,  4,  3,  0,  5,  5,  5,  0,  1,  5,  1,  0,
-         3, -1,  4, -1,  2, -1,  4, -1,  3,  6, -1, -1, -1,  6, -1, -1, -1,  7,  3, -1,  8, -1,  2, -1,  8, -1,  3,
-         0,  5,  1,  5,  0,  5,  1,  5,  0,  2, -1, -1, -1,  3,  8, -1,  8,  3,  0,  1,  5,  1,  0,  5,  5,  5,  0,
-         3,  4, -1,  4,  3, -1, -1, -1,  2,  6, -1, -1, -1,  7, -1, -1, -1,  6,  3,  8, -1,  8,  3, -1, -1, -1,  2,
-         7, -1, -1, -1,  6, -1, -1, -1,  6,  9, -1, -1, -1,  9, -1, -1, -1,  9,  7, -1, -1, -1,  6, -1, -1, -1,  6,
-         3,  8, -1,  8,  3, -1, -1, -1,  2,  6, -1, -1, -1,  7, -1, -1, -1,  6,  3,  4, -1,  4,  3, -1, -1, -1,  2,
-         0,  1,  5,  1,  0,  5,  5,  5,  0,  2, -1, -1, -1,  3,  8, -1,  8,  3,  0,  5,  1,  5,  0,  5,  1,  5,  0,
-         3, -1,  8, -1,  2, -1,  8, -1,  3,  6, -1, -1, -1,  6, -1, -1, -1,  7,  3, -1,  4, -1,  2, -1,  4, -1,  3,
-         0,  5,  5,  5,  0,  1,  5,  1,  0,  2, -1, -1, -1,  3,  4, -1,  4,  3,  0,  1,  1,  1,  0,  1,  1,  1,  0};
-    return t[i];
+#define DV_HEX_CLASS_TABLE \
+    0,  1,  1,  1,  0,  1,  1,  1,  0,  2, -1, -1, -1,  3,  4, -1,  4,  3,  0,  5,  5,  5,  0,  1,  5,  1,  0, \
+    3, -1,  4, -1,  2, -1,  4, -1,  3,  6, -1, -1, -1,  6, -1, -1, -1,  7,  3, -1,  8, -1,  2, -1,  8, -1,  3, \
+    0,  5,  1,  5,  0,  5,  1,  5,  0,  2, -1, -1, -1,  3,  8, -1,  8,  3,  0,  1,  5,  1,  0,  5,  5,  5,  0, \
+    3,  4, -1,  4,  3, -1, -1, -1,  2,  6, -1, -1, -1,  7, -1, -1, -1,  6,  3,  8, -1,  8,  3, -1, -1, -1,  2, \
+    7, -1, -1, -1,  6, -1, -1, -1,  6,  9, -1, -1, -1,  9, -1, -1, -1,  9,  7, -1, -1, -1,  6, -1, -1, -1,  6, \
+    3,  8, -1,  8,  3, -1, -1, -1,  2,  6, -1, -1, -1,  7, -1, -1, -1,  6,  3,  4, -1,  4,  3, -1, -1, -1,  2, \
+    0,  1,  5,  1,  0,  5,  5,  5,  0,  2, -1, -1, -1,  3,  8, -1,  8,  3,  0,  5,  1,  5,  0,  5,  1,  5,  0, \
+    3, -1,  8, -1,  2, -1,  8, -1,  3,  6, -1, -1, -1,  6, -1, -1, -1,  7,  3, -1,  4, -1,  2, -1,  4, -1,  3, \
+    0,  5,  5,  5,  0,  1,  5,  1,  0,  2, -1, -1, -1,  3,  4, -1,  4,  3,  0,  1,  1,  1,  0,  1,  1,  1,  0
+// The same table in device and host memory: device code indexes the __device__ copy, which
+// the compiler folds to constants after unrolling (a table local to a constexpr function
+// would be rebuilt at every inlined call).
+__device__ constexpr signed char kHexClassDev[243] = {DV_HEX_CLASS_TABLE};
+constexpr signed char kHexClassHost[243] = {DV_HEX_CLASS_TABLE};
+__host__ __device__ __forceinline__ constexpr int hex_class(int i) {
+#ifdef __CUDA_ARCH__
+    return kHexClassDev[i];
+#else
+    return kHexClassHost[i];
+#endif
 }
 
 constexpr int kGridTX = 32, kGridTY = 8;                        // tile of groups per block (one warp per row)
@@ -986,18 +1035,95 @@ __device__ __forceinline__ AT grid_term(AT acc, const GridCoef<AT> &cf, int k, i
     }
 }
 
+// Asynchronous global -> shared copies (cp.async, zero fill when `valid` is false: no global read).
+template <int BYTES>
+__device__ __forceinline__ void cp_async_zfill(void *dst, const void *src, bool valid) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(d), "l"(src), "n"(BYTES), "r"(valid ? BYTES : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// How a gather is staged through shared memory: its source arrays (x; or w and b when the
+// gathered value is w .* b) are copied plane by plane, and a staged value is formed from them
+// (the same arithmetic as the gather, so results do not depend on the path).
+template <class G>
+struct StageSrc;
+template <class XT, class AT>
+struct StageSrc<GatherVec<XT, AT>> {
+    using ST = XT;
+    static constexpr int N = 1;
+    __device__ static const XT *src(const GatherVec<XT, AT> &g, int) { return g.x; }
+    __device__ static AT value(const XT *pl, int i) { return (AT)pl[i]; }
+};
+template <class T>
+struct StageSrc<GatherWB<T>> {
+    using ST = T;
+    static constexpr int N = 2;
+    __device__ static const T *src(const GatherWB<T> &g, int k) { return k == 0 ? g.w : g.b; }
+    __device__ static T value(const T *pl, int i) { return pl[i] * pl[i + kGridPlane]; }
+};
+constexpr int kGridStages = 4;   // staged planes in flight per block (a plane is consumed 3 steps after its copy)
+
+// Staging slots of a thread: plane value k = threadIdx.x + 256 j is node (sx, sy) of the halo tile
+// (offsets from the tile's first node), dof sc; sy = -1000000 past the plane.
+struct StageSlots {
+    int sx[kGridLoads], sy[kGridLoads], sc[kGridLoads];
+    __device__ StageSlots() {
+#pragma unroll
+        for (int j = 0; j < kGridLoads; ++j) {
+            const int k = threadIdx.x + 256 * j;
+            const int row = k / (kGridPX * 3), col = k - row * (kGridPX * 3);
+            sx[j] = col / 3 - 1;
+            sc[j] = col - 3 * (col / 3);
+            sy[j] = k < kGridPlane ? row - 1 : -1000000;
+        }
+    }
+    // per tile: offset of each slot inside a plane of the lx x ly node box (-1: outside the box)
+    __device__ void plane_offsets(int x0, int y0, int lx, int ly, int32_t (&poff)[kGridLoads]) const {
+#pragma unroll
+        for (int j = 0; j < kGridLoads; ++j) {
+            const int xn = x0 + sx[j], yn = y0 + sy[j];
+            poff[j] = (xn >= 0 && xn < lx && yn >= 0 && yn < ly) ? 3 * (xn + lx * yn) + sc[j] : -1;
+        }
+    }
+    // copies plane z (zero outside 0 <= z < lz) of every source of the gather into one ring slot
+    template <class SS, class Gather>
+    __device__ void issue(const Gather &g, typename SS::ST *slot, const int32_t (&poff)[kGridLoads], int z, int lz,
+                          int32_t plane_len) const {
+        const bool zin = z >= 0 && z < lz;
+        const int32_t base = zin ? z * plane_len : 0;
+#pragma unroll
+        for (int k = 0; k < SS::N; ++k) {
+            const typename SS::ST *src = SS::src(g, k);
+#pragma unroll
+            for (int j = 0; j < kGridLoads; ++j)
+                if (sy[j] > -2) {
+                    const bool v = zin && poff[j] >= 0;
+                    cp_async_zfill<sizeof(typename SS::ST)>(slot + k * kGridPlane + threadIdx.x + 256 * j,
+                                                            v ? src + base + poff[j] : src, v);
+                }
+        }
+        cp_async_commit();
+    }
+};
+
 // One staged plane applied to the three accumulated groups: below (DI: group p+1 takes the
 // plane as its dz = -1 neighbours), at (DM: group p, dz = 0) and above (DF: group p-1, dz = +1).
-template <class AT, bool FUSED, bool HEX, bool SKIP0, bool DI, bool DM, bool DF>
-__device__ __forceinline__ void grid_plane_step(const AT *__restrict__ pl, int tx, int ty, const GridCoef<AT> &cf,
-                                                AT (&a0)[3], AT (&a1)[3], AT (&a2)[3]) {
+template <class AT, class SS, bool FUSED, bool HEX, bool SKIP0, bool DI, bool DM, bool DF>
+__device__ __forceinline__ void grid_plane_step(const typename SS::ST *__restrict__ pl, int tx, int ty,
+                                                const GridCoef<AT> &cf, AT (&a0)[3], AT (&a1)[3], AT (&a2)[3]) {
 #pragma unroll
     for (int dy = 0; dy < 3; ++dy)
 #pragma unroll
         for (int dx = 0; dx < 3; ++dx)
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
-                const AT v = pl[((ty + dy) * kGridPX + tx + dx) * 3 + c];
+                const AT v = SS::value(pl, ((ty + dy) * kGridPX + tx + dx) * 3 + c);
                 const int k = 9 * dy + 3 * dx + c;
 #pragma unroll
                 for (int d = 0; d < 3; ++d) {
@@ -1030,55 +1156,46 @@ __global__ void __launch_bounds__(256, sizeof(AT) == 8 ? 2 : 3)
              i += (int64_t)G.bound_blocks * blockDim.x)
             pattern_group<AT, Gather, Op, 3, false, false>((int64_t)__ldg(bnode + i), rec, st, pid, nullptr, g, op, red);
     } else {
-        AT *plane = reinterpret_cast<AT *>(grid_smem);   // two staged planes
+        using SS = StageSrc<Gather>;
+        using ST = typename SS::ST;
+        constexpr int SLOT = SS::N * kGridPlane;
+        ST *ring = reinterpret_cast<ST *>(grid_smem);   // kGridStages slots of SS::N staged planes
         const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-        // this thread's staging slots: the same positions in every plane and tile
-        int sx[kGridLoads], sy[kGridLoads], sc[kGridLoads];
-#pragma unroll
-        for (int j = 0; j < kGridLoads; ++j) {
-            const int k = threadIdx.x + 256 * j;
-            const int row = k / (kGridPX * 3), col = k - row * (kGridPX * 3);
-            sx[j] = col / 3 - 1;
-            sc[j] = col - 3 * (col / 3);
-            sy[j] = k < kGridPlane ? row - 1 : -1000000;   // slots past the plane never load or store
-        }
+        const StageSlots slots;
         const int64_t lxy = (int64_t)G.lx * G.ly;
+        const int32_t plane_len = (int32_t)(3 * lxy);
         const int nblk = (int)gridDim.x - G.bound_blocks;
         for (int t = (int)blockIdx.x - G.bound_blocks; t < G.ntile; t += nblk) {
             const int txi = t % G.ntx, tyi = (t / G.ntx) % G.nty, tzi = t / (G.ntx * G.nty);
             const int x0 = txi * kGridTX, y0 = tyi * kGridTY, z0 = tzi * G.zc, z1 = min(G.lz, z0 + G.zc);
             const int ix = x0 + tx, iy = y0 + ty;
             const bool inxy = ix >= 1 && ix <= G.lx - 2 && iy >= 1 && iy <= G.ly - 2;
-            const int64_t col_xy = (int64_t)ix + (int64_t)G.lx * iy;   // group index in its plane
-            AT pre[kGridLoads];
-            auto load = [&](int z) {
-#pragma unroll
-                for (int j = 0; j < kGridLoads; ++j) {
-                    const int xn = x0 + sx[j], yn = y0 + sy[j];
-                    AT v = AT(0);
-                    if (xn >= 0 && xn < G.lx && yn >= 0 && yn < G.ly && z >= 0 && z < G.lz)
-                        v = g((uint32_t)(3 * ((int64_t)xn + (int64_t)G.lx * yn + lxy * z) + sc[j]));
-                    pre[j] = v;
-                }
-            };
+            const int32_t col_xy = ix + G.lx * iy;   // group index in its plane
+            int32_t poff[kGridLoads];
+            slots.plane_offsets(x0, y0, G.lx, G.ly, poff);
             // a stencil group (off the faces, interior pattern) that this thread finishes
             auto active = [&](int z) {
                 if (!inxy || z < 1 || z > G.lz - 2) return false;
                 return G.all_hot || (int)__ldg(pid + col_xy + lxy * z) == G.hot;
             };
-            load(z0 - 1);
+#pragma unroll
+            for (int q = 0; q < kGridStages - 1; ++q) {
+                if (z0 - 1 + q <= z1) slots.issue<SS>(g, ring + q * SLOT, poff, z0 - 1 + q, G.lz, plane_len);
+                else cp_async_commit();
+            }
             AT a0[3], a1[3], a2[3];
 #pragma unroll
             for (int d = 0; d < 3; ++d) a0[d] = a1[d] = a2[d] = AT(0);
             bool act0 = false, act1 = false, act2 = false;
-            int buf = 0;
-            for (int p = z0 - 1; p <= z1; ++p) {
-                AT *pl = plane + buf * kGridPlane;
-#pragma unroll
-                for (int j = 0; j < kGridLoads; ++j)
-                    if (sy[j] > -2) pl[threadIdx.x + 256 * j] = pre[j];
-                __syncthreads();
-                if (p + 1 <= z1) load(p + 1);
+            for (int p = z0 - 1, k = 0; p <= z1; ++p, ++k) {
+                cp_async_wait<kGridStages - 2>();   // plane p has landed (this thread's copies)
+                __syncthreads();                     // ... and everyone's; the slot of plane p-1 is free
+                if (p + kGridStages - 1 <= z1)
+                    slots.issue<SS>(g, ring + ((k + kGridStages - 1) % kGridStages) * SLOT, poff, p + kGridStages - 1,
+                                    G.lz, plane_len);
+                else
+                    cp_async_commit();
+                const ST *pl = ring + (k % kGridStages) * SLOT;
                 const bool di = p + 1 >= z0 && p + 1 < z1, dm = p >= z0 && p < z1, df = p - 1 >= z0 && p - 1 < z1;
                 if (di) {
                     act2 = active(p + 1);
@@ -1086,12 +1203,13 @@ __global__ void __launch_bounds__(256, sizeof(AT) == 8 ? 2 : 3)
 #pragma unroll
                     for (int d = 0; d < 3; ++d) a2[d] = act2 ? op.init(r + d) : AT(0);
                 }
-                if (di && dm && df) grid_plane_step<AT, FU, HEX, S0, true, true, true>(pl, tx, ty, cf, a0, a1, a2);
-                else if (di && dm) grid_plane_step<AT, FU, HEX, S0, true, true, false>(pl, tx, ty, cf, a0, a1, a2);
-                else if (dm && df) grid_plane_step<AT, FU, HEX, S0, false, true, true>(pl, tx, ty, cf, a0, a1, a2);
-                else if (di) grid_plane_step<AT, FU, HEX, S0, true, false, false>(pl, tx, ty, cf, a0, a1, a2);
-                else if (dm) grid_plane_step<AT, FU, HEX, S0, false, true, false>(pl, tx, ty, cf, a0, a1, a2);
-                else if (df) grid_plane_step<AT, FU, HEX, S0, false, false, true>(pl, tx, ty, cf, a0, a1, a2);
+                if (dm && act1) touch_rows(op, (int32_t)(3 * (col_xy + lxy * p)));   // finished next step
+                if (di && dm && df) grid_plane_step<AT, SS, FU, HEX, S0, true, true, true>(pl, tx, ty, cf, a0, a1, a2);
+                else if (di && dm) grid_plane_step<AT, SS, FU, HEX, S0, true, true, false>(pl, tx, ty, cf, a0, a1, a2);
+                else if (dm && df) grid_plane_step<AT, SS, FU, HEX, S0, false, true, true>(pl, tx, ty, cf, a0, a1, a2);
+                else if (di) grid_plane_step<AT, SS, FU, HEX, S0, true, false, false>(pl, tx, ty, cf, a0, a1, a2);
+                else if (dm) grid_plane_step<AT, SS, FU, HEX, S0, false, true, false>(pl, tx, ty, cf, a0, a1, a2);
+                else if (df) grid_plane_step<AT, SS, FU, HEX, S0, false, false, true>(pl, tx, ty, cf, a0, a1, a2);
                 if (df && act0) {
                     const int32_t r = (int32_t)(3 * (col_xy + lxy * (p - 1)));
 #pragma unroll
@@ -1105,14 +1223,71 @@ __global__ void __launch_bounds__(256, sizeof(AT) == 8 ? 2 : 3)
                 act0 = act1;
                 act1 = act2;
                 act2 = false;
-                buf ^= 1;
             }
+            cp_async_wait<0>();
+            __syncthreads();   // the next tile refills the ring
         }
     }
     if constexpr (Op::NRED > 0) {
         double tot[Op::NRED];
         if (grid_reduce<Op::NRED, Op::MAXMASK>(red, partials, ticket, tot)) op.finish(tot);
     }
+}
+
+// Planes per z run of a streaming tile: the run that minimises (waves of tiles) x (plane steps
+// per tile), with `conc` tiles resident at once; ties go to the longer run.
+inline int stream_run_length(int64_t plane_tiles, int lz, int64_t conc) {
+    int best = 4;
+    int64_t best_cost = INT64_MAX;
+    for (int zc = 4; zc <= 64; zc *= 2) {
+        const int64_t tiles = plane_tiles * ((lz + zc - 1) / zc);
+        const int64_t cost = ((tiles + conc - 1) / conc) * (int64_t)(std::min(zc, lz) + 2);
+        if (cost <= best_cost) {
+            best_cost = cost;
+            best = zc;
+        }
+    }
+    return best;
+}
+
+// Grid-stencil launch: boundary blocks first (they run alongside the tiles), then tile blocks over
+// runs of zc planes.
+template <class AT, class Gather, class Op, bool HEX>
+void launch_duvi_grid_h(const LaunchEnv &e, const dv_matrix *m, Gather g, Op op) {
+    auto kern = k_duvi_grid<AT, Gather, Op, HEX>;
+    using SS = StageSrc<Gather>;
+    const size_t smem = std::max(sizeof(typename SS::ST) * SS::N * kGridStages * (size_t)kGridPlane,
+                                 sizeof(PatRec<AT>) * (size_t)m->pat_entries + 4 * ((size_t)m->pat_count + 1));
+    static SmemLimit limit;   // per instantiation and device
+    limit.raise(kern, smem, e.ctx->device);
+    static OccupancyCache occupancy;   // per instantiation
+    const int occ = occupancy.get(kern, 256, smem, e.ctx->device);
+    GridCoef<AT> cf;
+    for (int k = 0; k < 81; ++k)
+        for (int d = 0; d < 3; ++d) cf.v[k][d] = (AT)m->grid_coef[3 * k + d];
+    for (int c = 0; c < kHexClasses; ++c) cf.cls[c] = HEX ? (AT)m->grid_cls[c] : AT(0);
+    GridGeom G;
+    G.lx = m->grid_lx;
+    G.ly = m->grid_ly;
+    G.lz = m->grid_lz;
+    G.ntx = (G.lx + kGridTX - 1) / kGridTX;
+    G.nty = (G.ly + kGridTY - 1) / kGridTY;
+    G.hot = m->grid_hot;
+    G.all_hot = m->grid_all_hot;
+    G.nbound = m->grid_nb;
+    const int64_t wave = (int64_t)e.ctx->num_sms * occ;
+    G.bound_blocks = G.nbound == 0 ? 0
+                     : (int32_t)std::min<int64_t>((G.nbound + 255) / 256, std::max<int64_t>(1, e.max_blocks / 4));
+    const int64_t plane_tiles = (int64_t)G.ntx * G.nty;
+    G.zc = stream_run_length(plane_tiles, G.lz, std::max<int64_t>(1, wave - G.bound_blocks / 2));
+    G.ntile = (int32_t)(plane_tiles * ((G.lz + G.zc - 1) / G.zc));
+    const int64_t tile_blocks = std::min<int64_t>(G.ntile, std::max<int64_t>(1, e.max_blocks - G.bound_blocks));
+    const int blocks = (int)(G.bound_blocks + tile_blocks);
+    kern<<<blocks, 256, smem, e.stream>>>(G, cf, m->pat_id.as<uint16_t>(), m->pat_start.as<uint32_t>(),
+                                          static_cast<const PatRec<AT> *>(m->pat_rec.p), m->grid_bnode.as<uint32_t>(),
+                                          m->pat_count, m->pat_entries, g, op, e.done, e.partials, e.ticket);
+    DV_CUDA(cudaGetLastError());
+    e.ctx->count();
 }
 
 template <class AT, class Gather, class Op, int G, bool BASED, bool SHIFT>
@@ -1138,46 +1313,6 @@ void launch_duvi_pattern_gbs(const LaunchEnv &e, const dv_matrix *m, Gather g, O
     e.ctx->count();
 }
 
-// Grid-stencil launch: boundary blocks first (they run alongside the tiles), then tile blocks over
-// runs of zc planes; zc shrinks until the tiles fill at least four waves of resident blocks.
-template <class AT, class Gather, class Op, bool HEX>
-void launch_duvi_grid_h(const LaunchEnv &e, const dv_matrix *m, Gather g, Op op) {
-    auto kern = k_duvi_grid<AT, Gather, Op, HEX>;
-    const size_t smem = std::max(2 * sizeof(AT) * (size_t)kGridPlane,
-                                 sizeof(PatRec<AT>) * (size_t)m->pat_entries + 4 * ((size_t)m->pat_count + 1));
-    static SmemLimit limit;   // per instantiation and device
-    limit.raise(kern, smem, e.ctx->device);
-    static OccupancyCache occupancy;   // per instantiation
-    const int occ = occupancy.get(kern, 256, smem, e.ctx->device);
-    GridCoef<AT> cf;
-    for (int k = 0; k < 81; ++k)
-        for (int d = 0; d < 3; ++d) cf.v[k][d] = (AT)m->grid_coef[3 * k + d];
-    for (int c = 0; c < kHexClasses; ++c) cf.cls[c] = HEX ? (AT)m->grid_cls[c] : AT(0);
-    GridGeom G;
-    G.lx = m->grid_lx;
-    G.ly = m->grid_ly;
-    G.lz = m->grid_lz;
-    G.ntx = (G.lx + kGridTX - 1) / kGridTX;
-    G.nty = (G.ly + kGridTY - 1) / kGridTY;
-    G.hot = m->grid_hot;
-    G.all_hot = m->grid_all_hot;
-    G.nbound = m->grid_nb;
-    const int64_t wave = (int64_t)e.ctx->num_sms * occ;
-    G.bound_blocks = G.nbound == 0 ? 0
-                     : (int32_t)std::min<int64_t>((G.nbound + 255) / 256, std::max<int64_t>(1, e.max_blocks / 4));
-    const int64_t plane_tiles = (int64_t)G.ntx * G.nty;
-    int zc = 16;
-    while (zc > 4 && plane_tiles * ((G.lz + zc - 1) / zc) < 4 * wave) zc /= 2;
-    G.zc = zc;
-    G.ntile = (int32_t)(plane_tiles * ((G.lz + zc - 1) / zc));
-    const int64_t tile_blocks = std::min<int64_t>(G.ntile, std::max<int64_t>(1, e.max_blocks - G.bound_blocks));
-    const int blocks = (int)(G.bound_blocks + tile_blocks);
-    kern<<<blocks, 256, smem, e.stream>>>(G, cf, m->pat_id.as<uint16_t>(), m->pat_start.as<uint32_t>(),
-                                          static_cast<const PatRec<AT> *>(m->pat_rec.p), m->grid_bnode.as<uint32_t>(),
-                                          m->pat_count, m->pat_entries, g, op, e.done, e.partials, e.ticket);
-    DV_CUDA(cudaGetLastError());
-    e.ctx->count();
-}
 
 template <class AT, class Gather, class Op, int G>
 void launch_duvi_pattern_g(const LaunchEnv &e, const dv_matrix *m, Gather g, Op op);
@@ -1268,33 +1403,42 @@ void launch_csr_tpr(const LaunchEnv &e, const dv_matrix *m, Gather g, Op op) {
 // for every modulus and Poisson ratio (the element's symmetries; no entry is structurally
 // zero).  Checked against Ke when an operator is created.
 constexpr int kKeClasses = 14;
-__host__ __device__ constexpr int ke_class(int i) {
-    constexpr signed char t[576] = {
-         0,  1,  1,  2,  3,  3,  4,  5,  6,  7,  8,  9,  7,  9,  8,  4,  6,  5, 10, 11, 11, 12, 13, 13,
-         1,  0,  1,  8,  7,  9,  5,  4,  6,  3,  2,  3,  9,  7,  8, 13, 12, 13, 11, 10, 11,  6,  4,  5,
-         1,  1,  0,  8,  9,  7, 13, 13, 12,  9,  8,  7,  3,  3,  2,  5,  6,  4, 11, 11, 10,  6,  5,  4,
-         2,  8,  8,  0,  5,  5,  7,  3, 11,  4,  1, 13,  4, 13,  1,  7, 11,  3, 12,  6,  6, 10,  9,  9,
-         3,  7,  9,  5,  0,  1,  8,  2,  3,  1,  4,  6,  6, 12, 13, 11,  7,  8, 13,  4,  5,  9, 10, 11,
-         3,  9,  7,  5,  1,  0, 11,  8,  7,  6, 13, 12,  1,  6,  4,  8,  3,  2, 13,  5,  4,  9, 11, 10,
-         4,  5, 13,  7,  8, 11,  0,  1,  5,  2,  3,  8, 10, 11,  9, 12, 13,  6,  7,  9,  3,  4,  6,  1,
-         5,  4, 13,  3,  2,  8,  1,  0,  5,  8,  7, 11, 11, 10,  9,  6,  4,  1,  9,  7,  3, 13, 12,  6,
-         6,  6, 12, 11,  3,  7,  5,  5,  0,  3, 11,  7,  9,  9, 10, 13,  1,  4,  8,  8,  2,  1, 13,  4,
-         7,  3,  9,  4,  1,  6,  2,  8,  3,  0,  5,  1, 12,  6, 13, 10,  9, 11,  4, 13,  5,  7, 11,  8,
-         8,  2,  8,  1,  4, 13,  3,  7, 11,  5,  0,  5, 13,  4,  1,  9, 10,  9,  6, 12,  6, 11,  7,  3,
-         9,  3,  7, 13,  6, 12,  8, 11,  7,  1,  5,  0,  6,  1,  4, 11,  9, 10,  5, 13,  4,  3,  8,  2,
-         7,  9,  3,  4,  6,  1, 10, 11,  9, 12, 13,  6,  0,  1,  5,  2,  3,  8,  4,  5, 13,  7,  8, 11,
-         9,  7,  3, 13, 12,  6, 11, 10,  9,  6,  4,  1,  1,  0,  5,  8,  7, 11,  5,  4, 13,  3,  2,  8,
-         8,  8,  2,  1, 13,  4,  9,  9, 10, 13,  1,  4,  5,  5,  0,  3, 11,  7,  6,  6, 12, 11,  3,  7,
-         4, 13,  5,  7, 11,  8, 12,  6, 13, 10,  9, 11,  2,  8,  3,  0,  5,  1,  7,  3,  9,  4,  1,  6,
-         6, 12,  6, 11,  7,  3, 13,  4,  1,  9, 10,  9,  3,  7, 11,  5,  0,  5,  8,  2,  8,  1,  4, 13,
-         5, 13,  4,  3,  8,  2,  6,  1,  4, 11,  9, 10,  8, 11,  7,  1,  5,  0,  9,  3,  7, 13,  6, 12,
-        10, 11, 11, 12, 13, 13,  7,  9,  8,  4,  6,  5,  4,  5,  6,  7,  8,  9,  0,  1,  1,  2,  3,  3,
-        11, 10, 11,  6,  4,  5,  9,  7,  8, 13, 12, 13,  5,  4,  6,  3,  2,  3,  1,  0,  1,  8,  7,  9,
-        11, 11, 10,  6,  5,  4,  3,  3,  2,  5,  6,  4, 13, 13, 12,  9,  8,  7,  1,  1,  0,  8,  9,  7,
-        12,  6,  6, 10,  9,  9,  4, 13,  1,  7, 11,  3,  7,  3, 11,  4,  1, 13,  2,  8,  8,  0,  5,  5,
-        13,  4,  5,  9, 10, 11,  6, 12, 13, 11,  7,  8,  8,  2,  3,  1,  4,  6,  3,  7,  9,  5,  0,  1,
-        13,  5,  4,  9, 11, 10,  1,  6,  4,  8,  3,  2, 11,  8,  7,  6, 13, 12,  3,  9,  7,  5,  1,  0};
-    return t[i];
+#define DV_KE_CLASS_TABLE \
+    0,  1,  1,  2,  3,  3,  4,  5,  6,  7,  8,  9,  7,  9,  8,  4,  6,  5, 10, 11, 11, 12, 13, 13, \
+    1,  0,  1,  8,  7,  9,  5,  4,  6,  3,  2,  3,  9,  7,  8, 13, 12, 13, 11, 10, 11,  6,  4,  5, \
+    1,  1,  0,  8,  9,  7, 13, 13, 12,  9,  8,  7,  3,  3,  2,  5,  6,  4, 11, 11, 10,  6,  5,  4, \
+    2,  8,  8,  0,  5,  5,  7,  3, 11,  4,  1, 13,  4, 13,  1,  7, 11,  3, 12,  6,  6, 10,  9,  9, \
+    3,  7,  9,  5,  0,  1,  8,  2,  3,  1,  4,  6,  6, 12, 13, 11,  7,  8, 13,  4,  5,  9, 10, 11, \
+    3,  9,  7,  5,  1,  0, 11,  8,  7,  6, 13, 12,  1,  6,  4,  8,  3,  2, 13,  5,  4,  9, 11, 10, \
+    4,  5, 13,  7,  8, 11,  0,  1,  5,  2,  3,  8, 10, 11,  9, 12, 13,  6,  7,  9,  3,  4,  6,  1, \
+    5,  4, 13,  3,  2,  8,  1,  0,  5,  8,  7, 11, 11, 10,  9,  6,  4,  1,  9,  7,  3, 13, 12,  6, \
+    6,  6, 12, 11,  3,  7,  5,  5,  0,  3, 11,  7,  9,  9, 10, 13,  1,  4,  8,  8,  2,  1, 13,  4, \
+    7,  3,  9,  4,  1,  6,  2,  8,  3,  0,  5,  1, 12,  6, 13, 10,  9, 11,  4, 13,  5,  7, 11,  8, \
+    8,  2,  8,  1,  4, 13,  3,  7, 11,  5,  0,  5, 13,  4,  1,  9, 10,  9,  6, 12,  6, 11,  7,  3, \
+    9,  3,  7, 13,  6, 12,  8, 11,  7,  1,  5,  0,  6,  1,  4, 11,  9, 10,  5, 13,  4,  3,  8,  2, \
+    7,  9,  3,  4,  6,  1, 10, 11,  9, 12, 13,  6,  0,  1,  5,  2,  3,  8,  4,  5, 13,  7,  8, 11, \
+    9,  7,  3, 13, 12,  6, 11, 10,  9,  6,  4,  1,  1,  0,  5,  8,  7, 11,  5,  4, 13,  3,  2,  8, \
+    8,  8,  2,  1, 13,  4,  9,  9, 10, 13,  1,  4,  5,  5,  0,  3, 11,  7,  6,  6, 12, 11,  3,  7, \
+    4, 13,  5,  7, 11,  8, 12,  6, 13, 10,  9, 11,  2,  8,  3,  0,  5,  1,  7,  3,  9,  4,  1,  6, \
+    6, 12,  6, 11,  7,  3, 13,  4,  1,  9, 10,  9,  3,  7, 11,  5,  0,  5,  8,  2,  8,  1,  4, 13, \
+    5, 13,  4,  3,  8,  2,  6,  1,  4, 11,  9, 10,  8, 11,  7,  1,  5,  0,  9,  3,  7, 13,  6, 12, \
+    10, 11, 11, 12, 13, 13,  7,  9,  8,  4,  6,  5,  4,  5,  6,  7,  8,  9,  0,  1,  1,  2,  3,  3, \
+    11, 10, 11,  6,  4,  5,  9,  7,  8, 13, 12, 13,  5,  4,  6,  3,  2,  3,  1,  0,  1,  8,  7,  9, \
+    11, 11, 10,  6,  5,  4,  3,  3,  2,  5,  6,  4, 13, 13, 12,  9,  8,  7,  1,  1,  0,  8,  9,  7, \
+    12,  6,  6, 10,  9,  9,  4, 13,  1,  7, 11,  3,  7,  3, 11,  4,  1, 13,  2,  8,  8,  0,  5,  5, \
+    13,  4,  5,  9, 10, 11,  6, 12, 13, 11,  7,  8,  8,  2,  3,  1,  4,  6,  3,  7,  9,  5,  0,  1, \
+    13,  5,  4,  9, 11, 10,  1,  6,  4,  8,  3,  2, 11,  8,  7,  6, 13, 12,  3,  9,  7,  5,  1,  0
+// The same table in device and host memory: device code indexes the __device__ copy, which
+// the compiler folds to constants after unrolling (a table local to a constexpr function
+// would be rebuilt at every inlined call).
+__device__ constexpr signed char kKeClassDev[576] = {DV_KE_CLASS_TABLE};
+constexpr signed char kKeClassHost[576] = {DV_KE_CLASS_TABLE};
+__host__ __device__ __forceinline__ constexpr int ke_class(int i) {
+#ifdef __CUDA_ARCH__
+    return kKeClassDev[i];
+#else
+    return kKeClassHost[i];
+#endif
 }
 
 template <class AT>
@@ -1364,95 +1508,86 @@ __global__ void __launch_bounds__(256, sizeof(AT) == 8 ? 1 : 3)
     if (done && *(volatile const int *)done) return;
     extern __shared__ uint4 hex_smem[];
     constexpr bool FU = op_fused<Op>::value;
-    AT *plane = reinterpret_cast<AT *>(hex_smem);    // 2 x kGridPlane node values
-    AT *layer = plane + 2 * kGridPlane;              // 3 x kHexLayer element factors
+    using SS = StageSrc<Gather>;
+    using ST = typename SS::ST;
+    constexpr int SLOT = SS::N * kGridPlane;
+    constexpr int NL = kGridStages + 1;              // factor layers: each is read in two consecutive steps
+    ST *ring = reinterpret_cast<ST *>(hex_smem);     // kGridStages slots of node planes
+    AT *layer = reinterpret_cast<AT *>(ring + kGridStages * SLOT);   // NL slots of element factors
     double red[Op::NRED > 0 ? Op::NRED : 1];
 #pragma unroll
     for (int i = 0; i < (Op::NRED > 0 ? Op::NRED : 1); ++i) red[i] = 0.0;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-    int sx[kGridLoads], sy[kGridLoads], sc[kGridLoads];
-#pragma unroll
-    for (int j = 0; j < kGridLoads; ++j) {
-        const int k = threadIdx.x + 256 * j;
-        const int row = k / (kGridPX * 3), col = k - row * (kGridPX * 3);
-        sx[j] = col / 3 - 1;
-        sc[j] = col - 3 * (col / 3);
-        sy[j] = k < kGridPlane ? row - 1 : -1000000;
-    }
-    int ex_[kHexLayerLoads], ey_[kHexLayerLoads];
-#pragma unroll
-    for (int j = 0; j < kHexLayerLoads; ++j) {
-        const int k = threadIdx.x + 256 * j;
-        ey_[j] = k < kHexLayer ? k / kHexEX : -1000000;
-        ex_[j] = k - (k / kHexEX) * kHexEX;
-    }
+    const StageSlots slots;
     const int64_t lxy = (int64_t)G.lx * G.ly;
+    const int32_t plane_len = (int32_t)(3 * lxy), layer_len = G.ne0 * G.ne1;
     for (int t = blockIdx.x; t < G.ntile; t += gridDim.x) {
         const int txi = t % G.ntx, tyi = (t / G.ntx) % G.nty, tzi = t / (G.ntx * G.nty);
         const int x0 = txi * kGridTX, y0 = tyi * kGridTY, z0 = tzi * G.zc, z1 = min(G.lz, z0 + G.zc);
         const int ix = x0 + tx, iy = y0 + ty;
         const bool inxy = ix < G.lx && iy < G.ly;
-        const int64_t col_xy = (int64_t)ix + (int64_t)G.lx * iy;
-        AT pre[kGridLoads], pe[kHexLayerLoads];
-        auto load = [&](int z) {   // node plane z and element layer z (elements between planes z and z + 1)
+        const int32_t col_xy = ix + G.lx * iy;
+        int32_t poff[kGridLoads], loff[kHexLayerLoads];
+        slots.plane_offsets(x0, y0, G.lx, G.ly, poff);
 #pragma unroll
-            for (int j = 0; j < kGridLoads; ++j) {
-                const int xn = x0 + sx[j], yn = y0 + sy[j];
-                AT v = AT(0);
-                if (xn >= 0 && xn < G.lx && yn >= 0 && yn < G.ly && z >= 0 && z < G.lz)
-                    v = g((uint32_t)(3 * ((int64_t)xn + (int64_t)G.lx * yn + lxy * z) + sc[j]));
-                pre[j] = v;
-            }
+        for (int j = 0; j < kHexLayerLoads; ++j) {   // element (ex, ey) of the layer tile (x index 0 is clamped)
+            const int k = threadIdx.x + 256 * j;
+            const int ex = x0 + k % kHexEX, ey = y0 - 1 + k / kHexEX;
+            loff[j] = (k < kHexLayer && ex < G.ne0 && ey >= 0 && ey < G.ne1) ? ex + G.ne0 * ey : (k < kHexLayer ? -1 : -2);
+        }
+        // node plane z and element layer z (elements between planes z and z + 1), one copy group
+        auto issue = [&](int z, int k) {
+            const bool lin = z >= 0 && z < G.ne2;
+            const int32_t lbase = lin ? z * layer_len : 0;
+            AT *ld = layer + (k % NL) * kHexLayer;
 #pragma unroll
-            for (int j = 0; j < kHexLayerLoads; ++j) {
-                const int ex = x0 + ex_[j], ey = y0 - 1 + ey_[j];   // element (ex, ey, z): nodes x ex..ex+1 (x index 0 clamped)
-                AT v = AT(0);
-                if (ex < G.ne0 && ey >= 0 && ey < G.ne1 && z >= 0 && z < G.ne2)
-                    v = __ldg(ef + (ex + (int64_t)G.ne0 * (ey + (int64_t)G.ne1 * z)));
-                pe[j] = v;
-            }
+            for (int j = 0; j < kHexLayerLoads; ++j)
+                if (loff[j] > -2) {
+                    const bool v = lin && loff[j] >= 0;
+                    cp_async_zfill<sizeof(AT)>(ld + threadIdx.x + 256 * j, v ? ef + lbase + loff[j] : ef, v);
+                }
+            slots.issue<SS>(g, ring + (k % kGridStages) * SLOT, poff, z, G.lz, plane_len);   // commits the group
         };
-        load(z0 - 1);
+#pragma unroll
+        for (int q = 0; q < kGridStages - 1; ++q) {
+            if (z0 - 1 + q <= z1) issue(z0 - 1 + q, q);
+            else cp_async_commit();
+        }
         AT a0[3], a1[3], a2[3];
 #pragma unroll
         for (int d = 0; d < 3; ++d) a0[d] = a1[d] = a2[d] = AT(0);
-        for (int p = z0 - 1; p <= z1; ++p) {
-            AT *pl = plane + (p & 1) * kGridPlane;
-            AT *lay_up = layer + ((p + 3) % 3) * kHexLayer;       // layer p: elements between planes p and p + 1
-            const AT *lay_dn = layer + ((p + 2) % 3) * kHexLayer; // layer p - 1
-#pragma unroll
-            for (int j = 0; j < kGridLoads; ++j)
-                if (sy[j] > -2) pl[threadIdx.x + 256 * j] = pre[j];
-#pragma unroll
-            for (int j = 0; j < kHexLayerLoads; ++j)
-                if (ey_[j] >= 0) lay_up[threadIdx.x + 256 * j] = pe[j];
+        for (int p = z0 - 1, k = 0; p <= z1; ++p, ++k) {
+            cp_async_wait<kGridStages - 2>();
             __syncthreads();
-            if (p + 1 <= z1) load(p + 1);
+            if (p + kGridStages - 1 <= z1) issue(p + kGridStages - 1, k + kGridStages - 1);
+            else cp_async_commit();
+            const ST *pl = ring + (k % kGridStages) * SLOT;
+            const AT *lay_up = layer + (k % NL) * kHexLayer;             // layer p
+            const AT *lay_dn = layer + ((k + NL - 1) % NL) * kHexLayer;  // layer p - 1
             const bool di = p + 1 >= z0 && p + 1 < z1, dm = p >= z0 && p < z1, df = p - 1 >= z0 && p - 1 < z1;
             if (di) {
                 const int32_t r = (int32_t)(3 * (col_xy + lxy * (p + 1)));
 #pragma unroll
                 for (int d = 0; d < 3; ++d) a2[d] = inxy ? op.init(r + d) : AT(0);
             }
+            if (dm && inxy) touch_rows(op, (int32_t)(3 * (col_xy + lxy * p)));   // finished next step
             AT xv[27];
 #pragma unroll
             for (int dy = 0; dy < 3; ++dy)
 #pragma unroll
                 for (int dx = 0; dx < 3; ++dx)
 #pragma unroll
-                    for (int c = 0; c < 3; ++c) xv[9 * dy + 3 * dx + c] = pl[((ty + dy) * kGridPX + tx + dx) * 3 + c];
+                    for (int c = 0; c < 3; ++c) xv[9 * dy + 3 * dx + c] = SS::value(pl, ((ty + dy) * kGridPX + tx + dx) * 3 + c);
             if (di && dm && df) hex_plane_step<AT, FU, true, true, true>(xv, lay_up, lay_dn, tx, ty, kc, a0, a1, a2);
             else if (di && dm) hex_plane_step<AT, FU, true, true, false>(xv, lay_up, lay_dn, tx, ty, kc, a0, a1, a2);
             else if (dm && df) hex_plane_step<AT, FU, false, true, true>(xv, lay_up, lay_dn, tx, ty, kc, a0, a1, a2);
             else if (di) hex_plane_step<AT, FU, true, false, false>(xv, lay_up, lay_dn, tx, ty, kc, a0, a1, a2);
             else if (dm) hex_plane_step<AT, FU, false, true, false>(xv, lay_up, lay_dn, tx, ty, kc, a0, a1, a2);
             else if (df) hex_plane_step<AT, FU, false, false, true>(xv, lay_up, lay_dn, tx, ty, kc, a0, a1, a2);
-            if (df) {
-                if (inxy) {
-                    const int32_t r = (int32_t)(3 * (col_xy + lxy * (p - 1)));
+            if (df && inxy) {
+                const int32_t r = (int32_t)(3 * (col_xy + lxy * (p - 1)));
 #pragma unroll
-                    for (int d = 0; d < 3; ++d) op.row(r + d, a0[d], red);
-                }
+                for (int d = 0; d < 3; ++d) op.row(r + d, a0[d], red);
             }
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
@@ -1460,7 +1595,8 @@ __global__ void __launch_bounds__(256, sizeof(AT) == 8 ? 1 : 3)
                 a1[d] = a2[d];
             }
         }
-        __syncthreads();   // the next tile restarts the buffer rotation
+        cp_async_wait<0>();
+        __syncthreads();   // the next tile refills the rings
     }
     if constexpr (Op::NRED > 0) {
         double tot[Op::NRED];
@@ -1471,7 +1607,9 @@ __global__ void __launch_bounds__(256, sizeof(AT) == 8 ? 1 : 3)
 template <class AT, class Gather, class Op>
 void launch_hex_elem(const LaunchEnv &e, const dv_matrix *m, Gather g, Op op) {
     auto kern = k_hex_elem<AT, Gather, Op>;
-    const size_t smem = sizeof(AT) * (2 * (size_t)kGridPlane + 3 * (size_t)kHexLayer);
+    using SS = StageSrc<Gather>;
+    const size_t smem = sizeof(typename SS::ST) * SS::N * kGridStages * (size_t)kGridPlane +
+                        sizeof(AT) * (kGridStages + 1) * (size_t)kHexLayer;
     static SmemLimit limit;   // per instantiation and device
     limit.raise(kern, smem, e.ctx->device);
     static OccupancyCache occupancy;   // per instantiation
@@ -1487,11 +1625,9 @@ void launch_hex_elem(const LaunchEnv &e, const dv_matrix *m, Gather g, Op op) {
     G.lz = G.ne2 + 1;
     G.ntx = (G.lx + kGridTX - 1) / kGridTX;
     G.nty = (G.ly + kGridTY - 1) / kGridTY;
-    const int64_t wave = (int64_t)e.ctx->num_sms * occ, plane_tiles = (int64_t)G.ntx * G.nty;
-    int zc = 16;
-    while (zc > 4 && plane_tiles * ((G.lz + zc - 1) / zc) < 4 * wave) zc /= 2;
-    G.zc = zc;
-    G.ntile = (int32_t)(plane_tiles * ((G.lz + zc - 1) / zc));
+    const int64_t plane_tiles = (int64_t)G.ntx * G.nty;
+    G.zc = stream_run_length(plane_tiles, G.lz, (int64_t)e.ctx->num_sms * occ);
+    G.ntile = (int32_t)(plane_tiles * ((G.lz + G.zc - 1) / G.zc));
     const int blocks = (int)std::min<int64_t>(G.ntile, e.max_blocks);
     kern<<<blocks, 256, smem, e.stream>>>(G, kc, static_cast<const AT *>(m->hex_factor.p), g, op, e.done, e.partials,
                                           e.ticket);
