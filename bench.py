@@ -82,6 +82,7 @@ def parse():
     p.add_argument("--batch-size", type=int, default=64, help="mesh edge of the multi-load-case section")
     p.add_argument("--batch-k", type=int, default=64, help="load cases of the multi-load-case section")
     p.add_argument("--batch-meshes", type=int, default=32, help="meshes of the batched-mesh section")
+    p.add_argument("--resid", action="store_true", help="with --spmv-only: time r = b - A x instead of y = A x")
     p.add_argument("--spmv-only", default=None, metavar="FMT_PREC",
                    help="only time the SpMV of the finest operator (duvi_f32, duvi_f64, csr_f32, csr_f64, or the "
                         "matrix-free hex_f32, hex_f64 with E = 10^U(-2,0)): the case used for ncu captures")
@@ -833,14 +834,18 @@ def run_spmv_only(args):
     g = torch.Generator(device="cuda").manual_seed(20261203)
     x = torch.randn(M.shape[0], dtype=dt, device="cuda", generator=g)
     y = torch.zeros_like(x)
+    b = torch.randn(M.shape[0], dtype=dt, device="cuda", generator=g)
     torch.cuda.synchronize()
-    fn = lambda: M.multiply_device(x.data_ptr(), y.data_ptr(), prec)
+    if args.resid:
+        fn = lambda: M.residual_device(b.data_ptr(), x.data_ptr(), y.data_ptr(), prec)
+    else:
+        fn = lambda: M.multiply_device(x.data_ptr(), y.data_ptr(), prec)
     for _ in range(args.warmup):
         fn()
     ctx.synchronize()
     ms = time_events(torch.cuda.ExternalStream(ctx.stream), fn, args.steps)
-    alg = info["device_bytes"] + 2 * (4 if prec == "f32" else 8) * M.shape[0]
-    print(json.dumps({"spmv": args.spmv_only, "size": n, "ms": ms, "algorithmic_bytes": int(alg),
+    alg = info["device_bytes"] + (3 if args.resid else 2) * (4 if prec == "f32" else 8) * M.shape[0]
+    print(json.dumps({"spmv": args.spmv_only, "resid": args.resid, "size": n, "ms": ms, "algorithmic_bytes": int(alg),
                       "GBps": alg / ms / 1e6, "launch_shape": info["kernel_variant"]}), flush=True)
     M.release()
     ctx.close()
