@@ -192,6 +192,40 @@ std::vector<double> dv_number_values(const double *val, int64_t nnz, double tol,
     return map.keys;
 }
 
+bool dv_number_distinct(const double *distinct, int64_t nd, double tol, uint32_t *key_of, std::vector<double> &keys) {
+    for (int64_t i = 0; i < nd; ++i)
+        if (tol > 0 && !std::isfinite(distinct[i])) return false;
+    NetDoubleDict map(tol);
+    for (int64_t i = 0; i < nd; ++i) key_of[i] = (uint32_t)map.find_or_insert(distinct[i]);
+    // codes held by more than one key, and whether a value matches two of them
+    std::vector<std::pair<int32_t, int32_t>> ck(map.keys.size());
+    for (size_t k = 0; k < ck.size(); ++k) ck[k] = {map.codes[k], (int32_t)k};
+    std::sort(ck.begin(), ck.end());
+    std::vector<std::pair<int32_t, std::vector<int32_t>>> shared;
+    for (size_t k = 0; k < ck.size();) {
+        size_t e = k + 1;
+        while (e < ck.size() && ck[e].first == ck[k].first) ++e;
+        if (e - k > 1) {
+            shared.push_back({ck[k].first, {}});
+            for (size_t q = k; q < e; ++q) shared.back().second.push_back(ck[q].second);
+        }
+        k = e;
+    }
+    if (!shared.empty())
+        for (int64_t i = 0; i < nd; ++i) {
+            const double v = distinct[i];
+            const int32_t c = map.code(v);
+            auto it = std::lower_bound(shared.begin(), shared.end(), c,
+                                       [](const std::pair<int32_t, std::vector<int32_t>> &x, int32_t y) { return x.first < y; });
+            if (it == shared.end() || it->first != c) continue;
+            int hits = 0;
+            for (int32_t k : it->second) hits += map.eq(v, map.keys[k]) ? 1 : 0;
+            if (hits > 1) return false;
+        }
+    keys = std::move(map.keys);
+    return true;
+}
+
 // FromDokRowMajor (OpenCLDuViGeometricMultigridSolver.cs:753-851).  The block
 // ("DU") part is independent per row and built in parallel; the value ("VI")
 // part is sequential in CSR order because first occurrence defines the index.
@@ -673,6 +707,33 @@ void dv_build_duvi_patterns(const DuviHost &h, int32_t n, int32_t n_cols, int g,
     P.ok = 1;
 }
 
+bool dv_grid_geometry(const DuviPatternHost &P, int hot, int64_t ng, int32_t &lxo, int32_t &lyo, int32_t &lzo) {
+    if (P.group != 3 || P.based || P.shift || ng < 27 || hot < 0 || hot + 1 >= (int)P.start.size()) return false;
+    const uint32_t s0 = P.start[hot];
+    if (P.start[hot + 1] - s0 != 81) return false;
+    // the 27 neighbour groups, each with its 3 consecutive columns, in column order
+    int64_t no[27];
+    for (int j = 0; j < 27; ++j) {
+        const int64_t o = P.off[s0 + 3 * j];
+        for (int c = 1; c < 3; ++c)
+            if (P.off[s0 + 3 * j + c] != o + c) return false;
+        if (((o % 3) + 3) % 3 != 0) return false;
+        no[j] = o / 3;
+    }
+    const int64_t lx = no[16], lxy = no[22];   // offsets of the +y and +z neighbours
+    if (lx < 3 || lxy < 3 * lx || lxy % lx != 0) return false;
+    for (int dz = -1; dz <= 1; ++dz)
+        for (int dy = -1; dy <= 1; ++dy)
+            for (int dx = -1; dx <= 1; ++dx)
+                if (no[9 * (dz + 1) + 3 * (dy + 1) + dx + 1] != dx + lx * dy + lxy * dz) return false;
+    const int64_t ly = lxy / lx;
+    if (ly < 3 || ng % lxy != 0 || ng / lxy < 3 || lx > INT32_MAX || ly > INT32_MAX) return false;
+    lxo = (int32_t)lx;
+    lyo = (int32_t)ly;
+    lzo = (int32_t)(ng / lxy);
+    return true;
+}
+
 void dv_build_duvi_grid(const DuviPatternHost &P, DuviGridHost &G) {
     G = DuviGridHost();
     if (!P.ok || P.group != 3 || P.based || P.shift || P.ngroups < 27) return;
@@ -680,26 +741,9 @@ void dv_build_duvi_grid(const DuviPatternHost &P, DuviGridHost &G) {
     std::vector<int64_t> cnt(npat, 0);
     for (uint16_t id : P.id) cnt[id]++;
     const int hot = (int)(std::max_element(cnt.begin(), cnt.end()) - cnt.begin());
-    const uint32_t s0 = P.start[hot];
-    if (P.start[hot + 1] - s0 != 81) return;
-    // the 27 neighbour groups, each with its 3 consecutive columns, in column order
-    int64_t no[27];
-    for (int j = 0; j < 27; ++j) {
-        const int64_t o = P.off[s0 + 3 * j];
-        for (int c = 1; c < 3; ++c)
-            if (P.off[s0 + 3 * j + c] != o + c) return;
-        if (((o % 3) + 3) % 3 != 0) return;
-        no[j] = o / 3;
-    }
-    const int64_t lx = no[16], lxy = no[22];   // offsets of the +y and +z neighbours
-    if (lx < 3 || lxy < 3 * lx || lxy % lx != 0) return;
-    for (int dz = -1; dz <= 1; ++dz)
-        for (int dy = -1; dy <= 1; ++dy)
-            for (int dx = -1; dx <= 1; ++dx)
-                if (no[9 * (dz + 1) + 3 * (dy + 1) + dx + 1] != dx + lx * dy + lxy * dz) return;
-    const int64_t ly = lxy / lx, ng = P.ngroups;
-    if (ly < 3 || ng % lxy != 0 || ng / lxy < 3 || lx > INT32_MAX || ly > INT32_MAX) return;
-    const int64_t lz = ng / lxy;
+    int32_t lx, ly, lz;
+    if (!dv_grid_geometry(P, hot, P.ngroups, lx, ly, lz)) return;
+    const int64_t ng = P.ngroups, lxy = (int64_t)lx * ly;
     bool all_hot = true;
     for (int64_t gi = 0; gi < ng; ++gi) {
         const int64_t ix = gi % lx, iy = (gi / lx) % ly, iz = gi / lxy;
@@ -708,10 +752,11 @@ void dv_build_duvi_grid(const DuviPatternHost &P, DuviGridHost &G) {
         if (inner) all_hot = false;
         G.boundary.push_back((uint32_t)gi);
     }
+    const uint32_t s0 = P.start[hot];
     G.vi.assign(P.vi.begin() + 3 * (size_t)s0, P.vi.begin() + 3 * (size_t)(s0 + 81));
-    G.lx = (int32_t)lx;
-    G.ly = (int32_t)ly;
-    G.lz = (int32_t)lz;
+    G.lx = lx;
+    G.ly = ly;
+    G.lz = lz;
     G.hot = hot;
     G.all_hot = all_hot ? 1 : 0;
     G.ok = 1;

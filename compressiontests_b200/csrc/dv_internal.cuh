@@ -232,6 +232,7 @@ struct dv_matrix {
     int32_t hex_ne[3] = {0, 0, 0};       // DV_FORMAT_HEX: elements per axis
     DevMem hex_factor;                   // per-element factor scale * E_e, matrix precision
     double hex_cls[14] = {};             // value classes of Ke (dvk::ke_class)
+    int lanes_ok = 0;          // lane layout built (host-encoded matrices)
     int lanes_stencil = 0;     // stencil mode: lanes_off holds the column offsets (int32)
     DevMem lanes_off;
     int32_t lanes_noff = 0;
@@ -300,6 +301,14 @@ void dv_make_bundles(const DuviHost &h, int32_t n_rows, int vi_bits, std::vector
 // (default double comparer for tol == 0); idx[i] receives the value's key, the keys are
 // returned in insertion order.
 std::vector<double> dv_number_values(const double *val, int64_t n, double tol, uint32_t *idx);
+// The same numbering from the distinct bit patterns of the values, given in order of first
+// occurrence: key_of[i] receives the key of distinct[i], keys the keys in insertion order.
+// Equal to the sequential walk unless a value could match two keys of its hash code or a
+// non-finite value meets a tolerance: then returns false (number every value instead).
+bool dv_number_distinct(const double *distinct, int64_t nd, double tol, uint32_t *key_of, std::vector<double> &keys);
+// Node-pattern layout from its pattern table (off, vi, start, group, shift, based) without the
+// per-group ids: the hot pattern's grid geometry (see DuviGridHost), or false.
+bool dv_grid_geometry(const DuviPatternHost &P, int hot, int64_t ngroups, int32_t &lx, int32_t &ly, int32_t &lz);
 // Throws DV_ERR_ARG / DV_ERR_FORMAT unless a is a valid CSR matrix with strictly
 // increasing columns in every row.
 void dv_check_csr(const dv_csr_host &a);
@@ -319,6 +328,16 @@ void dv_hex_ke(double E, double nu, double *ke);
 int dv_block_coloring(const dv_csr_host &a, int bs, std::vector<int32_t> &color_of_block);
 // Level sets of the forward Gauss-Seidel dependency graph (row i depends on j < i).
 int dv_gs_level_sets(const dv_csr_host &a, std::vector<int32_t> &perm, std::vector<int32_t> &offsets);
+
+// Pattern tables (records, starts, bases) of P with the given value table, and the grid-stencil
+// fields of Gd (false when the stencil does not apply to this matrix); pattern ids and the
+// boundary list are uploaded by the caller (dv_matrix.cu).
+void dv_upload_patterns(dv_matrix *m, const DuviPatternHost &P, const std::vector<double> &values, cudaStream_t s);
+bool dv_set_grid(dv_matrix *m, const DuviGridHost &Gd, const std::vector<double> &values);
+// DuVi arrays, value table, diagonal and node-pattern / grid layouts of m (n_rows, n_cols, nnz,
+// precision set) from a device CSR matrix, on the device (dv_encode_device.cu).
+void dv_duvi_from_device_csr(dv_matrix *m, const int32_t *rp, const int32_t *col, const double *val, int force_bits,
+                             double tol);
 
 // Matrix creation (dv_matrix.cu)
 // encoded: a DuVi encoding of a made with the same vi_bits and tol, used instead of

@@ -91,6 +91,54 @@ static int pick_tpr(double mean_nnz) {
 
 // Uploads the SoA arrays of encoding h and derives the device layouts; h is only read
 // here (export reads the device arrays back), so callers keep it only while building.
+void dv_upload_patterns(dv_matrix *m, const DuviPatternHost &P, const std::vector<double> &values, cudaStream_t s) {
+    const int rec_bytes = m->precision == DV_F64 ? 32 : 16;
+    const size_t ne = P.off.size();
+    std::vector<unsigned char> recs(ne * rec_bytes, 0);
+    for (size_t k = 0; k < ne; ++k) {
+        unsigned char *r = recs.data() + k * rec_bytes;
+        std::memcpy(r, &P.off[k], 4);
+        for (int d = 0; d < P.group; ++d) {
+            const double v = values[P.vi[k * P.group + d]];
+            if (m->precision == DV_F64) std::memcpy(r + 8 + 8 * d, &v, 8);
+            else { const float f = (float)v; std::memcpy(r + 4 + 4 * d, &f, 4); }
+        }
+    }
+    upload(m->pat_start, P.start.data(), 4 * P.start.size(), s);
+    upload(m->pat_rec, recs.data(), recs.size(), s);
+    if (P.based) upload(m->pat_base, P.base.data(), 4 * P.base.size(), s);
+    DV_CUDA(cudaStreamSynchronize(s));
+    m->pat_ok = 1;
+    m->pat_based = P.based;
+    m->pat_shift = P.shift;
+    m->pat_count = (int32_t)P.start.size() - 1;
+    m->pat_entries = (int32_t)ne;
+}
+
+bool dv_set_grid(dv_matrix *m, const DuviGridHost &Gd, const std::vector<double> &values) {
+    m->grid_lx = Gd.lx;
+    m->grid_ly = Gd.ly;
+    m->grid_lz = Gd.lz;
+    m->grid_hot = Gd.hot;
+    m->grid_all_hot = Gd.all_hot;
+    m->grid_coef.resize(Gd.vi.size());
+    for (size_t i = 0; i < Gd.vi.size(); ++i) m->grid_coef[i] = values[Gd.vi[i]];
+    // the hex stencil's structure: equal values within each class, zeros where expected
+    bool hex = true, seen[dvk::kHexClasses] = {};
+    for (int i = 0; i < 243 && hex; ++i) {
+        const int c = dvk::hex_class(i);
+        const double v = m->grid_coef[i];
+        if (c < 0) hex = v == 0.0 && !std::signbit(v);
+        else if (!seen[c]) { seen[c] = true; m->grid_cls[c] = v; }
+        else hex = v == m->grid_cls[c] && std::signbit(v) == std::signbit(m->grid_cls[c]);
+    }
+    m->grid_hex = hex ? 1 : 0;
+    // FP64 runs the stencil with the hex structure only (the general FP64 stencil would hold 243
+    // coefficients in registers); otherwise the node patterns stay
+    m->grid_ok = m->grid_hex || m->precision == DV_F32;
+    return m->grid_ok;
+}
+
 static void finish_duvi_upload(dv_matrix *m, const DuviHost &h, cudaStream_t s) {
     m->vi_bits = h.vi_bits;
     m->nblocks = (int64_t)h.col_idx.size();
@@ -181,6 +229,7 @@ static void finish_duvi_upload(dv_matrix *m, const DuviHost &h, cudaStream_t s) 
                                    4 * L.nent.size() + 4 * L.offsets.size() +
                                    vs * (L.tuples ? 4 * (size_t)m->lanes_ntup : h.values.size()));
         // the lane kernel is the default when rows come in node groups
+        m->lanes_ok = 1;
         m->duvi_variant = L.group > 1 ? 1 : 0;
         const char *pe = getenv("DV_PATTERNS");   // DV_PATTERNS=0 keeps the lane layout (A/B comparisons)
         if (!(pe && pe[0] == '0')) {   // node patterns: records {offset, 3 values} in shared memory
@@ -188,58 +237,17 @@ static void finish_duvi_upload(dv_matrix *m, const DuviHost &h, cudaStream_t s) 
             DuviPatternHost P;
             dv_build_duvi_patterns(h, m->n_rows, m->n_cols, L.group, L.shift, 1024, (96 * 1024) / rec_bytes, P);
             if (P.ok) {
-                const size_t ne = P.off.size();
-                std::vector<unsigned char> recs(ne * rec_bytes, 0);
-                for (size_t k = 0; k < ne; ++k) {
-                    unsigned char *r = recs.data() + k * rec_bytes;
-                    std::memcpy(r, &P.off[k], 4);
-                    for (int d = 0; d < P.group; ++d) {
-                        const double v = h.values[P.vi[k * P.group + d]];
-                        if (m->precision == DV_F64) std::memcpy(r + 8 + 8 * d, &v, 8);
-                        else { const float f = (float)v; std::memcpy(r + 4 + 4 * d, &f, 4); }
-                    }
-                }
                 upload(m->pat_id, P.id.data(), 2 * P.id.size(), s);
-                upload(m->pat_start, P.start.data(), 4 * P.start.size(), s);
-                upload(m->pat_rec, recs.data(), recs.size(), s);
-                if (P.based) upload(m->pat_base, P.base.data(), 4 * P.base.size(), s);
-                DV_CUDA(cudaStreamSynchronize(s));
-                m->pat_ok = 1;
-                m->pat_based = P.based;
-                m->pat_shift = P.shift;
-                m->pat_count = (int32_t)P.start.size() - 1;
-                m->pat_entries = (int32_t)ne;
+                dv_upload_patterns(m, P, h.values, s);
                 m->duvi_variant = 2;
                 const char *ge = getenv("DV_GRID");   // DV_GRID=0 keeps the node-pattern kernel (A/B comparisons)
                 DuviGridHost Gd;
                 if (!(ge && ge[0] == '0')) dv_build_duvi_grid(P, Gd);
-                if (Gd.ok) {
-                    m->grid_lx = Gd.lx;
-                    m->grid_ly = Gd.ly;
-                    m->grid_lz = Gd.lz;
-                    m->grid_hot = Gd.hot;
-                    m->grid_all_hot = Gd.all_hot;
-                    m->grid_coef.resize(Gd.vi.size());
-                    for (size_t i = 0; i < Gd.vi.size(); ++i) m->grid_coef[i] = h.values[Gd.vi[i]];
-                    // the hex stencil's structure: equal values within each class, zeros where expected
-                    bool hex = true, seen[dvk::kHexClasses] = {};
-                    for (int i = 0; i < 243 && hex; ++i) {
-                        const int c = dvk::hex_class(i);
-                        const double v = m->grid_coef[i];
-                        if (c < 0) hex = v == 0.0 && !std::signbit(v);
-                        else if (!seen[c]) { seen[c] = true; m->grid_cls[c] = v; }
-                        else hex = v == m->grid_cls[c] && std::signbit(v) == std::signbit(m->grid_cls[c]);
-                    }
-                    m->grid_hex = hex ? 1 : 0;
-                    // FP64 runs the stencil with the hex structure only (the general FP64 stencil would
-                    // hold 243 coefficients in registers); otherwise the node patterns stay
-                    m->grid_ok = m->grid_hex || m->precision == DV_F32;
+                if (Gd.ok && dv_set_grid(m, Gd, h.values)) {
                     m->grid_nb = (int64_t)Gd.boundary.size();
-                    if (m->grid_ok) {
-                        upload(m->grid_bnode, Gd.boundary.data(), 4 * Gd.boundary.size(), s);
-                        DV_CUDA(cudaStreamSynchronize(s));
-                        m->duvi_variant = 3;
-                    }
+                    upload(m->grid_bnode, Gd.boundary.data(), 4 * Gd.boundary.size(), s);
+                    DV_CUDA(cudaStreamSynchronize(s));
+                    m->duvi_variant = 3;
                 }
             }
         }
@@ -305,7 +313,8 @@ static void autotune(dv_matrix *m) {
         }
     };
     // CSR: threads per row; DuVi: 4 / 9 = staged kernel with that batch width, 100 = lane kernel
-    std::vector<int> cand = m->format == DV_FORMAT_CSR ? std::vector<int>{8, 16, 32} : std::vector<int>{4, 9, 100};
+    std::vector<int> cand = m->format == DV_FORMAT_CSR ? std::vector<int>{8, 16, 32} : std::vector<int>{4, 9};
+    if (m->format == DV_FORMAT_DUVI && m->lanes_ok) cand.push_back(100);
     if (m->format == DV_FORMAT_DUVI && m->pat_ok) cand.push_back(200);
     if (m->format == DV_FORMAT_DUVI && m->grid_ok) cand.push_back(300);
     cudaEvent_t e0, e1;
@@ -391,6 +400,58 @@ dv_matrix *dv_matrix_build(dv_context *ctx, const dv_csr_host &a, int format, in
     }
     autotune(m.get());
     return m.release();
+}
+
+namespace {
+// rowptr monotone within [0, nnz], columns strictly increasing and in range; bad[0] = 1 otherwise
+__global__ void k_check_csr(const int32_t *__restrict__ rp, const int32_t *__restrict__ col, int32_t n, int32_t n_cols,
+                            int *__restrict__ bad) {
+    const int32_t nnz = rp[n];
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        bool ok = rp[i] >= 0 && rp[i + 1] >= rp[i] && rp[i + 1] <= nnz;
+        for (int32_t k = rp[i]; ok && k < rp[i + 1]; ++k)
+            ok = col[k] >= 0 && col[k] < n_cols && (k == rp[i] || col[k] > col[k - 1]);
+        if (!ok) atomicOr(bad, 1);
+    }
+}
+}  // namespace
+
+extern "C" DV_API int dv_matrix_create_duvi_device(dv_context *ctx, int32_t n_rows, int32_t n_cols,
+                                                   const int32_t *d_rowptr, const int32_t *d_col, const double *d_val,
+                                                   int32_t precision, int32_t value_index_bits, double dedup_tol,
+                                                   dv_matrix **out) {
+    return dv_guard([&] {
+        DV_REQUIRE(out && d_rowptr, DV_ERR_ARG, "null argument");
+        DV_REQUIRE(n_rows > 0 && n_cols > 0, DV_ERR_ARG, "empty matrix");
+        DV_REQUIRE(precision == DV_F64 || precision == DV_F32, DV_ERR_ARG, "precision must be DV_F64 or DV_F32");
+        dv_ctx_check(ctx);
+        cudaStream_t s = ctx->stream;
+        int32_t nnz = 0;
+        DV_CUDA(cudaMemcpyAsync(&nnz, d_rowptr + n_rows, 4, cudaMemcpyDeviceToHost, s));
+        DV_CUDA(cudaStreamSynchronize(s));
+        DV_REQUIRE(nnz >= 0 && (nnz == 0 || (d_col && d_val)), DV_ERR_FORMAT, "bad row offsets or null col/val");
+        {
+            DevMem bad(16);
+            DV_CUDA(cudaMemsetAsync(bad.p, 0, 16, s));
+            const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((n_rows + 255) / 256, (int64_t)ctx->num_sms * 16));
+            k_check_csr<<<grid, 256, 0, s>>>(d_rowptr, d_col, n_rows, n_cols, bad.as<int>());
+            DV_CUDA(cudaGetLastError());
+            int hb = 0;
+            DV_CUDA(cudaMemcpyAsync(&hb, bad.p, 4, cudaMemcpyDeviceToHost, s));
+            DV_CUDA(cudaStreamSynchronize(s));
+            DV_REQUIRE(!hb, DV_ERR_FORMAT, "not a CSR matrix with strictly increasing columns in range");
+        }
+        auto m = std::make_unique<dv_matrix>();
+        m->ctx = ctx;
+        m->n_rows = n_rows;
+        m->n_cols = n_cols;
+        m->nnz = nnz;
+        m->format = DV_FORMAT_DUVI;
+        m->precision = precision;
+        dv_duvi_from_device_csr(m.get(), d_rowptr, d_col, d_val, value_index_bits, dedup_tol);
+        autotune(m.get());
+        *out = m.release();
+    });
 }
 
 extern "C" DV_API int dv_matrix_create_csr(dv_context *ctx, const dv_csr_host *a, int32_t precision, dv_matrix **out) {

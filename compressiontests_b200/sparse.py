@@ -89,6 +89,20 @@ class SparseMatrix:
         self.precision = precision
 
     @classmethod
+    def duvi_from_device_csr(cls, ctx, n_rows, n_cols, d_rowptr, d_col, d_val, precision="f64", value_index_bits=0,
+                             dedup_tol=1e-10):
+        """DuVi matrix encoded on the device from device CSR arrays (pointers: int32 rowptr and col,
+        float64 values), the same arrays as the host encoder's."""
+        self = cls.__new__(cls)
+        h = C.c_void_p()
+        N.check(N.lib().dv_matrix_create_duvi_device(ctx.h, n_rows, n_cols, d_rowptr, d_col, d_val,
+                                                     {"f64": N.F64, "f32": N.F32}[precision], value_index_bits,
+                                                     dedup_tol, C.byref(h)))
+        self.ctx, self.h, self.shape, self.format, self.precision = ctx, h, (n_rows, n_cols), "duvi", precision
+        ctx.register(self)
+        return self
+
+    @classmethod
     def hex_operator(cls, ctx, ne, elem_E=None, scale=1.0, E=1.0, nu=0.3, precision="f64"):
         """Matrix-free structured hexahedral stiffness (format "hex"): the operator of
         hex_stiffness(ne, elem_E, scale, E, nu) applied element by element, nothing stored

@@ -163,6 +163,16 @@ DV_API int dv_units_encode(const dv_csr_host *a, double dedup_tol, int64_t *n_un
 DV_API int dv_units_decode(int32_t n_rows, int32_t n_cols, const uint8_t *bytes, int64_t n_bytes,
                            const int32_t *value_indices, int64_t n_indices, const double *values, int64_t nuniq,
                            int64_t *nnz, int32_t *rowptr, int32_t *col, double *val);
+/* The same DuVi encode of a CSR matrix that is already in device memory, run on the device:
+ * d_rowptr (n_rows + 1), d_col and d_val (nnz < 2^31) are device arrays (context stream).
+ * The arrays equal dv_matrix_create_duvi's bit for bit; the distinct values pass through the
+ * dedup_tol dictionary on the host (all values do when the tolerance makes a lookup depend on
+ * insertion time).  The node-pattern and grid-stencil layouts are derived on the device too; the
+ * lane layout is not built (matrices without node patterns run the staged kernel).  Pairs with
+ * dv_hex_assemble_device for an operator that never passes through host memory. */
+DV_API int dv_matrix_create_duvi_device(dv_context *ctx, int32_t n_rows, int32_t n_cols, const int32_t *d_rowptr,
+                                        const int32_t *d_col, const double *d_val, int32_t precision,
+                                        int32_t value_index_bits, double dedup_tol, dv_matrix **out);
 /* Upload an already encoded DuVi SoA (DuViMat8/16, :16-31). value_indices has
  * value_index_bits per entry. */
 DV_API int dv_matrix_create_duvi_soa(dv_context *ctx, int32_t n_rows, int32_t n_cols,
