@@ -115,6 +115,7 @@ _SIGNATURES = {
     "dv_pcg_destroy": (C.c_int, [_vp]),
     "dv_pcg_solve_noalloc": (C.c_int, [_vp, _vp, _vp, C.c_int32, C.c_int32, C.c_double, _P(Stats)]),
     "dv_mgpcg_create": (C.c_int, [_vp, C.c_int32, _P(CsrHost), _P(CsrHost), _P(MgpcgConfig), _P(_vp)]),
+    "dv_mgpcg_create_hex": (C.c_int, [_vp, _vp, C.c_double, C.c_double, C.c_int32, _P(MgpcgConfig), _P(_vp)]),
     "dv_mgpcg_solve": (C.c_int, [_vp, _vp, _vp, _P(Stats)]),
     "dv_mgpcg_solve_device": (C.c_int, [_vp, _vp, _vp, _P(Stats)]),
     "dv_mgpcg_omega": (C.c_int, [_vp, C.c_int32, _P(C.c_double)]),

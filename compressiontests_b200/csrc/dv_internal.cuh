@@ -339,6 +339,9 @@ bool dv_set_grid(dv_matrix *m, const DuviGridHost &Gd, const std::vector<double>
 void dv_duvi_from_device_csr(dv_matrix *m, const int32_t *rp, const int32_t *col, const double *val, int force_bits,
                              double tol);
 
+// Times the launch shapes of m's product and keeps the fastest (matrices of >= 100k rows).
+void dv_autotune(dv_matrix *m);
+
 // Matrix creation (dv_matrix.cu)
 // encoded: a DuVi encoding of a made with the same vi_bits and tol, used instead of
 // encoding again (one encoding serves matrices of both precisions).

@@ -999,10 +999,17 @@ __host__ __device__ __forceinline__ constexpr int hex_class(int i) {
 #endif
 }
 
-constexpr int kGridTX = 32, kGridTY = 8;                        // tile of groups per block (one warp per row)
-constexpr int kGridPX = kGridTX + 2, kGridPY = kGridTY + 2;     // with halo
-constexpr int kGridPlane = kGridPX * kGridPY * 3;               // staged values per plane (1020)
-constexpr int kGridLoads = (kGridPlane + 255) / 256;            // per thread (4)
+constexpr int kGridTX = 32, kGridTY = 8;   // tile of groups per block: one warp per row (of NY rows each)
+constexpr int kGridPX = kGridTX + 2;       // with halo
+template <int NY>
+struct PlaneDims {
+    static constexpr int TY = kGridTY * NY;             // tile rows
+    static constexpr int PY = TY + 2;                   // with halo
+    static constexpr int PLANE = kGridPX * PY * 3;      // staged values per plane
+    static constexpr int LOADS = (PLANE + 255) / 256;   // staging slots per thread
+};
+constexpr int kGridPlane = PlaneDims<1>::PLANE;   // 1020
+constexpr int kGridLoads = PlaneDims<1>::LOADS;   // 4
 
 template <class AT>
 struct GridCoef {
@@ -1058,6 +1065,7 @@ struct StageSrc<GatherVec<XT, AT>> {
     using ST = XT;
     static constexpr int N = 1;
     __device__ static const XT *src(const GatherVec<XT, AT> &g, int) { return g.x; }
+    template <int PLANE = kGridPlane>
     __device__ static AT value(const XT *pl, int i) { return (AT)pl[i]; }
 };
 template <class T>
@@ -1065,35 +1073,38 @@ struct StageSrc<GatherWB<T>> {
     using ST = T;
     static constexpr int N = 2;
     __device__ static const T *src(const GatherWB<T> &g, int k) { return k == 0 ? g.w : g.b; }
-    __device__ static T value(const T *pl, int i) { return pl[i] * pl[i + kGridPlane]; }
+    template <int PLANE = kGridPlane>
+    __device__ static T value(const T *pl, int i) { return pl[i] * pl[i + PLANE]; }
 };
 constexpr int kGridStages = 4;   // staged planes in flight per block (a plane is consumed 3 steps after its copy)
 
 // Staging slots of a thread: plane value k = threadIdx.x + 256 j is node (sx, sy) of the halo tile
 // (offsets from the tile's first node), dof sc; sy = -1000000 past the plane.
+template <int NY = 1>
 struct StageSlots {
-    int sx[kGridLoads], sy[kGridLoads], sc[kGridLoads];
+    static constexpr int LOADS = PlaneDims<NY>::LOADS, PLANE = PlaneDims<NY>::PLANE;
+    int sx[LOADS], sy[LOADS], sc[LOADS];
     __device__ StageSlots() {
 #pragma unroll
-        for (int j = 0; j < kGridLoads; ++j) {
+        for (int j = 0; j < LOADS; ++j) {
             const int k = threadIdx.x + 256 * j;
             const int row = k / (kGridPX * 3), col = k - row * (kGridPX * 3);
             sx[j] = col / 3 - 1;
             sc[j] = col - 3 * (col / 3);
-            sy[j] = k < kGridPlane ? row - 1 : -1000000;
+            sy[j] = k < PLANE ? row - 1 : -1000000;
         }
     }
     // per tile: offset of each slot inside a plane of the lx x ly node box (-1: outside the box)
-    __device__ void plane_offsets(int x0, int y0, int lx, int ly, int32_t (&poff)[kGridLoads]) const {
+    __device__ void plane_offsets(int x0, int y0, int lx, int ly, int32_t (&poff)[LOADS]) const {
 #pragma unroll
-        for (int j = 0; j < kGridLoads; ++j) {
+        for (int j = 0; j < LOADS; ++j) {
             const int xn = x0 + sx[j], yn = y0 + sy[j];
             poff[j] = (xn >= 0 && xn < lx && yn >= 0 && yn < ly) ? 3 * (xn + lx * yn) + sc[j] : -1;
         }
     }
     // copies plane z (zero outside 0 <= z < lz) of every source of the gather into one ring slot
     template <class SS, class Gather>
-    __device__ void issue(const Gather &g, typename SS::ST *slot, const int32_t (&poff)[kGridLoads], int z, int lz,
+    __device__ void issue(const Gather &g, typename SS::ST *slot, const int32_t (&poff)[LOADS], int z, int lz,
                           int32_t plane_len) const {
         const bool zin = z >= 0 && z < lz;
         const int32_t base = zin ? z * plane_len : 0;
@@ -1101,10 +1112,10 @@ struct StageSlots {
         for (int k = 0; k < SS::N; ++k) {
             const typename SS::ST *src = SS::src(g, k);
 #pragma unroll
-            for (int j = 0; j < kGridLoads; ++j)
+            for (int j = 0; j < LOADS; ++j)
                 if (sy[j] > -2) {
                     const bool v = zin && poff[j] >= 0;
-                    cp_async_zfill<sizeof(typename SS::ST)>(slot + k * kGridPlane + threadIdx.x + 256 * j,
+                    cp_async_zfill<sizeof(typename SS::ST)>(slot + k * PLANE + threadIdx.x + 256 * j,
                                                             v ? src + base + poff[j] : src, v);
                 }
         }
@@ -1112,29 +1123,38 @@ struct StageSlots {
     }
 };
 
-// One staged plane applied to the three accumulated groups: below (DI: group p+1 takes the
-// plane as its dz = -1 neighbours), at (DM: group p, dz = 0) and above (DF: group p-1, dz = +1).
-template <class AT, class SS, bool FUSED, bool HEX, bool SKIP0, bool DI, bool DM, bool DF>
+// One staged plane applied to the three accumulated groups of each of the thread's NY nodes
+// (rows q = 0 .. NY-1 of its column of the tile): below (DI: group p+1 takes the plane as its
+// dz = -1 neighbours), at (DM: group p, dz = 0) and above (DF: group p-1, dz = +1).  A staged
+// value of plane row r is loaded once and serves every node q with r - q in 0 .. 2.
+template <class AT, class SS, int NY, bool FUSED, bool HEX, bool SKIP0, bool DI, bool DM, bool DF>
 __device__ __forceinline__ void grid_plane_step(const typename SS::ST *__restrict__ pl, int tx, int ty,
-                                                const GridCoef<AT> &cf, AT (&a0)[3], AT (&a1)[3], AT (&a2)[3]) {
+                                                const GridCoef<AT> &cf, AT (&a0)[NY][3], AT (&a1)[NY][3],
+                                                AT (&a2)[NY][3]) {
+    constexpr int PLANE = PlaneDims<NY>::PLANE;
 #pragma unroll
-    for (int dy = 0; dy < 3; ++dy)
+    for (int r = 0; r < NY + 2; ++r)
 #pragma unroll
         for (int dx = 0; dx < 3; ++dx)
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
-                const AT v = SS::value(pl, ((ty + dy) * kGridPX + tx + dx) * 3 + c);
-                const int k = 9 * dy + 3 * dx + c;
+                const AT v = SS::template value<PLANE>(pl, ((NY * ty + r) * kGridPX + tx + dx) * 3 + c);
 #pragma unroll
-                for (int d = 0; d < 3; ++d) {
-                    if (DI) a2[d] = grid_term<AT, FUSED, HEX, SKIP0>(a2[d], cf, k, d, v);
-                    if (DM) a1[d] = grid_term<AT, FUSED, HEX, SKIP0>(a1[d], cf, 27 + k, d, v);
-                    if (DF) a0[d] = grid_term<AT, FUSED, HEX, SKIP0>(a0[d], cf, 54 + k, d, v);
+                for (int q = 0; q < NY; ++q) {
+                    const int dy = r - q;
+                    if (dy < 0 || dy > 2) continue;
+                    const int k = 9 * dy + 3 * dx + c;
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) {
+                        if (DI) a2[q][d] = grid_term<AT, FUSED, HEX, SKIP0>(a2[q][d], cf, k, d, v);
+                        if (DM) a1[q][d] = grid_term<AT, FUSED, HEX, SKIP0>(a1[q][d], cf, 27 + k, d, v);
+                        if (DF) a0[q][d] = grid_term<AT, FUSED, HEX, SKIP0>(a0[q][d], cf, 54 + k, d, v);
+                    }
                 }
             }
 }
 
-template <class AT, class Gather, class Op, bool HEX>
+template <class AT, class Gather, class Op, bool HEX, int NY>
 __global__ void __launch_bounds__(256, sizeof(AT) == 8 ? 2 : 3)
     k_duvi_grid(GridGeom G, GridCoef<AT> cf, const uint16_t *__restrict__ pid, const uint32_t *__restrict__ pstart,
                 const PatRec<AT> *__restrict__ grec, const uint32_t *__restrict__ bnode, int32_t npat, int32_t nrec,
@@ -1158,71 +1178,88 @@ __global__ void __launch_bounds__(256, sizeof(AT) == 8 ? 2 : 3)
     } else {
         using SS = StageSrc<Gather>;
         using ST = typename SS::ST;
-        constexpr int SLOT = SS::N * kGridPlane;
+        using SL = StageSlots<NY>;
+        constexpr int SLOT = SS::N * SL::PLANE;
         ST *ring = reinterpret_cast<ST *>(grid_smem);   // kGridStages slots of SS::N staged planes
         const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-        const StageSlots slots;
+        const SL slots;
         const int64_t lxy = (int64_t)G.lx * G.ly;
         const int32_t plane_len = (int32_t)(3 * lxy);
         const int nblk = (int)gridDim.x - G.bound_blocks;
         for (int t = (int)blockIdx.x - G.bound_blocks; t < G.ntile; t += nblk) {
             const int txi = t % G.ntx, tyi = (t / G.ntx) % G.nty, tzi = t / (G.ntx * G.nty);
-            const int x0 = txi * kGridTX, y0 = tyi * kGridTY, z0 = tzi * G.zc, z1 = min(G.lz, z0 + G.zc);
-            const int ix = x0 + tx, iy = y0 + ty;
-            const bool inxy = ix >= 1 && ix <= G.lx - 2 && iy >= 1 && iy <= G.ly - 2;
-            const int32_t col_xy = ix + G.lx * iy;   // group index in its plane
-            int32_t poff[kGridLoads];
+            const int x0 = txi * kGridTX, y0 = tyi * PlaneDims<NY>::TY, z0 = tzi * G.zc, z1 = min(G.lz, z0 + G.zc);
+            const int ix = x0 + tx;
+            int32_t col_xy[NY];   // group index in its plane of the thread's nodes
+            bool inxy[NY];
+#pragma unroll
+            for (int q = 0; q < NY; ++q) {
+                const int iy = y0 + NY * ty + q;
+                col_xy[q] = ix + G.lx * iy;
+                inxy[q] = ix >= 1 && ix <= G.lx - 2 && iy >= 1 && iy <= G.ly - 2;
+            }
+            int32_t poff[SL::LOADS];
             slots.plane_offsets(x0, y0, G.lx, G.ly, poff);
             // a stencil group (off the faces, interior pattern) that this thread finishes
-            auto active = [&](int z) {
-                if (!inxy || z < 1 || z > G.lz - 2) return false;
-                return G.all_hot || (int)__ldg(pid + col_xy + lxy * z) == G.hot;
+            auto active = [&](int q, int z) {
+                if (!inxy[q] || z < 1 || z > G.lz - 2) return false;
+                return G.all_hot || (int)__ldg(pid + col_xy[q] + lxy * z) == G.hot;
             };
 #pragma unroll
-            for (int q = 0; q < kGridStages - 1; ++q) {
-                if (z0 - 1 + q <= z1) slots.issue<SS>(g, ring + q * SLOT, poff, z0 - 1 + q, G.lz, plane_len);
+            for (int s2 = 0; s2 < kGridStages - 1; ++s2) {
+                if (z0 - 1 + s2 <= z1) slots.template issue<SS>(g, ring + s2 * SLOT, poff, z0 - 1 + s2, G.lz, plane_len);
                 else cp_async_commit();
             }
-            AT a0[3], a1[3], a2[3];
+            AT a0[NY][3], a1[NY][3], a2[NY][3];
+            bool act0[NY], act1[NY];
 #pragma unroll
-            for (int d = 0; d < 3; ++d) a0[d] = a1[d] = a2[d] = AT(0);
-            bool act0 = false, act1 = false, act2 = false;
+            for (int q = 0; q < NY; ++q) {
+                act0[q] = act1[q] = false;
+#pragma unroll
+                for (int d = 0; d < 3; ++d) a0[q][d] = a1[q][d] = a2[q][d] = AT(0);
+            }
             for (int p = z0 - 1, k = 0; p <= z1; ++p, ++k) {
                 cp_async_wait<kGridStages - 2>();   // plane p has landed (this thread's copies)
                 __syncthreads();                     // ... and everyone's; the slot of plane p-1 is free
                 if (p + kGridStages - 1 <= z1)
-                    slots.issue<SS>(g, ring + ((k + kGridStages - 1) % kGridStages) * SLOT, poff, p + kGridStages - 1,
-                                    G.lz, plane_len);
+                    slots.template issue<SS>(g, ring + ((k + kGridStages - 1) % kGridStages) * SLOT, poff,
+                                             p + kGridStages - 1, G.lz, plane_len);
                 else
                     cp_async_commit();
                 const ST *pl = ring + (k % kGridStages) * SLOT;
                 const bool di = p + 1 >= z0 && p + 1 < z1, dm = p >= z0 && p < z1, df = p - 1 >= z0 && p - 1 < z1;
-                if (di) {
-                    act2 = active(p + 1);
-                    const int32_t r = (int32_t)(3 * (col_xy + lxy * (p + 1)));
+                bool act2[NY];
 #pragma unroll
-                    for (int d = 0; d < 3; ++d) a2[d] = act2 ? op.init(r + d) : AT(0);
-                }
-                if (dm && act1) touch_rows(op, (int32_t)(3 * (col_xy + lxy * p)));   // finished next step
-                if (di && dm && df) grid_plane_step<AT, SS, FU, HEX, S0, true, true, true>(pl, tx, ty, cf, a0, a1, a2);
-                else if (di && dm) grid_plane_step<AT, SS, FU, HEX, S0, true, true, false>(pl, tx, ty, cf, a0, a1, a2);
-                else if (dm && df) grid_plane_step<AT, SS, FU, HEX, S0, false, true, true>(pl, tx, ty, cf, a0, a1, a2);
-                else if (di) grid_plane_step<AT, SS, FU, HEX, S0, true, false, false>(pl, tx, ty, cf, a0, a1, a2);
-                else if (dm) grid_plane_step<AT, SS, FU, HEX, S0, false, true, false>(pl, tx, ty, cf, a0, a1, a2);
-                else if (df) grid_plane_step<AT, SS, FU, HEX, S0, false, false, true>(pl, tx, ty, cf, a0, a1, a2);
-                if (df && act0) {
-                    const int32_t r = (int32_t)(3 * (col_xy + lxy * (p - 1)));
+                for (int q = 0; q < NY; ++q) {
+                    act2[q] = di && active(q, p + 1);
+                    if (di) {
+                        const int32_t r = (int32_t)(3 * (col_xy[q] + lxy * (p + 1)));
 #pragma unroll
-                    for (int d = 0; d < 3; ++d) op.row(r + d, a0[d], red);
+                        for (int d = 0; d < 3; ++d) a2[q][d] = act2[q] ? op.init(r + d) : AT(0);
+                    }
+                    if (dm && act1[q]) touch_rows(op, (int32_t)(3 * (col_xy[q] + lxy * p)));   // finished next step
                 }
+                if (di && dm && df) grid_plane_step<AT, SS, NY, FU, HEX, S0, true, true, true>(pl, tx, ty, cf, a0, a1, a2);
+                else if (di && dm) grid_plane_step<AT, SS, NY, FU, HEX, S0, true, true, false>(pl, tx, ty, cf, a0, a1, a2);
+                else if (dm && df) grid_plane_step<AT, SS, NY, FU, HEX, S0, false, true, true>(pl, tx, ty, cf, a0, a1, a2);
+                else if (di) grid_plane_step<AT, SS, NY, FU, HEX, S0, true, false, false>(pl, tx, ty, cf, a0, a1, a2);
+                else if (dm) grid_plane_step<AT, SS, NY, FU, HEX, S0, false, true, false>(pl, tx, ty, cf, a0, a1, a2);
+                else if (df) grid_plane_step<AT, SS, NY, FU, HEX, S0, false, false, true>(pl, tx, ty, cf, a0, a1, a2);
 #pragma unroll
-                for (int d = 0; d < 3; ++d) {
-                    a0[d] = a1[d];
-                    a1[d] = a2[d];
+                for (int q = 0; q < NY; ++q) {
+                    if (df && act0[q]) {
+                        const int32_t r = (int32_t)(3 * (col_xy[q] + lxy * (p - 1)));
+#pragma unroll
+                        for (int d = 0; d < 3; ++d) op.row(r + d, a0[q][d], red);
+                    }
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) {
+                        a0[q][d] = a1[q][d];
+                        a1[q][d] = a2[q][d];
+                    }
+                    act0[q] = act1[q];
+                    act1[q] = act2[q];
                 }
-                act0 = act1;
-                act1 = act2;
-                act2 = false;
             }
             cp_async_wait<0>();
             __syncthreads();   // the next tile refills the ring
@@ -1254,9 +1291,12 @@ inline int stream_run_length(int64_t plane_tiles, int lz, int64_t conc) {
 // runs of zc planes.
 template <class AT, class Gather, class Op, bool HEX>
 void launch_duvi_grid_h(const LaunchEnv &e, const dv_matrix *m, Gather g, Op op) {
-    auto kern = k_duvi_grid<AT, Gather, Op, HEX>;
+    // FP32: two nodes per thread in y (staged rows shared, per-step work amortised); FP64: one
+    // (registers)
+    constexpr int NY = sizeof(AT) == 4 ? 2 : 1;
+    auto kern = k_duvi_grid<AT, Gather, Op, HEX, NY>;
     using SS = StageSrc<Gather>;
-    const size_t smem = std::max(sizeof(typename SS::ST) * SS::N * kGridStages * (size_t)kGridPlane,
+    const size_t smem = std::max(sizeof(typename SS::ST) * SS::N * kGridStages * (size_t)PlaneDims<NY>::PLANE,
                                  sizeof(PatRec<AT>) * (size_t)m->pat_entries + 4 * ((size_t)m->pat_count + 1));
     static SmemLimit limit;   // per instantiation and device
     limit.raise(kern, smem, e.ctx->device);
@@ -1271,7 +1311,7 @@ void launch_duvi_grid_h(const LaunchEnv &e, const dv_matrix *m, Gather g, Op op)
     G.ly = m->grid_ly;
     G.lz = m->grid_lz;
     G.ntx = (G.lx + kGridTX - 1) / kGridTX;
-    G.nty = (G.ly + kGridTY - 1) / kGridTY;
+    G.nty = (G.ly + PlaneDims<NY>::TY - 1) / PlaneDims<NY>::TY;
     G.hot = m->grid_hot;
     G.all_hot = m->grid_all_hot;
     G.nbound = m->grid_nb;
@@ -1518,7 +1558,7 @@ __global__ void __launch_bounds__(256, sizeof(AT) == 8 ? 1 : 3)
 #pragma unroll
     for (int i = 0; i < (Op::NRED > 0 ? Op::NRED : 1); ++i) red[i] = 0.0;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-    const StageSlots slots;
+    const StageSlots<1> slots;
     const int64_t lxy = (int64_t)G.lx * G.ly;
     const int32_t plane_len = (int32_t)(3 * lxy), layer_len = G.ne0 * G.ne1;
     for (int t = blockIdx.x; t < G.ntile; t += gridDim.x) {
@@ -1546,7 +1586,7 @@ __global__ void __launch_bounds__(256, sizeof(AT) == 8 ? 1 : 3)
                     const bool v = lin && loff[j] >= 0;
                     cp_async_zfill<sizeof(AT)>(ld + threadIdx.x + 256 * j, v ? ef + lbase + loff[j] : ef, v);
                 }
-            slots.issue<SS>(g, ring + (k % kGridStages) * SLOT, poff, z, G.lz, plane_len);   // commits the group
+            slots.template issue<SS>(g, ring + (k % kGridStages) * SLOT, poff, z, G.lz, plane_len);   // commits the group
         };
 #pragma unroll
         for (int q = 0; q < kGridStages - 1; ++q) {

@@ -354,6 +354,8 @@ static void autotune(dv_matrix *m) {
     apply(best_v);
 }
 
+void dv_autotune(dv_matrix *m) { autotune(m); }
+
 dv_matrix *dv_matrix_build(dv_context *ctx, const dv_csr_host &a, int format, int precision, int vi_bits, double tol,
                            const DuviHost *encoded) {
     dv_ctx_check(ctx);

@@ -12,6 +12,7 @@
 #include "dv_mgpcg.cuh"
 
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <cmath>
 #include <type_traits>
@@ -430,10 +431,12 @@ extern "C" DV_API int dv_pcg_destroy(dv_pcg *s) {
 // ---------------------------------------------------------------------------
 // multigrid-preconditioned flexible CG
 // ---------------------------------------------------------------------------
+// prebuilt: operators of levels 0 .. L-2 already on the device (A[l] then only gives the shape)
 template <class T>
 static std::unique_ptr<VCycle<T>> build_vcycle(dv_context *ctx, SolverWs &ws, int32_t L, const dv_csr_host *A,
                                                const dv_csr_host *P, const dv_mgpcg_config &cfg,
-                                               std::vector<double> &omega_eff, const DuviHost *encoded0) {
+                                               std::vector<double> &omega_eff, const DuviHost *encoded0,
+                                               std::vector<std::unique_ptr<dv_matrix>> *prebuilt = nullptr) {
     auto v = std::make_unique<VCycle<T>>();
     v->ctx = ctx;
     v->nu = cfg.nu;
@@ -447,7 +450,9 @@ static std::unique_ptr<VCycle<T>> build_vcycle(dv_context *ctx, SolverWs &ws, in
         DV_REQUIRE(P[l].n_rows == A[l].n_rows && P[l].n_cols == A[l + 1].n_rows, DV_ERR_ARG,
                    "prolongation shape does not match the levels");
         lv.n = A[l].n_rows;
-        lv.A.reset(dv_matrix_build(ctx, A[l], cfg.format, prec, 0, 1e-10, l == 0 ? encoded0 : nullptr));
+        if (prebuilt) lv.A = std::move((*prebuilt)[l]);
+        else lv.A.reset(dv_matrix_build(ctx, A[l], cfg.format, prec, 0, 1e-10, l == 0 ? encoded0 : nullptr));
+        DV_REQUIRE(lv.A->n_rows == lv.n && lv.A->precision == prec, DV_ERR_ARG, "level operator does not match");
         lv.P.reset(dv_matrix_build(ctx, P[l], cfg.format, prec, 0, 1e-10));
         std::vector<int32_t> rp, ci;
         std::vector<double> va;
@@ -488,14 +493,111 @@ static std::unique_ptr<VCycle<T>> build_vcycle(dv_context *ctx, SolverWs &ws, in
     return v;
 }
 
+static void check_mgpcg_config(const dv_mgpcg_config *cfg) {
+    DV_REQUIRE(cfg->precision == DV_F64 || cfg->precision == DV_MIXED, DV_ERR_ARG, "precision must be DV_F64 or DV_MIXED");
+    DV_REQUIRE(cfg->nu >= 1 && cfg->max_iterations >= 1 && cfg->tol > 0, DV_ERR_ARG, "bad smoothing or stop parameters");
+    DV_REQUIRE(cfg->smoother >= DV_SMOOTHER_JACOBI && cfg->smoother <= DV_SMOOTHER_GS_COLOR, DV_ERR_ARG, "unknown smoother");
+}
+
+extern "C" DV_API int dv_mgpcg_create_hex(dv_context *ctx, const int32_t *ne, double E, double nu, int32_t coarse_ne,
+                                          const dv_mgpcg_config *cfg, dv_mgpcg **out) {
+    return dv_guard([&] {
+        DV_REQUIRE(ne && cfg && out, DV_ERR_ARG, "null argument");
+        check_mgpcg_config(cfg);
+        DV_REQUIRE(cfg->format == DV_FORMAT_DUVI && cfg->outer_format == DV_FORMAT_DUVI && cfg->smoother == DV_SMOOTHER_JACOBI,
+                   DV_ERR_UNSUPPORTED, "the device-built hierarchy is DuVi with the Jacobi smoother");
+        DV_REQUIRE(coarse_ne >= 1, DV_ERR_ARG, "coarse_ne must be positive");
+        dv_ctx_check(ctx);
+        cudaStream_t st = ctx->stream;
+        // levels of the factor-2 re-discretised hierarchy: element size 2^l, K_l = 2^l sum_e E Ke
+        std::vector<std::array<int32_t, 3>> dims;
+        std::array<int32_t, 3> cur = {ne[0], ne[1], ne[2]};
+        for (;;) {
+            dims.push_back(cur);
+            if (std::min(cur[0], std::min(cur[1], cur[2])) <= coarse_ne || (cur[0] | cur[1] | cur[2]) & 1) break;
+            for (auto &c : cur) c /= 2;
+        }
+        const int32_t L = (int32_t)dims.size();
+        DV_REQUIRE(L >= 2, DV_ERR_ARG, "mesh too small for a hierarchy");
+        auto s = std::make_unique<dv_mgpcg>();
+        s->ctx = ctx;
+        s->cfg = *cfg;
+        s->ws = std::make_unique<SolverWs>(ctx);
+        const int prec = cfg->precision == DV_MIXED ? DV_F32 : DV_F64;
+        std::vector<std::unique_ptr<dv_matrix>> prebuilt;
+        std::vector<dv_csr_host> Ash(L);
+        struct Owned { std::vector<int32_t> rp, ci; std::vector<double> va; };
+        std::vector<Owned> hostP(L - 1);
+        Owned coarse;
+        double scale = 1.0;
+        for (int32_t l = 0; l < L; ++l, scale *= 2.0) {
+            int32_t nr;
+            int64_t nnz;
+            int rc = dv_hex_csr_size(dims[l].data(), &nr, &nnz);
+            DV_REQUIRE(rc == DV_OK, rc, dv_last_error());
+            if (l == L - 1) {   // the coarsest level: host CSR for the dense inverse
+                coarse.rp.resize((size_t)nr + 1);
+                coarse.ci.resize(nnz);
+                coarse.va.resize(nnz);
+                rc = dv_hex_assemble(dims[l].data(), nullptr, scale, E, nu, coarse.rp.data(), coarse.ci.data(),
+                                     coarse.va.data());
+                DV_REQUIRE(rc == DV_OK, rc, dv_last_error());
+                Ash[l] = dv_csr_host{nr, nr, coarse.rp.data(), coarse.ci.data(), coarse.va.data()};
+                break;
+            }
+            DevMem rp(4 * ((size_t)nr + 1)), ci(4 * (size_t)nnz), va(8 * (size_t)nnz);
+            rc = dv_hex_assemble_device(ctx, dims[l].data(), nullptr, scale, E, nu, rp.as<int32_t>(), ci.as<int32_t>(),
+                                        va.as<double>());
+            DV_REQUIRE(rc == DV_OK, rc, dv_last_error());
+            auto build = [&](int p) {
+                auto m = std::make_unique<dv_matrix>();
+                m->ctx = ctx;
+                m->n_rows = m->n_cols = nr;
+                m->nnz = nnz;
+                m->format = DV_FORMAT_DUVI;
+                m->precision = p;
+                dv_duvi_from_device_csr(m.get(), rp.as<int32_t>(), ci.as<int32_t>(), va.as<double>(), 0, 1e-10);
+                dv_autotune(m.get());
+                return m;
+            };
+            if (l == 0) s->Aout = build(DV_F64);
+            prebuilt.push_back(build(prec));
+            Ash[l] = dv_csr_host{nr, nr, nullptr, nullptr, nullptr};
+            // trilinear prolongation to this level from the next (host CSR; small next to A)
+            int32_t pr, pc;
+            int64_t pnnz;
+            rc = dv_hex_trilinear_size(dims[l].data(), &pr, &pc, &pnnz);
+            DV_REQUIRE(rc == DV_OK, rc, dv_last_error());
+            Owned &P = hostP[l];
+            P.rp.resize((size_t)pr + 1);
+            P.ci.resize(pnnz);
+            P.va.resize(pnnz);
+            rc = dv_hex_trilinear(dims[l].data(), P.rp.data(), P.ci.data(), P.va.data());
+            DV_REQUIRE(rc == DV_OK, rc, dv_last_error());
+        }
+        std::vector<dv_csr_host> Psh(L - 1);
+        for (int32_t l = 0; l < L - 1; ++l)
+            Psh[l] = dv_csr_host{(int32_t)hostP[l].rp.size() - 1, Ash[l + 1].n_rows, hostP[l].rp.data(),
+                                 hostP[l].ci.data(), hostP[l].va.data()};
+        s->n = Ash[0].n_rows;
+        if (cfg->precision == DV_MIXED)
+            s->v32 = build_vcycle<float>(ctx, *s->ws, L, Ash.data(), Psh.data(), *cfg, s->omega_eff, nullptr, &prebuilt);
+        else
+            s->v64 = build_vcycle<double>(ctx, *s->ws, L, Ash.data(), Psh.data(), *cfg, s->omega_eff, nullptr, &prebuilt);
+        const size_t nb = 8 * (size_t)s->n;
+        s->b.alloc(nb); s->x.alloc(nb); s->r.alloc(nb); s->p.alloc(nb); s->q.alloc(nb);
+        if (cfg->precision == DV_MIXED) s->r32.alloc(4 * (size_t)s->n);
+        DV_CUDA(cudaStreamSynchronize(st));
+        *out = s.release();
+    });
+}
+
 extern "C" DV_API int dv_mgpcg_create(dv_context *ctx, int32_t L, const dv_csr_host *A, const dv_csr_host *P,
                                       const dv_mgpcg_config *cfg, dv_mgpcg **out) {
     return dv_guard([&] {
         DV_REQUIRE(A && cfg && out && L >= 1 && (L == 1 || P), DV_ERR_ARG, "null argument");
-        DV_REQUIRE(cfg->precision == DV_F64 || cfg->precision == DV_MIXED, DV_ERR_ARG, "precision must be DV_F64 or DV_MIXED");
-        DV_REQUIRE(cfg->nu >= 1 && cfg->max_iterations >= 1 && cfg->tol > 0, DV_ERR_ARG, "bad smoothing or stop parameters");
+        check_mgpcg_config(cfg);
         DV_REQUIRE(L >= 2, DV_ERR_ARG, "need at least two levels");
-        DV_REQUIRE(cfg->smoother >= DV_SMOOTHER_JACOBI && cfg->smoother <= DV_SMOOTHER_GS_COLOR, DV_ERR_ARG, "unknown smoother");
         dv_ctx_check(ctx);
         auto s = std::make_unique<dv_mgpcg>();
         s->ctx = ctx;

@@ -255,17 +255,41 @@ class MultigridPcgSolver:
         self.context = context
         ah, ka = _hosts(A_levels)
         ph, kp = _hosts(P_levels)
-        f = {"csr": N.FORMAT_CSR, "duvi": N.FORMAT_DUVI}
-        sm = {"jacobi": N.SMOOTHER_JACOBI, "gs_lex": N.SMOOTHER_GS_LEX, "gs_color": N.SMOOTHER_GS_COLOR}[smoother]
-        cfg = N.MgpcgConfig({"mixed": N.MIXED, "f64": N.F64}[precision], f[fmt], f[outer_fmt or fmt], nu, omega,
-                            {"absolute": N.OMEGA_ABSOLUTE, "spectral": N.OMEGA_SPECTRAL}[omega_mode], max_iterations,
-                            tol, iterations_per_sync, 1 if use_graphs else 0, sm)
+        cfg = self._config(precision, fmt, outer_fmt, nu, omega, omega_mode, tol, max_iterations, iterations_per_sync,
+                           use_graphs, smoother)
         h = C.c_void_p()
         N.check(N.lib().dv_mgpcg_create(context.h, len(A_levels), ah, ph, C.byref(cfg), C.byref(h)))
         del ka, kp
         self.h = h
         context.register(self)
         self.n = A_levels[0].shape[0]
+
+    @staticmethod
+    def _config(precision, fmt, outer_fmt, nu, omega, omega_mode, tol, max_iterations, iterations_per_sync, use_graphs,
+                smoother):
+        f = {"csr": N.FORMAT_CSR, "duvi": N.FORMAT_DUVI}
+        sm = {"jacobi": N.SMOOTHER_JACOBI, "gs_lex": N.SMOOTHER_GS_LEX, "gs_color": N.SMOOTHER_GS_COLOR}[smoother]
+        return N.MgpcgConfig({"mixed": N.MIXED, "f64": N.F64}[precision], f[fmt], f[outer_fmt or fmt], nu, omega,
+                             {"absolute": N.OMEGA_ABSOLUTE, "spectral": N.OMEGA_SPECTRAL}[omega_mode], max_iterations,
+                             tol, iterations_per_sync, 1 if use_graphs else 0, sm)
+
+    @classmethod
+    def from_hex(cls, context: CudaContext, ne, E=1.0, nu_poisson=0.3, coarse_ne=8, precision="mixed", nu=2,
+                 omega=2.0 / 3.0, omega_mode="spectral", tol=1e-8, max_iterations=500, iterations_per_sync=4,
+                 use_graphs=True):
+        """The solver of hex_hierarchy(ne, coarse_ne) for the uniform cantilever, with the
+        hierarchy assembled and DuVi-encoded on the device (same operators, same solves)."""
+        self = cls.__new__(cls)
+        self.context = context
+        cfg = cls._config(precision, "duvi", "duvi", nu, omega, omega_mode, tol, max_iterations, iterations_per_sync,
+                          use_graphs, "jacobi")
+        h = C.c_void_p()
+        nea = np.ascontiguousarray(ne, np.int32)
+        N.check(N.lib().dv_mgpcg_create_hex(context.h, N.ptr(nea), E, nu_poisson, coarse_ne, C.byref(cfg), C.byref(h)))
+        self.h = h
+        context.register(self)
+        self.n = 3 * int(nea[0]) * (int(nea[1]) + 1) * (int(nea[2]) + 1)
+        return self
 
     def omega(self, level):
         w = C.c_double()

@@ -308,6 +308,16 @@ typedef struct {
 
 DV_API int dv_mgpcg_create(dv_context *ctx, int32_t n_levels, const dv_csr_host *A,
                            const dv_csr_host *P, const dv_mgpcg_config *cfg, dv_mgpcg **out);
+/* The same solver for the uniform hexahedral cantilever (ne elements, modulus E, Poisson
+ * ratio nu, x = 0 face clamped), its hierarchy built on the device: the factor-2
+ * re-discretised levels K_l = 2^l sum_e E Ke down to coarse_ne elements along the shortest
+ * axis (or an odd count) are assembled by dv_hex_assemble_device and DuVi-encoded on the
+ * device; only the trilinear prolongations and the coarsest level are built on the host.
+ * The operators equal those of dv_mgpcg_create on the host-built hierarchy bit for bit, so
+ * solves match it exactly.  cfg: DuVi V-cycle and outer operators, Jacobi smoother
+ * (otherwise DV_ERR_UNSUPPORTED). */
+DV_API int dv_mgpcg_create_hex(dv_context *ctx, const int32_t *ne, double E, double nu, int32_t coarse_ne,
+                               const dv_mgpcg_config *cfg, dv_mgpcg **out);
 DV_API int dv_mgpcg_solve(dv_mgpcg *s, const double *b, double *x, dv_stats *stats);
 /* Device-resident right-hand side and solution (FP64), context stream. */
 DV_API int dv_mgpcg_solve_device(dv_mgpcg *s, const double *d_b, double *d_x, dv_stats *stats);

@@ -288,3 +288,23 @@ def test_mgpcg_chunk_lengths_do_not_change_the_iterate(ctx, native):
     for x, it in out[1:]:
         assert it == out[0][1]
         np.testing.assert_array_equal(x, out[0][0])
+
+
+@pytest.mark.parametrize("precision", ["mixed", "f64"])
+def test_mgpcg_device_built_hierarchy_equals_host_built(ctx, native, precision):
+    # dv_mgpcg_create_hex assembles and DuVi-encodes the hierarchy on the device: the operators are
+    # the host-built ones bit for bit, so the solve returns the same iterate and iteration count.
+    ne = (16, 16, 16)
+    A, P = native.hex_hierarchy(ne, coarse_ne=4)
+    b = native.traction_rhs(ne)
+    host = native.MultigridPcgSolver(ctx, A, P, precision=precision, fmt="duvi", tol=1e-10, max_iterations=200)
+    dev = native.MultigridPcgSolver.from_hex(ctx, ne, coarse_ne=4, precision=precision, tol=1e-10, max_iterations=200)
+    x_h, st_h = host.Solve(b)
+    x_d, st_d = dev.Solve(b)
+    assert st_h.HasConverged and st_d.HasConverged
+    assert st_d.NumIterationsRequired == st_h.NumIterationsRequired
+    np.testing.assert_array_equal(x_d, x_h)
+    for l in range(len(A) - 1):
+        assert dev.omega(l) == host.omega(l)
+    host.release()
+    dev.release()
