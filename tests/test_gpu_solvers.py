@@ -308,3 +308,24 @@ def test_mgpcg_device_built_hierarchy_equals_host_built(ctx, native, precision):
         assert dev.omega(l) == host.omega(l)
     host.release()
     dev.release()
+
+
+def test_slab_operator_on_device_single_rank(ctx, native, oracle):
+    # The slab layer's device path on one rank: the owned rows (all of them here) as a DuVi device
+    # matrix, the product through the C ABI, and the slab Jacobi-PCG against the oracle's PCG.
+    import torch
+    from compressiontests_b200 import slabs
+    ne = (8, 6, 7)
+    A = native.hex_stiffness(ne)
+    op = slabs.SlabOperator(ctx, A, ne, 0, 1, fmt="duvi")
+    x = np.random.default_rng(3).standard_normal(A.shape[0])
+    y = torch.empty(A.shape[0], dtype=torch.float64, device="cuda")
+    op.apply(torch.from_numpy(x).cuda(), y)
+    ref = A @ x
+    assert np.max(np.abs(y.cpu().numpy() - ref)) <= 1e-12 * np.max(np.abs(A) @ np.abs(x))
+    b = native.traction_rhs(ne)
+    xs, its, conv = slabs.slab_pcg(op, torch.from_numpy(b).cuda(), 2000, 1e-10, rel_l2=True)
+    x_ref, it_ref = oracle.pcg_jacobi(oracle.Csr.from_scipy(A), b, 2000, 1e-10, rel_l2=True)
+    assert conv and abs(its - it_ref) <= 1
+    assert rel(xs.cpu().numpy(), x_ref) < 1e-7
+    op.release()
