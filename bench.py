@@ -676,9 +676,9 @@ def batched_meshes(cb, ctx, stream, n_meshes, steps, tol):
     t = time.time()
     dims, meshes, rhs = cb.cantilever_batch(n_meshes, 8, 48, seed=20261203)
     t_build = time.time() - t
-    t = time.time()
-    s = cb.BatchedMultigridSolver(ctx, meshes, precision="mixed", fmt="duvi", nu=2, omega=2 / 3,
-                                  omega_mode="spectral", tol=tol, max_iterations=500)
+    t = time.time()   # hierarchies built in the library, finest operators matrix-free (one launch for all meshes)
+    s = cb.BatchedMultigridSolver.from_hex(ctx, dims, max_coarse_dofs=1000, precision="mixed", nu=2, omega=2 / 3,
+                                           omega_mode="spectral", tol=tol, max_iterations=500)
     t_setup = time.time() - t
     b = torch.from_numpy(np.concatenate(rhs)).cuda()
     x = torch.zeros_like(b)
@@ -716,7 +716,7 @@ def batched_meshes(cb, ctx, stream, n_meshes, steps, tol):
         one.release()
     return {"workload": f"{n_meshes} cantilevers, edge lengths U{{8..48}} per axis (seeded), unit traction, "
                         "Galerkin hierarchies to <= 1000 coarse dofs, mixed MG-PCG per mesh to "
-                        f"{tol:g}, one batched graph-captured solve",
+                        f"{tol:g}, one batched graph-captured solve, finest operators matrix-free",
             "n_dofs": int(s.n), "levels_max": info["n_levels_max"], "ms": round(ms_batch, 3),
             "iterations_max": int(its.max()), "worst_relative_residual_fp64": worst,
             "sequential_ms": round(ms_seq, 3), "sequential_iterations_max": int(max(its_seq)),

@@ -122,6 +122,8 @@ _SIGNATURES = {
     "dv_mgpcg_solve_multi": (C.c_int, [_vp, C.c_int32, _vp, _vp, _vp, _P(Stats)]),
     "dv_mgpcg_solve_multi_device": (C.c_int, [_vp, C.c_int32, _vp, _vp, _vp, _P(Stats)]),
     "dv_mgpcg_destroy": (C.c_int, [_vp]),
+    "dv_batch_create_hex": (C.c_int, [_vp, C.c_int32, _vp, C.c_double, C.c_double, C.c_int32, _P(MgpcgConfig),
+                                      _P(_vp)]),
     "dv_batch_create": (C.c_int, [_vp, C.c_int32, _vp, _vp, _vp, _P(MgpcgConfig), _P(_vp)]),
     "dv_batch_info": (C.c_int, [_vp, _P(C.c_int32), _P(C.c_int32), _P(C.c_int32)]),
     "dv_batch_omega": (C.c_int, [_vp, C.c_int32, _P(C.c_double)]),

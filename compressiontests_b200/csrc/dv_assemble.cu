@@ -136,52 +136,90 @@ extern "C" DV_API int dv_hex_assemble_device(dv_context *ctx, const int32_t *ne,
     });
 }
 
-extern "C" DV_API int dv_matrix_create_hex(dv_context *ctx, const int32_t *ne, const double *elem_E, double scale,
-                                           double E, double nu, int32_t precision, dv_matrix **out) {
-    return dv_guard([&] {
-        DV_REQUIRE(ne && out, DV_ERR_ARG, "null argument");
-        DV_REQUIRE(precision == DV_F64 || precision == DV_F32, DV_ERR_ARG, "precision must be DV_F64 or DV_F32");
-        dv_ctx_check(ctx);
-        int32_t nrows;
-        int64_t nnz;
-        const int st = dv_hex_csr_size(ne, &nrows, &nnz);
-        DV_REQUIRE(st == DV_OK, st, "bad mesh");
-        std::vector<double> ke(576);
-        dv_hex_ke(E, nu, ke.data());
-        auto m = std::make_unique<dv_matrix>();
-        bool seen[kKeClasses] = {};
-        for (int i = 0; i < 576; ++i) {
-            const int c = ke_class(i);
-            if (!seen[c]) {
-                seen[c] = true;
-                m->hex_cls[c] = ke[i];
-            } else {
-                DV_REQUIRE(ke[i] == m->hex_cls[c], DV_ERR_UNSUPPORTED, "element stiffness without the hexahedron's symmetries");
-            }
-        }
-        const int64_t nel = (int64_t)ne[0] * ne[1] * ne[2];
-        std::vector<double> f(nel);
-        for (int64_t e = 0; e < nel; ++e) f[e] = elem_E ? scale * elem_E[e] : scale;
-        m->ctx = ctx;
-        m->n_rows = m->n_cols = nrows;
-        m->nnz = nnz;
-        m->format = DV_FORMAT_HEX;
-        m->precision = precision;
-        for (int d = 0; d < 3; ++d) m->hex_ne[d] = ne[d];
-        cudaStream_t s = ctx->stream;
-        if (precision == DV_F64) {
-            m->hex_factor.alloc(8 * (size_t)nel);
-            DV_CUDA(cudaMemcpyAsync(m->hex_factor.p, f.data(), 8 * (size_t)nel, cudaMemcpyHostToDevice, s));
+// Matrix-free operator of several meshes (block-diagonal, meshes in the given order); ne holds
+// 3 element counts per mesh, elem_E (or NULL) the moduli of all meshes' elements in order.
+dv_matrix *dv_hex_operator_build(dv_context *ctx, int32_t nmesh, const int32_t *ne, const double *elem_E, double scale,
+                                 double E, double nu, int32_t precision) {
+    DV_REQUIRE(ne && nmesh >= 1, DV_ERR_ARG, "null argument");
+    DV_REQUIRE(precision == DV_F64 || precision == DV_F32, DV_ERR_ARG, "precision must be DV_F64 or DV_F32");
+    dv_ctx_check(ctx);
+    std::vector<double> ke(576);
+    dv_hex_ke(E, nu, ke.data());
+    auto m = std::make_unique<dv_matrix>();
+    bool seen[kKeClasses] = {};
+    for (int i = 0; i < 576; ++i) {
+        const int c = ke_class(i);
+        if (!seen[c]) {
+            seen[c] = true;
+            m->hex_cls[c] = ke[i];
         } else {
-            std::vector<float> f32(f.begin(), f.end());
-            m->hex_factor.alloc(4 * (size_t)nel);
-            DV_CUDA(cudaMemcpyAsync(m->hex_factor.p, f32.data(), 4 * (size_t)nel, cudaMemcpyHostToDevice, s));
-            DV_CUDA(cudaStreamSynchronize(s));
+            DV_REQUIRE(ke[i] == m->hex_cls[c], DV_ERR_UNSUPPORTED, "element stiffness without the hexahedron's symmetries");
         }
-        // diagonal: sum over the node's elements in increasing id of (scale E_e) Ke(a, a), as assembled
-        const int32_t nx = ne[0] + 1, ny = ne[1] + 1, nz = ne[2] + 1;
-        static const int vtk[8] = {0, 1, 3, 2, 4, 5, 7, 6};
-        m->host_diag.assign(nrows, 0.0);
+    }
+    // mesh table: tiles of 32 x 8 nodes over runs of z planes
+    std::vector<HexMesh> meshes(nmesh);
+    int64_t rows = 0, nnz = 0, nel = 0, tiles = 0;
+    int64_t plane_tiles_all = 0;
+    for (int32_t k = 0; k < nmesh; ++k) {
+        const int32_t *n = ne + 3 * k;
+        int32_t r;
+        int64_t z;
+        const int st = dv_hex_csr_size(n, &r, &z);
+        DV_REQUIRE(st == DV_OK, st, "bad mesh");
+        HexMesh &h = meshes[k];
+        h.ne0 = n[0];
+        h.ne1 = n[1];
+        h.ne2 = n[2];
+        h.ntx = (n[0] + kGridTX - 1) / kGridTX;
+        h.nty = (n[1] + 1 + kGridTY - 1) / kGridTY;
+        h.row0 = rows;
+        h.fac0 = nel;
+        h.pad = 0;
+        rows += r;
+        nnz += z;
+        nel += (int64_t)n[0] * n[1] * n[2];
+        plane_tiles_all += (int64_t)h.ntx * h.nty;
+    }
+    DV_REQUIRE(rows < INT32_MAX, DV_ERR_ARG, "operator exceeds int32 rows");
+    // run length: one mesh from the waves x steps model; several meshes share a run of 8 planes
+    const int64_t conc = (int64_t)ctx->num_sms * (precision == DV_F64 ? 1 : 3);
+    for (auto &h : meshes) {
+        h.zc = nmesh == 1 ? stream_run_length((int64_t)h.ntx * h.nty, h.ne2 + 1, conc) : 8;
+        h.tile0 = (int32_t)tiles;
+        tiles += (int64_t)h.ntx * h.nty * ((h.ne2 + 1 + h.zc - 1) / h.zc);
+    }
+    DV_REQUIRE(tiles < INT32_MAX, DV_ERR_ARG, "too many tiles");
+    std::vector<double> f(nel);
+    for (int64_t e = 0; e < nel; ++e) f[e] = elem_E ? scale * elem_E[e] : scale;
+    m->ctx = ctx;
+    m->n_rows = m->n_cols = (int32_t)rows;
+    m->nnz = nnz;
+    m->format = DV_FORMAT_HEX;
+    m->precision = precision;
+    for (int d = 0; d < 3; ++d) m->hex_ne[d] = ne[d];
+    m->hex_nmesh = nmesh;
+    m->hex_ntile = (int32_t)tiles;
+    cudaStream_t s = ctx->stream;
+    m->hex_meshes.alloc(sizeof(HexMesh) * meshes.size());
+    DV_CUDA(cudaMemcpyAsync(m->hex_meshes.p, meshes.data(), sizeof(HexMesh) * meshes.size(), cudaMemcpyHostToDevice, s));
+    if (precision == DV_F64) {
+        m->hex_factor.alloc(8 * (size_t)nel);
+        DV_CUDA(cudaMemcpyAsync(m->hex_factor.p, f.data(), 8 * (size_t)nel, cudaMemcpyHostToDevice, s));
+        DV_CUDA(cudaStreamSynchronize(s));
+    } else {
+        std::vector<float> f32(f.begin(), f.end());
+        m->hex_factor.alloc(4 * (size_t)nel);
+        DV_CUDA(cudaMemcpyAsync(m->hex_factor.p, f32.data(), 4 * (size_t)nel, cudaMemcpyHostToDevice, s));
+        DV_CUDA(cudaStreamSynchronize(s));
+    }
+    // diagonal: sum over the node's elements in increasing id of (scale E_e) Ke(a, a), as assembled
+    static const int vtk[8] = {0, 1, 3, 2, 4, 5, 7, 6};
+    m->host_diag.assign(rows, 0.0);
+    for (int32_t q = 0; q < nmesh; ++q) {
+        const int32_t *n = ne + 3 * q;
+        const int32_t nx = n[0] + 1, ny = n[1] + 1, nz = n[2] + 1;
+        const double *fq = f.data() + meshes[q].fac0;
+        double *dq = m->host_diag.data() + meshes[q].row0;
 #pragma omp parallel for collapse(2) schedule(static)
         for (int32_t k = 0; k < nz; ++k)
             for (int32_t j = 0; j < ny; ++j)
@@ -190,23 +228,31 @@ extern "C" DV_API int dv_matrix_create_hex(dv_context *ctx, const int32_t *ne, c
                     for (int d = 0; d < 3; ++d) {
                         double s2 = 0.0;
                         bool first = true;
-                        for (int32_t c = std::max(k - 1, 0); c <= std::min(k, ne[2] - 1); ++c)
-                            for (int32_t b = std::max(j - 1, 0); b <= std::min(j, ne[1] - 1); ++b)
-                                for (int32_t a = std::max(i - 1, 0); a <= std::min(i, ne[0] - 1); ++a) {
-                                    const int64_t e = a + (int64_t)ne[0] * (b + (int64_t)ne[1] * c);
+                        for (int32_t c = std::max(k - 1, 0); c <= std::min(k, n[2] - 1); ++c)
+                            for (int32_t b = std::max(j - 1, 0); b <= std::min(j, n[1] - 1); ++b)
+                                for (int32_t a = std::max(i - 1, 0); a <= std::min(i, n[0] - 1); ++a) {
+                                    const int64_t e = a + (int64_t)n[0] * (b + (int64_t)n[1] * c);
                                     const int la = vtk[(i - a) + 2 * (j - b) + 4 * (k - c)];
-                                    const double t = f[e] * ke[(3 * la + d) * 24 + 3 * la + d];
+                                    const double t = fq[e] * ke[(3 * la + d) * 24 + 3 * la + d];
                                     s2 = first ? t + 0.0 : t + s2;
                                     first = false;
                                 }
-                        m->host_diag[r0 + d] = s2;
+                        dq[r0 + d] = s2;
                     }
                 }
-        m->zero_diag = std::any_of(m->host_diag.begin(), m->host_diag.end(), [](double d) { return d == 0.0; });
-        m->diag.alloc(8 * (size_t)nrows);
-        DV_CUDA(cudaMemcpyAsync(m->diag.p, m->host_diag.data(), 8 * (size_t)nrows, cudaMemcpyHostToDevice, s));
-        DV_CUDA(cudaStreamSynchronize(s));
-        m->device_bytes = (int64_t)(precision == DV_F64 ? 8 : 4) * nel;
-        *out = m.release();
+    }
+    m->zero_diag = std::any_of(m->host_diag.begin(), m->host_diag.end(), [](double d) { return d == 0.0; });
+    m->diag.alloc(8 * (size_t)rows);
+    DV_CUDA(cudaMemcpyAsync(m->diag.p, m->host_diag.data(), 8 * (size_t)rows, cudaMemcpyHostToDevice, s));
+    DV_CUDA(cudaStreamSynchronize(s));
+    m->device_bytes = (int64_t)(precision == DV_F64 ? 8 : 4) * nel;
+    return m.release();
+}
+
+extern "C" DV_API int dv_matrix_create_hex(dv_context *ctx, const int32_t *ne, const double *elem_E, double scale,
+                                           double E, double nu, int32_t precision, dv_matrix **out) {
+    return dv_guard([&] {
+        DV_REQUIRE(ne && out, DV_ERR_ARG, "null argument");
+        *out = dv_hex_operator_build(ctx, 1, ne, elem_E, scale, E, nu, precision);
     });
 }

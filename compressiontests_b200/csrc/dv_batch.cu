@@ -684,6 +684,85 @@ extern "C" DV_API int dv_batch_create(dv_context *ctx, int32_t n_meshes, const i
     });
 }
 
+extern "C" DV_API int dv_batch_create_hex(dv_context *ctx, int32_t n_meshes, const int32_t *ne, double E, double nu,
+                                          int32_t max_coarse_dofs, const dv_mgpcg_config *cfg, dv_batch **out) {
+    return dv_guard([&] {
+        DV_REQUIRE(ctx && ne && cfg && out && n_meshes >= 1 && max_coarse_dofs >= 1, DV_ERR_ARG, "null argument");
+        // per mesh: the stiffness and its Galerkin hierarchy (vertex factor-2 coarsening, trilinear P)
+        std::vector<std::vector<HostCsr>> A(n_meshes), P(n_meshes);
+        for (int32_t m = 0; m < n_meshes; ++m) {
+            int32_t cur[3] = {ne[3 * m], ne[3 * m + 1], ne[3 * m + 2]};
+            HostCsr a;
+            int64_t nnz;
+            int st = dv_hex_csr_size(cur, &a.nr, &nnz);
+            DV_REQUIRE(st == DV_OK, st, dv_last_error());
+            a.nc = a.nr;
+            a.rp.resize((size_t)a.nr + 1);
+            a.ci.resize(nnz);
+            a.va.resize(nnz);
+            st = dv_hex_assemble(cur, nullptr, 1.0, E, nu, a.rp.data(), a.ci.data(), a.va.data());
+            DV_REQUIRE(st == DV_OK, st, dv_last_error());
+            A[m].push_back(std::move(a));
+            while (A[m].back().nr > max_coarse_dofs && std::max(cur[0], std::max(cur[1], cur[2])) > 1) {
+                HostCsr p, g;
+                int64_t pn;
+                st = dv_hex_trilinear_size(cur, &p.nr, &p.nc, &pn);
+                DV_REQUIRE(st == DV_OK, st, dv_last_error());
+                p.rp.resize((size_t)p.nr + 1);
+                p.ci.resize(pn);
+                p.va.resize(pn);
+                st = dv_hex_trilinear(cur, p.rp.data(), p.ci.data(), p.va.data());
+                DV_REQUIRE(st == DV_OK, st, dv_last_error());
+                const dv_csr_host av = A[m].back().view(), pv = p.view();
+                int64_t gn;
+                st = dv_galerkin_size(&av, &pv, &g.nr, &gn);
+                DV_REQUIRE(st == DV_OK, st, dv_last_error());
+                g.nc = g.nr;
+                g.rp.resize((size_t)g.nr + 1);
+                g.ci.resize(gn);
+                g.va.resize(gn);
+                st = dv_galerkin(&av, &pv, g.rp.data(), g.ci.data(), g.va.data());
+                DV_REQUIRE(st == DV_OK, st, dv_last_error());
+                P[m].push_back(std::move(p));
+                A[m].push_back(std::move(g));
+                for (auto &c : cur) c = (c + 1) / 2;
+            }
+        }
+        std::vector<std::vector<dv_csr_host>> av(n_meshes), pv(n_meshes);
+        std::vector<const dv_csr_host *> ap(n_meshes), pp(n_meshes);
+        std::vector<int32_t> nlev(n_meshes);
+        for (int32_t m = 0; m < n_meshes; ++m) {
+            for (auto &a : A[m]) av[m].push_back(a.view());
+            for (auto &p : P[m]) pv[m].push_back(p.view());
+            if (pv[m].empty()) pv[m].push_back(dv_csr_host{});
+            ap[m] = av[m].data();
+            pp[m] = pv[m].data();
+            nlev[m] = (int32_t)A[m].size();
+        }
+        dv_batch *B = nullptr;
+        int st = dv_batch_create(ctx, n_meshes, nlev.data(), ap.data(), pp.data(), cfg, &B);
+        DV_REQUIRE(st == DV_OK, st, dv_last_error());
+        std::unique_ptr<dv_batch, int (*)(dv_batch *)> guard(B, dv_batch_destroy);
+        // the finest operators applied matrix-free: the outer FP64 one over every mesh, the V-cycle's level 0
+        // over the meshes that smooth there (internal order, the block-diagonal layout of the batch)
+        const char *mf = getenv("DV_MATRIX_FREE");
+        if (!(mf && mf[0] == '0')) {
+            std::vector<int32_t> all, smoothed;
+            for (int32_t m : B->order) {
+                all.insert(all.end(), ne + 3 * m, ne + 3 * m + 3);
+                if (nlev[m] >= 2) smoothed.insert(smoothed.end(), ne + 3 * m, ne + 3 * m + 3);
+            }
+            B->Aout.reset(dv_hex_operator_build(ctx, n_meshes, all.data(), nullptr, 1.0, E, nu, DV_F64));
+            if (!smoothed.empty()) {
+                const int32_t ns = (int32_t)smoothed.size() / 3;
+                if (B->c32) B->c32->lv[0].A.reset(dv_hex_operator_build(ctx, ns, smoothed.data(), nullptr, 1.0, E, nu, DV_F32));
+                else B->c64->lv[0].A.reset(dv_hex_operator_build(ctx, ns, smoothed.data(), nullptr, 1.0, E, nu, DV_F64));
+            }
+        }
+        *out = guard.release();
+    });
+}
+
 extern "C" DV_API int dv_batch_info(const dv_batch *B, int32_t *n_rows, int32_t *n_levels_max, int32_t *n_launches_per_cycle) {
     return dv_guard([&] {
         DV_REQUIRE(B != nullptr, DV_ERR_NOT_INITIALIZED, "batch not created");

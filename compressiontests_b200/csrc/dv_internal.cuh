@@ -229,8 +229,10 @@ struct dv_matrix {
     double grid_cls[10] = {};            // its class values
     DevMem grid_bnode;                   // u32 boundary groups
     int64_t grid_nb = 0;
-    int32_t hex_ne[3] = {0, 0, 0};       // DV_FORMAT_HEX: elements per axis
-    DevMem hex_factor;                   // per-element factor scale * E_e, matrix precision
+    int32_t hex_ne[3] = {0, 0, 0};       // DV_FORMAT_HEX: elements per axis (of the first mesh)
+    DevMem hex_factor;                   // per-element factor scale * E_e, matrix precision, meshes in order
+    DevMem hex_meshes;                   // dvk::HexMesh per mesh (tiles, first row, first factor)
+    int32_t hex_nmesh = 0, hex_ntile = 0;
     double hex_cls[14] = {};             // value classes of Ke (dvk::ke_class)
     int lanes_ok = 0;          // lane layout built (host-encoded matrices)
     int lanes_stencil = 0;     // stencil mode: lanes_off holds the column offsets (int32)
@@ -339,6 +341,9 @@ bool dv_set_grid(dv_matrix *m, const DuviGridHost &Gd, const std::vector<double>
 void dv_duvi_from_device_csr(dv_matrix *m, const int32_t *rp, const int32_t *col, const double *val, int force_bits,
                              double tol);
 
+// Matrix-free hexahedral operator of nmesh meshes placed block-diagonally (dv_assemble.cu).
+dv_matrix *dv_hex_operator_build(dv_context *ctx, int32_t nmesh, const int32_t *ne, const double *elem_E, double scale,
+                                 double E, double nu, int32_t precision);
 // Times the launch shapes of m's product and keeps the fastest (matrices of >= 100k rows).
 void dv_autotune(dv_matrix *m);
 

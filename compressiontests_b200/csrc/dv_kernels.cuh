@@ -1105,9 +1105,9 @@ struct StageSlots {
     // copies plane z (zero outside 0 <= z < lz) of every source of the gather into one ring slot
     template <class SS, class Gather>
     __device__ void issue(const Gather &g, typename SS::ST *slot, const int32_t (&poff)[LOADS], int z, int lz,
-                          int32_t plane_len) const {
+                          int32_t plane_len, int64_t origin = 0) const {
         const bool zin = z >= 0 && z < lz;
-        const int32_t base = zin ? z * plane_len : 0;
+        const int64_t base = zin ? origin + (int64_t)z * plane_len : 0;
 #pragma unroll
         for (int k = 0; k < SS::N; ++k) {
             const typename SS::ST *src = SS::src(g, k);
@@ -1486,10 +1486,13 @@ struct KeCoef {
     AT cls[kKeClasses];
 };
 
-struct HexOpGeom {
-    int32_t ne0, ne1, ne2;     // elements per axis
-    int32_t lx, ly, lz;        // free-node box: lx = ne0 (x index 1..ne0), ly = ne1 + 1, lz = ne2 + 1
-    int32_t ntx, nty, zc, ntile;
+// One mesh of a (possibly batched) matrix-free operator: its element counts, the tiles it is
+// streamed in, its first tile in the launch, and where its rows and element factors start.
+struct HexMesh {
+    int32_t ne0, ne1, ne2;     // elements per axis (free-node box: ne0 x (ne1 + 1) x (ne2 + 1))
+    int32_t ntx, nty, zc;      // tiles per plane in x and y, planes per z run
+    int32_t tile0, pad;        // first tile of this mesh
+    int64_t row0, fac0;        // first row, first element factor
 };
 
 constexpr int kHexEX = kGridTX + 1, kHexEY = kGridTY + 1;   // element tile per layer (33 x 9)
@@ -1543,8 +1546,9 @@ __device__ __forceinline__ void hex_plane_step(const AT (&xv)[27], const AT *lay
 
 template <class AT, class Gather, class Op>
 __global__ void __launch_bounds__(256, sizeof(AT) == 8 ? 1 : 3)
-    k_hex_elem(HexOpGeom G, KeCoef<AT> kc, const AT *__restrict__ ef, Gather g, Op op, const int *__restrict__ done,
-               double *partials, unsigned *ticket) {
+    k_hex_elem(const HexMesh *__restrict__ meshes, int32_t nmesh, int32_t ntile, KeCoef<AT> kc,
+               const AT *__restrict__ ef_all, Gather g, Op op, const int *__restrict__ done, double *partials,
+               unsigned *ticket) {
     if (done && *(volatile const int *)done) return;
     extern __shared__ uint4 hex_smem[];
     constexpr bool FU = op_fused<Op>::value;
@@ -1559,16 +1563,26 @@ __global__ void __launch_bounds__(256, sizeof(AT) == 8 ? 1 : 3)
     for (int i = 0; i < (Op::NRED > 0 ? Op::NRED : 1); ++i) red[i] = 0.0;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     const StageSlots<1> slots;
-    const int64_t lxy = (int64_t)G.lx * G.ly;
-    const int32_t plane_len = (int32_t)(3 * lxy), layer_len = G.ne0 * G.ne1;
-    for (int t = blockIdx.x; t < G.ntile; t += gridDim.x) {
-        const int txi = t % G.ntx, tyi = (t / G.ntx) % G.nty, tzi = t / (G.ntx * G.nty);
-        const int x0 = txi * kGridTX, y0 = tyi * kGridTY, z0 = tzi * G.zc, z1 = min(G.lz, z0 + G.zc);
+    for (int t = blockIdx.x; t < ntile; t += gridDim.x) {
+        int lo = 0, hi = nmesh - 1;   // the mesh of tile t: the last with tile0 <= t
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (meshes[mid].tile0 <= t) lo = mid;
+            else hi = mid - 1;
+        }
+        const HexMesh G = meshes[lo];
+        const int32_t lx = G.ne0, ly = G.ne1 + 1, lz = G.ne2 + 1;
+        const int64_t lxy = (int64_t)lx * ly;
+        const int32_t plane_len = (int32_t)(3 * lxy), layer_len = G.ne0 * G.ne1;
+        const AT *ef = ef_all + G.fac0;
+        const int tl = t - G.tile0;
+        const int txi = tl % G.ntx, tyi = (tl / G.ntx) % G.nty, tzi = tl / (G.ntx * G.nty);
+        const int x0 = txi * kGridTX, y0 = tyi * kGridTY, z0 = tzi * G.zc, z1 = min(lz, z0 + G.zc);
         const int ix = x0 + tx, iy = y0 + ty;
-        const bool inxy = ix < G.lx && iy < G.ly;
-        const int32_t col_xy = ix + G.lx * iy;
+        const bool inxy = ix < lx && iy < ly;
+        const int64_t col_xy = G.row0 / 3 + ix + (int64_t)lx * iy;   // node index in the batch
         int32_t poff[kGridLoads], loff[kHexLayerLoads];
-        slots.plane_offsets(x0, y0, G.lx, G.ly, poff);
+        slots.plane_offsets(x0, y0, lx, ly, poff);
 #pragma unroll
         for (int j = 0; j < kHexLayerLoads; ++j) {   // element (ex, ey) of the layer tile (x index 0 is clamped)
             const int k = threadIdx.x + 256 * j;
@@ -1586,7 +1600,7 @@ __global__ void __launch_bounds__(256, sizeof(AT) == 8 ? 1 : 3)
                     const bool v = lin && loff[j] >= 0;
                     cp_async_zfill<sizeof(AT)>(ld + threadIdx.x + 256 * j, v ? ef + lbase + loff[j] : ef, v);
                 }
-            slots.template issue<SS>(g, ring + (k % kGridStages) * SLOT, poff, z, G.lz, plane_len);   // commits the group
+            slots.template issue<SS>(g, ring + (k % kGridStages) * SLOT, poff, z, lz, plane_len, G.row0);   // commits
         };
 #pragma unroll
         for (int q = 0; q < kGridStages - 1; ++q) {
@@ -1652,24 +1666,11 @@ void launch_hex_elem(const LaunchEnv &e, const dv_matrix *m, Gather g, Op op) {
                         sizeof(AT) * (kGridStages + 1) * (size_t)kHexLayer;
     static SmemLimit limit;   // per instantiation and device
     limit.raise(kern, smem, e.ctx->device);
-    static OccupancyCache occupancy;   // per instantiation
-    const int occ = occupancy.get(kern, 256, smem, e.ctx->device);
     KeCoef<AT> kc;
     for (int c = 0; c < kKeClasses; ++c) kc.cls[c] = (AT)m->hex_cls[c];
-    HexOpGeom G;
-    G.ne0 = m->hex_ne[0];
-    G.ne1 = m->hex_ne[1];
-    G.ne2 = m->hex_ne[2];
-    G.lx = G.ne0;
-    G.ly = G.ne1 + 1;
-    G.lz = G.ne2 + 1;
-    G.ntx = (G.lx + kGridTX - 1) / kGridTX;
-    G.nty = (G.ly + kGridTY - 1) / kGridTY;
-    const int64_t plane_tiles = (int64_t)G.ntx * G.nty;
-    G.zc = stream_run_length(plane_tiles, G.lz, (int64_t)e.ctx->num_sms * occ);
-    G.ntile = (int32_t)(plane_tiles * ((G.lz + G.zc - 1) / G.zc));
-    const int blocks = (int)std::min<int64_t>(G.ntile, e.max_blocks);
-    kern<<<blocks, 256, smem, e.stream>>>(G, kc, static_cast<const AT *>(m->hex_factor.p), g, op, e.done, e.partials,
+    const int blocks = (int)std::min<int64_t>(m->hex_ntile, e.max_blocks);
+    kern<<<blocks, 256, smem, e.stream>>>(m->hex_meshes.as<HexMesh>(), m->hex_nmesh, m->hex_ntile, kc,
+                                          static_cast<const AT *>(m->hex_factor.p), g, op, e.done, e.partials,
                                           e.ticket);
     DV_CUDA(cudaGetLastError());
     e.ctx->count();

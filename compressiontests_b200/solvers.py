@@ -382,6 +382,27 @@ class BatchedMultigridSolver:
         self.offsets = np.concatenate([[0], np.cumsum(self.sizes)]).astype(np.int64)
         self.n = int(self.offsets[-1])
 
+    @classmethod
+    def from_hex(cls, context: CudaContext, dims, E=1.0, nu_poisson=0.3, max_coarse_dofs=1000, precision="mixed",
+                 nu=2, omega=2.0 / 3.0, omega_mode="spectral", tol=1e-8, max_iterations=500, iterations_per_sync=4,
+                 use_graphs=True):
+        """The batch of cantilever_batch's meshes (dims: element counts per mesh) with its Galerkin
+        hierarchies built in the library and the finest operators of all meshes applied matrix-free."""
+        self = cls.__new__(cls)
+        self.context = context
+        cfg = MultigridPcgSolver._config(precision, "duvi", "duvi", nu, omega, omega_mode, tol, max_iterations,
+                                         iterations_per_sync, use_graphs, "jacobi")
+        ne = np.ascontiguousarray(np.asarray(dims, np.int32).reshape(-1))
+        h = C.c_void_p()
+        N.check(N.lib().dv_batch_create_hex(context.h, len(dims), N.ptr(ne), E, nu_poisson, max_coarse_dofs,
+                                            C.byref(cfg), C.byref(h)))
+        self.h = h
+        context.register(self)
+        self.sizes = [3 * int(d[0]) * (int(d[1]) + 1) * (int(d[2]) + 1) for d in dims]
+        self.offsets = np.concatenate([[0], np.cumsum(self.sizes)]).astype(np.int64)
+        self.n = int(self.offsets[-1])
+        return self
+
     def info(self):
         n, L, k = C.c_int32(), C.c_int32(), C.c_int32()
         N.check(N.lib().dv_batch_info(self.h, C.byref(n), C.byref(L), C.byref(k)))

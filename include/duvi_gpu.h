@@ -351,6 +351,13 @@ DV_API int dv_mgpcg_destroy(dv_mgpcg *s);
  * model (GeometricMultigridSolver.Initialize, GeometricMultigridSolver.cs:57-77). */
 DV_API int dv_batch_create(dv_context *ctx, int32_t n_meshes, const int32_t *n_levels, const dv_csr_host *const *A,
                            const dv_csr_host *const *P, const dv_mgpcg_config *cfg, dv_batch **out);
+/* The same batch for n_meshes uniform hexahedral cantilevers (ne: 3 element counts per mesh,
+ * modulus E, Poisson ratio nu, x = 0 faces clamped): each mesh's Galerkin hierarchy (vertex
+ * factor-2 coarsening, trilinear P) down to at most max_coarse_dofs dofs is built here, and the
+ * finest operators of all meshes are applied matrix-free in one launch (the element operator of
+ * dv_matrix_create_hex over a table of meshes); DV_MATRIX_FREE=0 keeps them assembled. */
+DV_API int dv_batch_create_hex(dv_context *ctx, int32_t n_meshes, const int32_t *ne, double E, double nu,
+                               int32_t max_coarse_dofs, const dv_mgpcg_config *cfg, dv_batch **out);
 /* Total fine rows, levels of the deepest mesh, kernel launches per captured chunk (0 before the first solve). */
 DV_API int dv_batch_info(const dv_batch *b, int32_t *n_rows, int32_t *n_levels_max, int32_t *n_launches_per_chunk);
 /* Effective Jacobi weight of batch level l (one weight for all meshes smoothing on that level). */

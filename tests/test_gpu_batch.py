@@ -87,3 +87,22 @@ def test_batch_iteration_limit_and_single_mesh(ctx, native, batch):
     assert conv.all()
     A = meshes[2][0][0]
     assert np.linalg.norm(rhs[2] - A @ xs[0]) / np.linalg.norm(rhs[2]) <= 1e-9
+
+
+@pytest.mark.parametrize("precision", ["mixed", "f64"])
+def test_batch_from_hex_matrix_free_finest_level(ctx, native, oracle, batch, precision):
+    # dv_batch_create_hex: the same meshes and Galerkin hierarchies built in the library, the finest
+    # operators of all meshes applied matrix-free in one launch (a table of meshes, some with a
+    # single level): every mesh's solution matches the oracle's FP64 MG-FCG solve at 1e-10.
+    meshes, rhs = batch
+    s = native.BatchedMultigridSolver.from_hex(ctx, DIMS, max_coarse_dofs=200, precision=precision, tol=1e-10,
+                                               max_iterations=300)
+    xs, st, conv, its = s.Solve(rhs)
+    assert conv.all() and st.HasConverged and st.RelativeResidual <= 1e-10
+    for m, ((A, P), b, x) in enumerate(zip(meshes, rhs, xs)):
+        assert np.linalg.norm(b - A[0] @ x) / np.linalg.norm(b) <= 1e-10, m
+        Ao = [oracle.Csr.from_scipy(a) for a in A]
+        Po = [oracle.Csr.from_scipy(p) for p in P]
+        x_ref, _, _ = oracle.mg_fcg(Ao, Po, b, 4 / (3 * 3.09), 2, 300, 1e-10)
+        assert rel(x, x_ref) < 1e-8, m
+    s.release()
