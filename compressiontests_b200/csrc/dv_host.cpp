@@ -128,6 +128,36 @@ struct BitsTable {
 // themselves, so every occurrence becomes a key).
 }  // namespace
 
+// True when none of the values could match two keys of its hash code, so that a lookup
+// returns the same key whenever it happens (the parallel numberings rely on it).
+static bool unambiguous(const NetDoubleDict &map, const double *vals, int64_t n) {
+    std::vector<std::pair<int32_t, int32_t>> ck(map.keys.size());   // (code, key) for codes held by 2+ keys
+    for (size_t k = 0; k < ck.size(); ++k) ck[k] = {map.codes[k], (int32_t)k};
+    std::sort(ck.begin(), ck.end());
+    std::vector<std::pair<int32_t, std::vector<int32_t>>> shared;
+    for (size_t k = 0; k < ck.size();) {
+        size_t e = k + 1;
+        while (e < ck.size() && ck[e].first == ck[k].first) ++e;
+        if (e - k > 1) {
+            shared.push_back({ck[k].first, {}});
+            for (size_t q = k; q < e; ++q) shared.back().second.push_back(ck[q].second);
+        }
+        k = e;
+    }
+    if (shared.empty()) return true;
+    for (int64_t i = 0; i < n; ++i) {
+        const double v = vals[i];
+        const int32_t c = map.code(v);
+        auto it = std::lower_bound(shared.begin(), shared.end(), c,
+                                   [](const std::pair<int32_t, std::vector<int32_t>> &x, int32_t y) { return x.first < y; });
+        if (it == shared.end() || it->first != c) continue;
+        int hits = 0;
+        for (int32_t k : it->second) hits += map.eq(v, map.keys[k]) ? 1 : 0;
+        if (hits > 1) return false;
+    }
+    return true;
+}
+
 std::vector<double> dv_number_values(const double *val, int64_t nnz, double tol, uint32_t *vidx) {
     auto sequential = [&] {
         NetDoubleDict map(tol);
@@ -157,32 +187,8 @@ std::vector<double> dv_number_values(const double *val, int64_t nnz, double tol,
         key[t].reserve(distinct[t].size());
         for (double v : distinct[t]) key[t].push_back((uint32_t)map.find_or_insert(v));
     }
-    // codes held by more than one key, and whether a value matches two of them
-    std::vector<std::pair<int32_t, int32_t>> ck(map.keys.size());
-    for (size_t k = 0; k < ck.size(); ++k) ck[k] = {map.codes[k], (int32_t)k};
-    std::sort(ck.begin(), ck.end());
-    std::vector<std::pair<int32_t, std::vector<int32_t>>> shared;
-    for (size_t k = 0; k < ck.size();) {
-        size_t e = k + 1;
-        while (e < ck.size() && ck[e].first == ck[k].first) ++e;
-        if (e - k > 1) {
-            shared.push_back({ck[k].first, {}});
-            for (size_t q = k; q < e; ++q) shared.back().second.push_back(ck[q].second);
-        }
-        k = e;
-    }
-    if (!shared.empty()) {
-        for (int t = 0; t < T; ++t)
-            for (double v : distinct[t]) {
-                const int32_t c = map.code(v);
-                auto it = std::lower_bound(shared.begin(), shared.end(), c,
-                                           [](const std::pair<int32_t, std::vector<int32_t>> &x, int32_t y) { return x.first < y; });
-                if (it == shared.end() || it->first != c) continue;
-                int hits = 0;
-                for (int32_t k : it->second) hits += map.eq(v, map.keys[k]) ? 1 : 0;
-                if (hits > 1) return sequential();
-            }
-    }
+    for (int t = 0; t < T; ++t)
+        if (!unambiguous(map, distinct[t].data(), (int64_t)distinct[t].size())) return sequential();
 #pragma omp parallel for schedule(static, 1)
     for (int t = 0; t < T; ++t) {
         const int64_t b = nnz * t / T, e = nnz * (t + 1) / T;
@@ -197,31 +203,7 @@ bool dv_number_distinct(const double *distinct, int64_t nd, double tol, uint32_t
         if (tol > 0 && !std::isfinite(distinct[i])) return false;
     NetDoubleDict map(tol);
     for (int64_t i = 0; i < nd; ++i) key_of[i] = (uint32_t)map.find_or_insert(distinct[i]);
-    // codes held by more than one key, and whether a value matches two of them
-    std::vector<std::pair<int32_t, int32_t>> ck(map.keys.size());
-    for (size_t k = 0; k < ck.size(); ++k) ck[k] = {map.codes[k], (int32_t)k};
-    std::sort(ck.begin(), ck.end());
-    std::vector<std::pair<int32_t, std::vector<int32_t>>> shared;
-    for (size_t k = 0; k < ck.size();) {
-        size_t e = k + 1;
-        while (e < ck.size() && ck[e].first == ck[k].first) ++e;
-        if (e - k > 1) {
-            shared.push_back({ck[k].first, {}});
-            for (size_t q = k; q < e; ++q) shared.back().second.push_back(ck[q].second);
-        }
-        k = e;
-    }
-    if (!shared.empty())
-        for (int64_t i = 0; i < nd; ++i) {
-            const double v = distinct[i];
-            const int32_t c = map.code(v);
-            auto it = std::lower_bound(shared.begin(), shared.end(), c,
-                                       [](const std::pair<int32_t, std::vector<int32_t>> &x, int32_t y) { return x.first < y; });
-            if (it == shared.end() || it->first != c) continue;
-            int hits = 0;
-            for (int32_t k : it->second) hits += map.eq(v, map.keys[k]) ? 1 : 0;
-            if (hits > 1) return false;
-        }
+    if (!unambiguous(map, distinct, nd)) return false;
     keys = std::move(map.keys);
     return true;
 }
