@@ -24,7 +24,7 @@ DV_ERR_FORMAT = -6
 DV_ERR_NO_DEVICE = -7
 DV_ERR_SINGULAR = -8
 
-FORMAT_CSR, FORMAT_DUVI, FORMAT_HEX = 0, 1, 2
+FORMAT_CSR, FORMAT_DUVI, FORMAT_HEX, FORMAT_TRILINEAR = 0, 1, 2, 3
 F64, F32, MIXED = 0, 1, 2
 SMOOTHER_JACOBI, SMOOTHER_GS_LEX, SMOOTHER_GS_COLOR = 0, 1, 2
 OMEGA_ABSOLUTE, OMEGA_SPECTRAL = 0, 1
@@ -142,6 +142,7 @@ _SIGNATURES = {
     "dv_matrix_create_duvi_device": (C.c_int, [_vp, C.c_int32, C.c_int32, _vp, _vp, _vp, C.c_int32, C.c_int32,
                                                C.c_double, _P(_vp)]),
     "dv_matrix_create_hex": (C.c_int, [_vp, _vp, _vp, C.c_double, C.c_double, C.c_double, C.c_int32, _P(_vp)]),
+    "dv_matrix_create_trilinear": (C.c_int, [_vp, _vp, C.c_int32, C.c_int32, _P(_vp)]),
     "dv_hex_assemble_device": (C.c_int, [_vp, _vp, _vp, C.c_double, C.c_double, C.c_double, _vp, _vp, _vp]),
     "dv_hex_trilinear_size": (C.c_int, [_vp, _P(C.c_int32), _P(C.c_int32), _P(C.c_int64)]),
     "dv_hex_trilinear": (C.c_int, [_vp, _vp, _vp, _vp]),

@@ -256,3 +256,34 @@ extern "C" DV_API int dv_matrix_create_hex(dv_context *ctx, const int32_t *ne, c
         *out = dv_hex_operator_build(ctx, 1, ne, elem_E, scale, E, nu, precision);
     });
 }
+
+dv_matrix *dv_trilinear_build(dv_context *ctx, const int32_t *nef, int restrict_, int32_t precision) {
+    DV_REQUIRE(nef && nef[0] >= 2 && nef[1] >= 2 && nef[2] >= 2, DV_ERR_ARG, "element counts must be >= 2");
+    DV_REQUIRE(!(nef[0] & 1) && !(nef[1] & 1) && !(nef[2] & 1), DV_ERR_UNSUPPORTED,
+               "matrix-free transfers need even element counts");
+    DV_REQUIRE(precision == DV_F64 || precision == DV_F32, DV_ERR_ARG, "precision must be DV_F64 or DV_F32");
+    dv_ctx_check(ctx);
+    int32_t nr, nc;
+    int64_t nnz;
+    const int st = dv_hex_trilinear_size(nef, &nr, &nc, &nnz);
+    DV_REQUIRE(st == DV_OK, st, "bad mesh");
+    auto m = std::make_unique<dv_matrix>();
+    m->ctx = ctx;
+    m->n_rows = restrict_ ? nc : nr;
+    m->n_cols = restrict_ ? nr : nc;
+    m->nnz = nnz;
+    m->format = DV_FORMAT_TRILINEAR;
+    m->precision = precision;
+    for (int d = 0; d < 3; ++d) m->tri_ne[d] = nef[d];
+    m->tri_restrict = restrict_ ? 1 : 0;
+    m->device_bytes = 0;
+    return m.release();
+}
+
+extern "C" DV_API int dv_matrix_create_trilinear(dv_context *ctx, const int32_t *ne_fine, int32_t restrict_,
+                                                 int32_t precision, dv_matrix **out) {
+    return dv_guard([&] {
+        DV_REQUIRE(out, DV_ERR_ARG, "null argument");
+        *out = dv_trilinear_build(ctx, ne_fine, restrict_, precision);
+    });
+}

@@ -471,9 +471,45 @@ void launch_bprod_pattern(const LaunchEnv &e, const dv_matrix *m, int kc, Gather
     else launch_bprod_pattern_u<AT, 4, EXACT, BASED, SHIFT>(e, m, kc, g, ep);
 }
 
+// Matrix-free trilinear transfer (DV_FORMAT_TRILINEAR): one thread per (node, column j), the
+// node's three rows summed from zero in column order like the stored kernels.
+template <bool RESTRICT, class AT, class Gather, class Epi>
+__global__ void __launch_bounds__(kThreads) k_bprod_tri(dvk::TriGeom G, int kc, Gather g, Epi ep,
+                                                         const int *__restrict__ done) {
+    static_assert(Epi::NC == 0, "transfers carry no reductions");
+    if (done && *(volatile const int *)done) return;
+    const int64_t work = G.nodes(RESTRICT) * kc;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < work; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t q = t / kc;
+        const int j = (int)(t - q * kc);
+        AT s[3] = {AT(0), AT(0), AT(0)};
+        dvk::tri_walk<RESTRICT, AT>(G, q, [&](uint32_t col, AT w) {
+#pragma unroll
+            for (int d = 0; d < 3; ++d) s[d] = madd<AT>(s[d], w, g(col + d, j));
+        });
+#pragma unroll
+        for (int d = 0; d < 3; ++d) ep.apply((int32_t)(3 * q + d), j, s[d], nullptr);
+    }
+}
+
 template <class AT, bool EXACT = true, class Gather, class Epi>
 void launch_bprod(const LaunchEnv &e, const dv_matrix *m, int kc, Gather g, Epi ep) {
     DV_REQUIRE(kc >= 1 && kc <= kMaxCols, DV_ERR_ARG, "block product of more than 128 columns");
+    DV_REQUIRE(m->format != DV_FORMAT_HEX, DV_ERR_UNSUPPORTED, "block products need an assembled matrix");
+    if constexpr (Epi::NC == 0) {
+        if (m->format == DV_FORMAT_TRILINEAR) {
+            const dvk::TriGeom G{m->tri_ne[0], m->tri_ne[1], m->tri_ne[2]};
+            const int64_t work = G.nodes(m->tri_restrict) * kc;
+            const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((work + kThreads - 1) / kThreads, e.max_blocks));
+            if (m->tri_restrict) k_bprod_tri<true, AT><<<blocks, kThreads, 0, e.stream>>>(G, kc, g, ep, e.done);
+            else k_bprod_tri<false, AT><<<blocks, kThreads, 0, e.stream>>>(G, kc, g, ep, e.done);
+            DV_CUDA(cudaGetLastError());
+            e.ctx->count();
+            return;
+        }
+    }
+    DV_REQUIRE(m->format == DV_FORMAT_CSR || m->format == DV_FORMAT_DUVI, DV_ERR_UNSUPPORTED,
+               "block products need an assembled matrix");
     if (m->format == DV_FORMAT_DUVI && m->pat_ok && m->lanes_group == 3) {   // node patterns, 3-row groups
         if (!m->pat_based && !m->pat_shift) {
             launch_bprod_pattern<AT, EXACT, false, false>(e, m, kc, g, ep);

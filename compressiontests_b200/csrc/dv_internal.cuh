@@ -233,6 +233,8 @@ struct dv_matrix {
     DevMem hex_factor;                   // per-element factor scale * E_e, matrix precision, meshes in order
     DevMem hex_meshes;                   // dvk::HexMesh per mesh (tiles, first row, first factor)
     int32_t hex_nmesh = 0, hex_ntile = 0;
+    int32_t tri_ne[3] = {0, 0, 0};       // DV_FORMAT_TRILINEAR: fine element counts (even)
+    int tri_restrict = 0;                // 1: restriction P^T, 0: prolongation P
     double hex_cls[14] = {};             // value classes of Ke (dvk::ke_class)
     int lanes_ok = 0;          // lane layout built (host-encoded matrices)
     int lanes_stencil = 0;     // stencil mode: lanes_off holds the column offsets (int32)
@@ -341,6 +343,9 @@ bool dv_set_grid(dv_matrix *m, const DuviGridHost &Gd, const std::vector<double>
 void dv_duvi_from_device_csr(dv_matrix *m, const int32_t *rp, const int32_t *col, const double *val, int force_bits,
                              double tol);
 
+// Trilinear prolongation (restrict = 0) or restriction (restrict = 1) of the factor-2 coarsening of
+// an even grid of ne_fine elements, applied without a matrix (dv_assemble.cu).
+dv_matrix *dv_trilinear_build(dv_context *ctx, const int32_t *ne_fine, int restrict_, int32_t precision);
 // Matrix-free hexahedral operator of nmesh meshes placed block-diagonally (dv_assemble.cu).
 dv_matrix *dv_hex_operator_build(dv_context *ctx, int32_t nmesh, const int32_t *ne, const double *elem_E, double scale,
                                  double E, double nu, int32_t precision);

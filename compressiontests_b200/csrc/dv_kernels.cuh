@@ -1676,11 +1676,105 @@ void launch_hex_elem(const LaunchEnv &e, const dv_matrix *m, Gather g, Op op) {
     e.ctx->count();
 }
 
+// ---------------------------------------------------------------------------
+// Trilinear transfers without a matrix (DV_FORMAT_TRILINEAR): the factor-2 coarsening of an even
+// structured grid (coarse nodes at the even fine nodes, x = 0 clamped), prolongation y_f = P x_c
+// (a fine node takes 1 or 2 coarse nodes per axis, weights 1 or 1/2) and restriction y_c = P^T x_f
+// (a coarse node takes the fine nodes at -1, 0, +1 per axis, weights 1/2, 1, 1/2).  Each row sums
+// its columns in increasing order with the same multiply-add rounding as a stored matrix, so the
+// products equal those of the assembled P and P^T (dv_hex_trilinear) bit for bit.
+// ---------------------------------------------------------------------------
+struct TriGeom {
+    int32_t f0, f1, f2;   // fine element counts (even)
+    __host__ __device__ int64_t nodes(bool restrict_) const {   // rows / 3
+        return restrict_ ? (int64_t)(f0 / 2) * (f1 / 2 + 1) * (f2 / 2 + 1) : (int64_t)f0 * (f1 + 1) * (f2 + 1);
+    }
+};
+
+// Calls f(first column, weight) for the coarse nodes of fine free node q (prolongation, a row of P)
+// or the fine nodes of coarse free node q (restriction, a row of P^T), in increasing column order.
+template <bool RESTRICT, class AT, class F>
+__device__ __forceinline__ void tri_walk(const TriGeom &G, int64_t q, F &&f) {
+    if constexpr (!RESTRICT) {
+        const int32_t ny = G.f1 + 1, cx = G.f0 / 2, cy = G.f1 / 2 + 1;
+        const int32_t X = (int32_t)(q % G.f0) + 1, Y = (int32_t)((q / G.f0) % ny), Z = (int32_t)(q / ((int64_t)G.f0 * ny));
+        const int nx_ = (X & 1) ? 2 : 1, ny_ = (Y & 1) ? 2 : 1, nz_ = (Z & 1) ? 2 : 1;
+        const AT w = (nx_ == 2 ? AT(0.5) : AT(1)) * (ny_ == 2 ? AT(0.5) : AT(1)) * (nz_ == 2 ? AT(0.5) : AT(1));
+        for (int c = 0; c < nz_; ++c)
+            for (int b = 0; b < ny_; ++b)
+                for (int a = 0; a < nx_; ++a) {
+                    const int32_t xc = X / 2 + a;
+                    if (xc == 0) continue;   // clamped coarse node
+                    f((uint32_t)(3 * ((xc - 1) + cx * ((int64_t)(Y / 2 + b) + cy * (int64_t)(Z / 2 + c)))), w);
+                }
+    } else {
+        const int32_t ny = G.f1 + 1, cx = G.f0 / 2, cy = G.f1 / 2 + 1;
+        const int32_t Xc = (int32_t)(q % cx) + 1, Yc = (int32_t)((q / cx) % cy), Zc = (int32_t)(q / ((int64_t)cx * cy));
+        for (int c = -1; c <= 1; ++c) {
+            const int32_t Z = 2 * Zc + c;
+            if (Z < 0 || Z > G.f2) continue;
+            for (int b = -1; b <= 1; ++b) {
+                const int32_t Y = 2 * Yc + b;
+                if (Y < 0 || Y > G.f1) continue;
+                for (int a = -1; a <= 1; ++a) {
+                    const int32_t X = 2 * Xc + a;
+                    if (X > G.f0) continue;   // X >= 1 always (Xc >= 1)
+                    const AT w = (a ? AT(0.5) : AT(1)) * (b ? AT(0.5) : AT(1)) * (c ? AT(0.5) : AT(1));
+                    f((uint32_t)(3 * ((X - 1) + G.f0 * ((int64_t)Y + ny * (int64_t)Z))), w);
+                }
+            }
+        }
+    }
+}
+
+// One thread per node: its three rows (dof d takes column d of each node).
+template <bool RESTRICT, class AT, class Gather, class Op>
+__global__ void __launch_bounds__(256) k_tri(TriGeom G, Gather g, Op op, const int *__restrict__ done,
+                                             double *partials, unsigned *ticket) {
+    if (done && *(volatile const int *)done) return;
+    constexpr bool FU = op_fused<Op>::value;
+    double red[Op::NRED > 0 ? Op::NRED : 1];
+#pragma unroll
+    for (int i = 0; i < (Op::NRED > 0 ? Op::NRED : 1); ++i) red[i] = 0.0;
+    const int64_t nodes = G.nodes(RESTRICT);
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < nodes; q += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t r0 = (int32_t)(3 * q);
+        AT s[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) s[d] = op.init(r0 + d);
+        tri_walk<RESTRICT, AT>(G, q, [&](uint32_t col, AT w) {
+#pragma unroll
+            for (int d = 0; d < 3; ++d) s[d] = madd_op<AT, FU>(s[d], w, g(col + d));
+        });
+#pragma unroll
+        for (int d = 0; d < 3; ++d) op.row(r0 + d, s[d], red);
+    }
+    if constexpr (Op::NRED > 0) {
+        double tot[Op::NRED];
+        if (grid_reduce<Op::NRED, Op::MAXMASK>(red, partials, ticket, tot)) op.finish(tot);
+    }
+}
+
+template <class AT, class Gather, class Op>
+void launch_trilinear(const LaunchEnv &e, const dv_matrix *m, Gather g, Op op) {
+    const TriGeom G{m->tri_ne[0], m->tri_ne[1], m->tri_ne[2]};
+    const int64_t nodes = m->n_rows / 3;
+    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((nodes + 255) / 256, e.max_blocks));
+    if (m->tri_restrict) k_tri<true, AT, Gather, Op><<<blocks, 256, 0, e.stream>>>(G, g, op, e.done, e.partials, e.ticket);
+    else k_tri<false, AT, Gather, Op><<<blocks, 256, 0, e.stream>>>(G, g, op, e.done, e.partials, e.ticket);
+    DV_CUDA(cudaGetLastError());
+    e.ctx->count();
+}
+
 // Runs op over every row of m with the accumulator type AT (= value precision).
 template <class AT, class Gather, class Op>
 void launch_rows(const LaunchEnv &e, const dv_matrix *m, Gather g, Op op) {
     if (m->format == DV_FORMAT_HEX) {
         launch_hex_elem<AT>(e, m, g, op);
+        return;
+    }
+    if (m->format == DV_FORMAT_TRILINEAR) {
+        launch_trilinear<AT>(e, m, g, op);
         return;
     }
     if (m->format == DV_FORMAT_DUVI && m->duvi_variant == 3) {
@@ -1762,6 +1856,30 @@ __global__ void k_dense_gemv(const T *__restrict__ a, const T *__restrict__ b, T
         for (int32_t k = lane; k < n; k += 32) s += ar[k] * __ldg(b + k);
         s = warp_sum(s);
         if (lane == 0) y[r] = s;
+    }
+}
+
+// Dense y = Ainv b with one block of 128 threads per row (the coarse solve of the MG-PCG V-cycle):
+// every row's products split over 4 warps, two partial sums per thread, a shared-memory sum.
+template <class T>
+__global__ void __launch_bounds__(128) k_dense_gemv_rows(const T *__restrict__ a, const T *__restrict__ b,
+                                                         T *__restrict__ y, int32_t n, const int *__restrict__ done) {
+    if (done && *(volatile const int *)done) return;
+    __shared__ T part[4];
+    for (int32_t r = blockIdx.x; r < n; r += gridDim.x) {
+        const T *ar = a + (size_t)r * n;
+        T s0 = 0, s1 = 0;
+        int32_t k = threadIdx.x;
+        for (; k + 128 < n; k += 256) {
+            s0 += ar[k] * __ldg(b + k);
+            s1 += ar[k + 128] * __ldg(b + k + 128);
+        }
+        if (k < n) s0 += ar[k] * __ldg(b + k);
+        T v = warp_sum(s0 + s1);
+        if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = v;
+        __syncthreads();
+        if (threadIdx.x == 0) y[r] = (part[0] + part[1]) + (part[2] + part[3]);
+        __syncthreads();
     }
 }
 

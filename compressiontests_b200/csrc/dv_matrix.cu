@@ -537,7 +537,8 @@ extern "C" DV_API int dv_matrix_get_info(const dv_matrix *m, dv_matrix_info *inf
         info->format = m->format;
         info->precision = m->precision;
         info->value_index_bits = m->format == DV_FORMAT_DUVI ? m->vi_bits : 0;
-        info->kernel_variant = m->format == DV_FORMAT_HEX ? 400 : m->format == DV_FORMAT_CSR ? m->csr_tpr
+        info->kernel_variant = m->format == DV_FORMAT_HEX ? 400 : m->format == DV_FORMAT_TRILINEAR ? 500
+                               : m->format == DV_FORMAT_CSR ? m->csr_tpr
                                : (m->duvi_variant == 3 ? 300 + m->lanes_group
                                   : m->duvi_variant == 2 ? 200 + m->lanes_group
                                   : m->duvi_variant == 1 ? 100 + m->lanes_group : m->duvi_batch);

@@ -49,7 +49,7 @@ struct VCycle {
     T *level(const LaunchEnv &e, size_t l, const T *b) {
         cudaStream_t s = e.stream;
         if (l == lv.size()) {
-            k_dense_gemv<T><<<std::max(1, std::min(nc / 8 + 1, ctx->num_sms * 8)), kThreads, 0, s>>>(
+            k_dense_gemv_rows<T><<<std::max(1, std::min(nc, ctx->num_sms * 16)), 128, 0, s>>>(
                 ainv.template as<T>(), b, xc.template as<T>(), nc, e.done);
             DV_CUDA(cudaGetLastError());
             ctx->count();

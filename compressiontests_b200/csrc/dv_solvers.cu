@@ -431,12 +431,15 @@ extern "C" DV_API int dv_pcg_destroy(dv_pcg *s) {
 // ---------------------------------------------------------------------------
 // multigrid-preconditioned flexible CG
 // ---------------------------------------------------------------------------
-// prebuilt: operators of levels 0 .. L-2 already on the device (A[l] then only gives the shape)
+// prebuilt: operators of levels 0 .. L-2 already on the device (A[l] then only gives the shape).
+// tri: element counts of levels 0 .. L-2 (all even); the transfers are then the matrix-free
+// trilinear ones (P[l] only gives the shape).
 template <class T>
 static std::unique_ptr<VCycle<T>> build_vcycle(dv_context *ctx, SolverWs &ws, int32_t L, const dv_csr_host *A,
                                                const dv_csr_host *P, const dv_mgpcg_config &cfg,
                                                std::vector<double> &omega_eff, const DuviHost *encoded0,
-                                               std::vector<std::unique_ptr<dv_matrix>> *prebuilt = nullptr) {
+                                               std::vector<std::unique_ptr<dv_matrix>> *prebuilt = nullptr,
+                                               const std::array<int32_t, 3> *tri = nullptr) {
     auto v = std::make_unique<VCycle<T>>();
     v->ctx = ctx;
     v->nu = cfg.nu;
@@ -453,12 +456,18 @@ static std::unique_ptr<VCycle<T>> build_vcycle(dv_context *ctx, SolverWs &ws, in
         if (prebuilt) lv.A = std::move((*prebuilt)[l]);
         else lv.A.reset(dv_matrix_build(ctx, A[l], cfg.format, prec, 0, 1e-10, l == 0 ? encoded0 : nullptr));
         DV_REQUIRE(lv.A->n_rows == lv.n && lv.A->precision == prec, DV_ERR_ARG, "level operator does not match");
-        lv.P.reset(dv_matrix_build(ctx, P[l], cfg.format, prec, 0, 1e-10));
-        std::vector<int32_t> rp, ci;
-        std::vector<double> va;
-        dv_csr_transpose(P[l], rp, ci, va);
-        dv_csr_host rt{P[l].n_cols, P[l].n_rows, rp.data(), ci.data(), va.data()};
-        lv.R.reset(dv_matrix_build(ctx, rt, cfg.format, prec, 0, 1e-10));
+        if (tri) {
+            lv.P.reset(dv_trilinear_build(ctx, tri[l].data(), 0, prec));
+            lv.R.reset(dv_trilinear_build(ctx, tri[l].data(), 1, prec));
+            DV_REQUIRE(lv.P->n_rows == P[l].n_rows && lv.P->n_cols == P[l].n_cols, DV_ERR_ARG, "transfer shape mismatch");
+        } else {
+            lv.P.reset(dv_matrix_build(ctx, P[l], cfg.format, prec, 0, 1e-10));
+            std::vector<int32_t> rp, ci;
+            std::vector<double> va;
+            dv_csr_transpose(P[l], rp, ci, va);
+            dv_csr_host rt{P[l].n_cols, P[l].n_rows, rp.data(), ci.data(), va.data()};
+            lv.R.reset(dv_matrix_build(ctx, rt, cfg.format, prec, 0, 1e-10));
+        }
         for (double d : lv.A->host_diag) DV_REQUIRE(d != 0.0, DV_ERR_SINGULAR, "zero diagonal entry");
         double om = cfg.omega;
         if (cfg.omega_mode == DV_OMEGA_SPECTRAL) {
@@ -527,8 +536,11 @@ extern "C" DV_API int dv_mgpcg_create_hex(dv_context *ctx, const int32_t *ne, do
         std::vector<std::unique_ptr<dv_matrix>> prebuilt;
         std::vector<dv_csr_host> Ash(L);
         struct Owned { std::vector<int32_t> rp, ci; std::vector<double> va; };
-        std::vector<Owned> hostP(L - 1);
+        std::vector<Owned> hostP(L - 1);   // empty with matrix-free transfers
+        std::vector<std::array<int32_t, 2>> pshape(L - 1);
         Owned coarse;
+        const char *mft = getenv("DV_MATRIX_FREE_TRANSFERS");
+        const bool free_transfers = !(mft && mft[0] == '0');
         double scale = 1.0;
         for (int32_t l = 0; l < L; ++l, scale *= 2.0) {
             int32_t nr;
@@ -563,11 +575,14 @@ extern "C" DV_API int dv_mgpcg_create_hex(dv_context *ctx, const int32_t *ne, do
             if (l == 0) s->Aout = build(DV_F64);
             prebuilt.push_back(build(prec));
             Ash[l] = dv_csr_host{nr, nr, nullptr, nullptr, nullptr};
-            // trilinear prolongation to this level from the next (host CSR; small next to A)
+            // trilinear prolongation to this level from the next: matrix-free, or host CSR when
+            // DV_MATRIX_FREE_TRANSFERS=0 (A/B comparisons)
             int32_t pr, pc;
             int64_t pnnz;
             rc = dv_hex_trilinear_size(dims[l].data(), &pr, &pc, &pnnz);
             DV_REQUIRE(rc == DV_OK, rc, dv_last_error());
+            pshape[l] = {pr, pc};
+            if (free_transfers) continue;
             Owned &P = hostP[l];
             P.rp.resize((size_t)pr + 1);
             P.ci.resize(pnnz);
@@ -577,13 +592,13 @@ extern "C" DV_API int dv_mgpcg_create_hex(dv_context *ctx, const int32_t *ne, do
         }
         std::vector<dv_csr_host> Psh(L - 1);
         for (int32_t l = 0; l < L - 1; ++l)
-            Psh[l] = dv_csr_host{(int32_t)hostP[l].rp.size() - 1, Ash[l + 1].n_rows, hostP[l].rp.data(),
-                                 hostP[l].ci.data(), hostP[l].va.data()};
+            Psh[l] = dv_csr_host{pshape[l][0], pshape[l][1], hostP[l].rp.data(), hostP[l].ci.data(), hostP[l].va.data()};
         s->n = Ash[0].n_rows;
+        const std::array<int32_t, 3> *tri = free_transfers ? dims.data() : nullptr;
         if (cfg->precision == DV_MIXED)
-            s->v32 = build_vcycle<float>(ctx, *s->ws, L, Ash.data(), Psh.data(), *cfg, s->omega_eff, nullptr, &prebuilt);
+            s->v32 = build_vcycle<float>(ctx, *s->ws, L, Ash.data(), Psh.data(), *cfg, s->omega_eff, nullptr, &prebuilt, tri);
         else
-            s->v64 = build_vcycle<double>(ctx, *s->ws, L, Ash.data(), Psh.data(), *cfg, s->omega_eff, nullptr, &prebuilt);
+            s->v64 = build_vcycle<double>(ctx, *s->ws, L, Ash.data(), Psh.data(), *cfg, s->omega_eff, nullptr, &prebuilt, tri);
         const size_t nb = 8 * (size_t)s->n;
         s->b.alloc(nb); s->x.alloc(nb); s->r.alloc(nb); s->p.alloc(nb); s->q.alloc(nb);
         if (cfg->precision == DV_MIXED) s->r32.alloc(4 * (size_t)s->n);

@@ -15,7 +15,6 @@ static void spmm(dv_matrix *m, int32_t k, const T *X, T *Y, int clear) {
 extern "C" DV_API int dv_spmm_device(dv_matrix *m, int32_t k, const void *X, void *Y, int32_t vprec, int32_t clear) {
     return dv_guard([&] {
         DV_REQUIRE(m && X && Y && k >= 1, DV_ERR_ARG, "null argument or k < 1");
-        DV_REQUIRE(m->format != DV_FORMAT_HEX, DV_ERR_UNSUPPORTED, "block products need an assembled matrix");
         dv_ctx_check(m->ctx);
         if (m->precision == DV_F64) {
             DV_REQUIRE(vprec == DV_F64, DV_ERR_ARG, "FP64 matrix needs FP64 vectors");

@@ -119,6 +119,23 @@ class SparseMatrix:
         return self
 
     @classmethod
+    def trilinear_transfer(cls, ctx, ne_fine, restriction=False, precision="f64"):
+        """Matrix-free trilinear transfer of an even structured grid (format "trilinear"): the
+        prolongation hex_trilinear(ne_fine) or, with restriction=True, its transpose, applied
+        without storing the matrix (same products bit for bit)."""
+        self = cls.__new__(cls)
+        nea = np.ascontiguousarray(ne_fine, np.int32)
+        h = C.c_void_p()
+        N.check(N.lib().dv_matrix_create_trilinear(ctx.h, N.ptr(nea), int(bool(restriction)),
+                                                   {"f64": N.F64, "f32": N.F32}[precision], C.byref(h)))
+        nf = 3 * int(nea[0]) * (int(nea[1]) + 1) * (int(nea[2]) + 1)
+        nc = 3 * (int(nea[0]) // 2) * (int(nea[1]) // 2 + 1) * (int(nea[2]) // 2 + 1)
+        self.ctx, self.h, self.format, self.precision = ctx, h, "trilinear", precision
+        self.shape = (nc, nf) if restriction else (nf, nc)
+        ctx.register(self)
+        return self
+
+    @classmethod
     def from_duvi_soa(cls, ctx, n_rows, n_cols, arrays, precision="f64"):
         """Upload pre-encoded DuVi arrays (row_to_col, row_to_dist, col_idx, dist, vidx, values, vi_bits)."""
         self = cls.__new__(cls)

@@ -52,7 +52,9 @@ enum {
     DV_ERR_SINGULAR = -8
 };
 
-enum { DV_FORMAT_CSR = 0, DV_FORMAT_DUVI = 1, DV_FORMAT_HEX = 2 };
+/* DV_FORMAT_HEX: matrix-free hexahedral operator (dv_matrix_create_hex); DV_FORMAT_TRILINEAR:
+ * matrix-free trilinear transfer of a structured grid (dv_matrix_create_trilinear). */
+enum { DV_FORMAT_CSR = 0, DV_FORMAT_DUVI = 1, DV_FORMAT_HEX = 2, DV_FORMAT_TRILINEAR = 3 };
 enum { DV_F64 = 0, DV_F32 = 1, DV_MIXED = 2 };
 enum { DV_SMOOTHER_JACOBI = 0, DV_SMOOTHER_GS_LEX = 1, DV_SMOOTHER_GS_COLOR = 2 };
 enum { DV_TOL_ABS_MAX = 0, DV_TOL_REL_L2 = 1 };
@@ -192,6 +194,13 @@ DV_API int dv_matrix_create_duvi_soa(dv_context *ctx, int32_t n_rows, int32_t n_
  * matrix-free counterpart. */
 DV_API int dv_matrix_create_hex(dv_context *ctx, const int32_t *ne, const double *elem_E, double scale, double E,
                                 double nu, int32_t precision, dv_matrix **out);
+/* The trilinear prolongation of dv_hex_trilinear (restrict = 0; fine free x coarse free) or its
+ * transpose, the restriction (restrict = 1), for an even grid of ne_fine elements, applied without
+ * storing the matrix; products equal the assembled matrix's bit for bit (same column order and
+ * rounding).  Replaces the transfer matrices of IGeometricMultigridModel.cs:76-194 on structured
+ * grids.  Odd element counts: DV_ERR_UNSUPPORTED. */
+DV_API int dv_matrix_create_trilinear(dv_context *ctx, const int32_t *ne_fine, int32_t restrict_, int32_t precision,
+                                      dv_matrix **out);
 DV_API int dv_matrix_get_info(const dv_matrix *m, dv_matrix_info *info);
 /* Copy the DuVi arrays back (value indices widened to uint32). */
 DV_API int dv_matrix_export_duvi(const dv_matrix *m, uint32_t *row_to_col, uint32_t *row_to_dist,

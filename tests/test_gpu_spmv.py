@@ -439,3 +439,31 @@ def test_matrix_free_hex_operator(ctx, native, rng, ne, moduli):
     assert rowwise_rel(_device_product(ctx, F, x, np.float32).astype(np.float64), ref, A, x) <= REL32
     with pytest.raises(native.DuviError):
         H.multiply_many_device(2, dx.data_ptr(), dr.data_ptr(), "f64")
+
+
+@pytest.mark.parametrize("ne", [(2, 2, 2), (8, 6, 6), (16, 10, 14), (4, 8, 2)])
+def test_matrix_free_trilinear_transfers_bit_exact(ctx, native, oracle, rng, ne):
+    # Format "trilinear" applies the prolongation P = hex_trilinear(ne) and the restriction P^T
+    # from the grid indices alone, summing each row's columns in increasing order with the
+    # stored kernels' multiply-add: FP64 products equal the oracle's walk of the assembled
+    # matrix bit for bit, FP32 products equal the FP32 DuVi kernel's, and block products
+    # equal the oracle column by column.
+    P = native.hex_trilinear(ne)
+    P.sort_indices()
+    for restriction, M0 in ((False, P), (True, P.T.tocsr())):
+        M0.sort_indices()
+        T = native.SparseMatrix.trilinear_transfer(ctx, ne, restriction=restriction)
+        assert T.shape == M0.shape
+        assert T.info()["kernel_variant"] == 500 and T.info()["format"] == 3
+        x = rng.standard_normal(M0.shape[1])
+        ref = oracle.DuVi(oracle.Csr.from_scipy(M0))
+        np.testing.assert_array_equal(T.Multiply(x), ref.spmv(x))
+        T32 = native.SparseMatrix.trilinear_transfer(ctx, ne, restriction=restriction, precision="f32")
+        D32 = native.SparseMatrix(ctx, M0, "duvi", "f32")
+        np.testing.assert_array_equal(_device_product(ctx, T32, x, np.float32), _device_product(ctx, D32, x, np.float32))
+        X = rng.standard_normal((M0.shape[1], 5))
+        Y = _spmm(native, T, X, np.float64)
+        for j in range(5):
+            np.testing.assert_array_equal(Y[:, j], ref.spmv(X[:, j]))
+    with pytest.raises(native.DuviError):
+        native.SparseMatrix.trilinear_transfer(ctx, (8, 7, 6))
