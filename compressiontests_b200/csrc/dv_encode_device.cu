@@ -138,28 +138,44 @@ __global__ void k_diag(const int32_t *__restrict__ rp, const int32_t *__restrict
 
 // ---- node patterns -------------------------------------------------------------
 // groups of 3 rows with one column list; bad[0] set otherwise
-__global__ void k_group_check(const int32_t *__restrict__ rp, const int32_t *__restrict__ col, int64_t ng,
+// groups of 3 rows with one column list: row d's columns equal row 0's plus shift * d
+// (shift 1: the trilinear transfers, component d coupling to component d); bad[0] set otherwise
+__global__ void k_group_check(const int32_t *__restrict__ rp, const int32_t *__restrict__ col, int64_t ng, int shift,
                               int *__restrict__ bad) {
     for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < ng; g += (int64_t)gridDim.x * blockDim.x) {
         const int32_t r0 = (int32_t)(3 * g);
         const int32_t len = rp[r0 + 1] - rp[r0];
         bool ok = rp[r0 + 2] - rp[r0 + 1] == len && rp[r0 + 3] - rp[r0 + 2] == len;
         for (int32_t e = 0; ok && e < len; ++e)
-            ok = col[rp[r0 + 1] + e] == col[rp[r0] + e] && col[rp[r0 + 2] + e] == col[rp[r0] + e];
+            ok = col[rp[r0 + 1] + e] == col[rp[r0] + e] + shift && col[rp[r0 + 2] + e] == col[rp[r0] + e] + 2 * shift;
         if (!ok) atomicOr(bad, 1);
     }
 }
+// the column the offsets of group g count from: its first row (square, unshifted operators) or
+// its first column (0 for an empty group), as in the host builder
+__device__ __forceinline__ int64_t group_origin(const int32_t *__restrict__ rp, const int32_t *__restrict__ col, int64_t g,
+                                                bool based) {
+    const int32_t r0 = (int32_t)(3 * g);
+    if (!based) return r0;
+    return rp[r0 + 1] > rp[r0] ? col[rp[r0]] : 0;
+}
+__global__ void k_group_base(const int32_t *__restrict__ rp, const int32_t *__restrict__ col, int64_t ng,
+                             uint32_t *__restrict__ base) {
+    for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < ng; g += (int64_t)gridDim.x * blockDim.x)
+        base[g] = (uint32_t)group_origin(rp, col, g, true);
+}
 // signature of a group: the host builder's FNV-1a hash of its entry count and, per entry, the
-// column offset from the group's first row and the 3 value indices
+// column offset from the group's origin and the 3 value indices
 __global__ void k_group_sig(const int32_t *__restrict__ rp, const int32_t *__restrict__ col,
-                            const uint32_t *__restrict__ vidx, int64_t ng, unsigned long long *__restrict__ sig,
-                            uint32_t *__restrict__ gid) {
+                            const uint32_t *__restrict__ vidx, int64_t ng, int based,
+                            unsigned long long *__restrict__ sig, uint32_t *__restrict__ gid) {
     for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < ng; g += (int64_t)gridDim.x * blockDim.x) {
         const int32_t r0 = (int32_t)(3 * g);
+        const int64_t b0 = group_origin(rp, col, g, based);
         const int32_t len = rp[r0 + 1] - rp[r0];
         unsigned long long x = 1469598103934665603ull ^ (unsigned long long)(4 * (int64_t)len);
         for (int32_t e = 0; e < len; ++e) {
-            x = (x ^ (unsigned long long)(int64_t)(col[rp[r0] + e] - r0)) * 1099511628211ull;
+            x = (x ^ (unsigned long long)((int64_t)col[rp[r0] + e] - b0)) * 1099511628211ull;
             for (int d = 0; d < 3; ++d) x = (x ^ (unsigned long long)vidx[rp[r0 + d] + e]) * 1099511628211ull;
         }
         sig[g] = x;
@@ -169,13 +185,15 @@ __global__ void k_group_sig(const int32_t *__restrict__ rp, const int32_t *__res
 // every group equal to its pattern's first group, entry by entry; bad[0] set otherwise
 __global__ void k_group_verify(const int32_t *__restrict__ rp, const int32_t *__restrict__ col,
                                const uint32_t *__restrict__ vidx, const uint16_t *__restrict__ pid,
-                               const uint32_t *__restrict__ rep, int64_t ng, int *__restrict__ bad) {
+                               const uint32_t *__restrict__ rep, int64_t ng, int based, int *__restrict__ bad) {
     for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < ng; g += (int64_t)gridDim.x * blockDim.x) {
-        const int32_t r0 = (int32_t)(3 * g), q0 = (int32_t)(3 * (int64_t)rep[pid[g]]);
+        const int64_t q = rep[pid[g]];
+        const int32_t r0 = (int32_t)(3 * g), q0 = (int32_t)(3 * q);
+        const int64_t b0 = group_origin(rp, col, g, based), c0 = group_origin(rp, col, q, based);
         const int32_t len = rp[r0 + 1] - rp[r0];
         bool ok = rp[q0 + 1] - rp[q0] == len;
         for (int32_t e = 0; ok && e < len; ++e) {
-            ok = col[rp[r0] + e] - r0 == col[rp[q0] + e] - q0;
+            ok = (int64_t)col[rp[r0] + e] - b0 == (int64_t)col[rp[q0] + e] - c0;
             for (int d = 0; d < 3 && ok; ++d) ok = vidx[rp[r0 + d] + e] == vidx[rp[q0 + d] + e];
         }
         if (!ok) atomicOr(bad, 1);
@@ -385,21 +403,29 @@ void dv_duvi_from_device_csr(dv_matrix *m, const int32_t *rp, const int32_t *col
     }
     const size_t vs = m->precision == DV_F64 ? 8 : 4;
     m->device_bytes = (int64_t)(nnz * (1 + bits / 8) + 4 * (int64_t)nblocks + 8 * ((int64_t)n + 1) + vs * nu);
-    // node patterns: square, groups of 3 rows with one column list, at most 1024 patterns
+    // node patterns: groups of 3 rows with one column list (shifted by the row's index in the
+    // group for the transfers), at most 1024 patterns; offsets from the group's first row on square
+    // unshifted operators, else from its first column
     const char *pe = getenv("DV_PATTERNS");
-    if ((pe && pe[0] == '0') || n != m->n_cols || n % 3 != 0 || n == 0) return;
+    if ((pe && pe[0] == '0') || n % 3 != 0 || n == 0) return;
     const int64_t ng = n / 3;
     DevMem bad(16);
+    int hbad = 0, shift = -1;
+    for (int sh : {0, 1}) {
+        DV_CUDA(cudaMemsetAsync(bad.p, 0, 16, s));
+        k_group_check<<<blocks_for(ng, ctx), kT, 0, s>>>(rp, col, ng, sh, bad.as<int>());
+        DV_CUDA(cudaGetLastError());
+        DV_CUDA(cudaMemcpyAsync(&hbad, bad.p, 4, cudaMemcpyDeviceToHost, s));
+        DV_CUDA(cudaStreamSynchronize(s));
+        if (!hbad) { shift = sh; break; }
+    }
+    if (shift < 0) return;
+    const int based = shift || n != m->n_cols;
     DV_CUDA(cudaMemsetAsync(bad.p, 0, 16, s));
-    k_group_check<<<blocks_for(ng, ctx), kT, 0, s>>>(rp, col, ng, bad.as<int>());
-    DV_CUDA(cudaGetLastError());
-    int hbad = 0;
-    DV_CUDA(cudaMemcpyAsync(&hbad, bad.p, 4, cudaMemcpyDeviceToHost, s));
-    DV_CUDA(cudaStreamSynchronize(s));
-    if (hbad) return;
     using K = unsigned long long;
     DevMem sig(8 * (size_t)ng), gid(4 * (size_t)ng), sig_s(8 * (size_t)ng), gid_s(4 * (size_t)ng);
-    k_group_sig<<<blocks_for(ng, ctx), kT, 0, s>>>(rp, col, vidx32.as<uint32_t>(), ng, sig.as<K>(), gid.as<uint32_t>());
+    k_group_sig<<<blocks_for(ng, ctx), kT, 0, s>>>(rp, col, vidx32.as<uint32_t>(), ng, based, sig.as<K>(),
+                                                   gid.as<uint32_t>());
     DV_CUDA(cudaGetLastError());
     sort_pairs<K, uint32_t>(s, sig.as<K>(), sig_s.as<K>(), gid.as<uint32_t>(), gid_s.as<uint32_t>(), ng, 64);
     Runs R;
@@ -414,7 +440,7 @@ void dv_duvi_from_device_csr(dv_matrix *m, const int32_t *rp, const int32_t *col
     DV_CUDA(cudaGetLastError());
     // R.first_sorted[p] = the first group of pattern p
     k_group_verify<<<blocks_for(ng, ctx), kT, 0, s>>>(rp, col, vidx32.as<uint32_t>(), pid.as<uint16_t>(),
-                                                      R.first_sorted.as<uint32_t>(), ng, bad.as<int>());
+                                                      R.first_sorted.as<uint32_t>(), ng, based, bad.as<int>());
     DV_CUDA(cudaGetLastError());
     DV_CUDA(cudaMemcpyAsync(&hbad, bad.p, 4, cudaMemcpyDeviceToHost, s));
     DV_CUDA(cudaStreamSynchronize(s));
@@ -429,6 +455,7 @@ void dv_duvi_from_device_csr(dv_matrix *m, const int32_t *rp, const int32_t *col
     P.start.assign(1, 0);
     for (int64_t p = 0; p < npat; ++p) {
         const int32_t r0 = (int32_t)(3 * (int64_t)rep[p]);
+        int64_t b0 = r0;
         DV_CUDA(cudaMemcpyAsync(hrp.data(), rp + r0, 16, cudaMemcpyDeviceToHost, s));
         DV_CUDA(cudaStreamSynchronize(s));
         const int32_t len = hrp[1] - hrp[0];
@@ -441,8 +468,9 @@ void dv_duvi_from_device_csr(dv_matrix *m, const int32_t *rp, const int32_t *col
                                         cudaMemcpyDeviceToHost, s));
             DV_CUDA(cudaStreamSynchronize(s));
         }
+        if (based) b0 = len ? c[0] : 0;
         for (int32_t e = 0; e < len; ++e) {
-            P.off.push_back(c[e] - r0);
+            P.off.push_back((int32_t)(c[e] - b0));
             for (int d = 0; d < 3; ++d) P.vi.push_back(v[(size_t)d * len + e]);
         }
         P.start.push_back((uint32_t)P.off.size());
@@ -450,7 +478,14 @@ void dv_duvi_from_device_csr(dv_matrix *m, const int32_t *rp, const int32_t *col
     const int rec_bytes = m->precision == DV_F64 ? 32 : 16;
     if ((int64_t)P.off.size() > (96 * 1024) / rec_bytes) return;
     P.ok = 1;
+    P.shift = shift;
+    P.based = based;   // the per-group origins stay on the device (k_group_base)
     dv_upload_patterns(m, P, keys, s);
+    if (based) {
+        m->pat_base.alloc(4 * (size_t)ng);
+        k_group_base<<<blocks_for(ng, ctx), kT, 0, s>>>(rp, col, ng, m->pat_base.as<uint32_t>());
+        DV_CUDA(cudaGetLastError());
+    }
     m->pat_id = std::move(pid);
     m->lanes_group = 3;
     m->row_group = 3;
