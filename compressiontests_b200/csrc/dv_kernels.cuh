@@ -1155,7 +1155,7 @@ __device__ __forceinline__ void grid_plane_step(const typename SS::ST *__restric
 }
 
 template <class AT, class Gather, class Op, bool HEX, int NY>
-__global__ void __launch_bounds__(256, sizeof(AT) == 8 ? 2 : 3)
+__global__ void __launch_bounds__(256, 3)   // 3 blocks an SM: FP64 fits 80 registers without spills
     k_duvi_grid(GridGeom G, GridCoef<AT> cf, const uint16_t *__restrict__ pid, const uint32_t *__restrict__ pstart,
                 const PatRec<AT> *__restrict__ grec, const uint32_t *__restrict__ bnode, int32_t npat, int32_t nrec,
                 Gather g, Op op, const int *__restrict__ done, double *partials, unsigned *ticket) {
