@@ -1020,7 +1020,7 @@ struct GridCoef {
 struct GridGeom {
     int32_t lx, ly, lz;        // group box
     int32_t ntx, nty, zc;      // tiles per plane in x and y, planes per z run
-    int32_t ntile;             // ntx * nty * ceil(lz / zc)
+    int32_t ntile;             // ntx * nty * ceil((lz - 2) / zc): tiles over the interior nodes
     int32_t bound_blocks;      // blocks [0, bound_blocks) run the boundary list, the rest the tiles
     int32_t hot, all_hot;      // interior pattern id; 1 when no interior group has another pattern
     int64_t nbound;
@@ -1188,7 +1188,9 @@ __global__ void __launch_bounds__(256, 3)   // 3 blocks an SM: FP64 fits 80 regi
         const int nblk = (int)gridDim.x - G.bound_blocks;
         for (int t = (int)blockIdx.x - G.bound_blocks; t < G.ntile; t += nblk) {
             const int txi = t % G.ntx, tyi = (t / G.ntx) % G.nty, tzi = t / (G.ntx * G.nty);
-            const int x0 = txi * kGridTX, y0 = tyi * PlaneDims<NY>::TY, z0 = tzi * G.zc, z1 = min(G.lz, z0 + G.zc);
+            // tiles cover the interior nodes 1 .. l-2 of each axis (the faces are boundary groups)
+            const int x0 = 1 + txi * kGridTX, y0 = 1 + tyi * PlaneDims<NY>::TY, z0 = 1 + tzi * G.zc,
+                      z1 = min(G.lz - 1, z0 + G.zc);
             const int ix = x0 + tx;
             int32_t col_xy[NY];   // group index in its plane of the thread's nodes
             bool inxy[NY];
@@ -1272,7 +1274,9 @@ __global__ void __launch_bounds__(256, 3)   // 3 blocks an SM: FP64 fits 80 regi
 }
 
 // Planes per z run of a streaming tile: the run that minimises (waves of tiles) x (plane steps
-// per tile), with `conc` tiles resident at once; ties go to the longer run.
+// per tile), with `conc` tiles resident at once; ties go to the longer run.  Runs of 4, 8, .. 64
+// planes: measured at 128^3, the run that fits every tile into one wave (13 planes, 320 tiles) left
+// SMs with fewer resident blocks and was slower (FP32 residual 54 against 46 us) than 512 tiles of 8.
 inline int stream_run_length(int64_t plane_tiles, int lz, int64_t conc) {
     int best = 4;
     int64_t best_cost = INT64_MAX;
@@ -1310,19 +1314,22 @@ void launch_duvi_grid_h(const LaunchEnv &e, const dv_matrix *m, Gather g, Op op)
     G.lx = m->grid_lx;
     G.ly = m->grid_ly;
     G.lz = m->grid_lz;
-    G.ntx = (G.lx + kGridTX - 1) / kGridTX;
-    G.nty = (G.ly + PlaneDims<NY>::TY - 1) / PlaneDims<NY>::TY;
+    G.ntx = std::max(0, (G.lx - 2 + kGridTX - 1) / kGridTX);   // tiles over the interior nodes 1 .. l-2
+    G.nty = std::max(0, (G.ly - 2 + PlaneDims<NY>::TY - 1) / PlaneDims<NY>::TY);
     G.hot = m->grid_hot;
     G.all_hot = m->grid_all_hot;
     G.nbound = m->grid_nb;
     const int64_t wave = (int64_t)e.ctx->num_sms * occ;
+    // one boundary group a thread: more per thread puts the boundary blocks on the critical path
+    // (measured: two or four a thread slowed the solve by 6 and 14 %)
     G.bound_blocks = G.nbound == 0 ? 0
                      : (int32_t)std::min<int64_t>((G.nbound + 255) / 256, std::max<int64_t>(1, e.max_blocks / 4));
     const int64_t plane_tiles = (int64_t)G.ntx * G.nty;
-    G.zc = stream_run_length(plane_tiles, G.lz, std::max<int64_t>(1, wave - G.bound_blocks / 2));
-    G.ntile = (int32_t)(plane_tiles * ((G.lz + G.zc - 1) / G.zc));
+    const int lzi = std::max(1, G.lz - 2);
+    G.zc = stream_run_length(plane_tiles, lzi, std::max<int64_t>(1, wave - G.bound_blocks / 2));
+    G.ntile = G.lz > 2 ? (int32_t)(plane_tiles * ((lzi + G.zc - 1) / G.zc)) : 0;
     const int64_t tile_blocks = std::min<int64_t>(G.ntile, std::max<int64_t>(1, e.max_blocks - G.bound_blocks));
-    const int blocks = (int)(G.bound_blocks + tile_blocks);
+    const int blocks = (int)std::max<int64_t>(1, G.bound_blocks + tile_blocks);
     kern<<<blocks, 256, smem, e.stream>>>(G, cf, m->pat_id.as<uint16_t>(), m->pat_start.as<uint32_t>(),
                                           static_cast<const PatRec<AT> *>(m->pat_rec.p), m->grid_bnode.as<uint32_t>(),
                                           m->pat_count, m->pat_entries, g, op, e.done, e.partials, e.ticket);
