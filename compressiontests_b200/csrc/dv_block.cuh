@@ -389,7 +389,7 @@ __global__ void __launch_bounds__(kThreads) k_bprod_pattern(const uint16_t *__re
                                                             const uint32_t *__restrict__ base, int32_t npat,
                                                             int32_t nrec, int32_t ngroups, int kc, Gather g, Epi ep,
                                                             const int *__restrict__ done, double *partials,
-                                                            unsigned *ticket) {
+                                                            unsigned *ticket, const uint32_t *__restrict__ list) {
     if (done && *(volatile const int *)done) return;
     extern __shared__ uint4 bpat_smem[];
     dvk::PatRec<AT> *rec = reinterpret_cast<dvk::PatRec<AT> *>(bpat_smem);
@@ -409,7 +409,8 @@ __global__ void __launch_bounds__(kThreads) k_bprod_pattern(const uint16_t *__re
         for (int c = 0; c < NC; ++c) red[u][c] = 0.0;
     const int lane = threadIdx.x & 31;
     const int32_t nw = (gridDim.x * blockDim.x) >> 5;
-    for (int32_t grp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; grp < ngroups; grp += nw) {
+    for (int32_t gi = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; gi < ngroups; gi += nw) {
+        const int32_t grp = list ? (int32_t)__ldg(list + gi) : gi;   // list: the groups to run (ngroups of them)
         const uint32_t p = __ldg(pid + grp);
         const uint32_t b = st[p], e = st[p + 1];
         const int32_t r0 = grp * G;
@@ -448,20 +449,26 @@ __global__ void __launch_bounds__(kThreads) k_bprod_pattern(const uint16_t *__re
 }
 
 template <class AT, int U, bool EXACT, bool BASED, bool SHIFT, class Gather, class Epi>
-void launch_bprod_pattern_u(const LaunchEnv &e, const dv_matrix *m, int kc, Gather g, Epi ep) {
+void launch_bprod_pattern_u(const LaunchEnv &e, const dv_matrix *m, int kc, Gather g, Epi ep,
+                            const uint32_t *list = nullptr, int64_t nlist = 0) {
     constexpr int G = 3;
     auto kern = k_bprod_pattern<AT, G, U, EXACT, BASED, SHIFT, Gather, Epi>;
     const size_t smem = sizeof(dvk::PatRec<AT>) * (size_t)m->pat_entries + 4 * ((size_t)m->pat_count + 1);
     static dvk::SmemLimit limit;   // per instantiation and device
     limit.raise(kern, smem, e.ctx->device);
-    const int32_t ngroups = m->n_rows / G;
+    const int32_t ngroups = list ? (int32_t)nlist : m->n_rows / G;
     const int blocks = bprod_blocks(e, ngroups, Epi::NC > 0);
     kern<<<blocks, kThreads, smem, e.stream>>>(m->pat_id.as<uint16_t>(), m->pat_start.as<uint32_t>(),
                                                static_cast<const dvk::PatRec<AT> *>(m->pat_rec.p),
                                                m->pat_base.as<uint32_t>(), m->pat_count, m->pat_entries, ngroups, kc,
-                                               g, ep, e.done, e.partials, e.ticket);
+                                               g, ep, e.done, e.partials, e.ticket, list);
     DV_CUDA(cudaGetLastError());
     e.ctx->count();
+}
+
+template <int U, class Gather, class Epi>
+void launch_bprod_boundary(const LaunchEnv &e, const dv_matrix *m, int kc, Gather g, Epi ep) {
+    launch_bprod_pattern_u<float, U, true, false, false>(e, m, kc, g, ep, m->grid_bnode.as<uint32_t>(), m->grid_nb);
 }
 
 template <class AT, bool EXACT, bool BASED, bool SHIFT, class Gather, class Epi>
@@ -469,6 +476,214 @@ void launch_bprod_pattern(const LaunchEnv &e, const dv_matrix *m, int kc, Gather
     if (kc <= 32) launch_bprod_pattern_u<AT, 1, EXACT, BASED, SHIFT>(e, m, kc, g, ep);
     else if (kc <= 64) launch_bprod_pattern_u<AT, 2, EXACT, BASED, SHIFT>(e, m, kc, g, ep);
     else launch_bprod_pattern_u<AT, 4, EXACT, BASED, SHIFT>(e, m, kc, g, ep);
+}
+
+// ---------------------------------------------------------------------------
+// Block products on the grid-stencil layout (FP32 hex operators, epilogues without column
+// reductions).  A block owns a tile of 8 x 4 interior nodes of a plane, streams a run of z planes
+// and covers 32 right-hand sides (lane = column).  Each plane of the tile with its one-node halo
+// (10 x 6 nodes, 3 dofs, 32 columns: 180 rows of 128 bytes) is copied into a ring of shared-memory
+// slots with 16-byte cp.async copies, two planes ahead; warp w takes the 4 nodes x = 4 (w % 2) .. +3
+// of tile row w / 2 and applies every staged value of the plane to the nodes it couples in z - 1,
+// z and z + 1 (the streaming accumulators of k_duvi_grid) with the hex stencil's class values.
+// Each row sums its terms in column order with one FMA each, as the pattern kernel does (the
+// stencil's structural zeros skipped: they add exact zeros).  Face groups and interior groups of
+// other patterns run on the pattern kernel over the boundary list.
+// ---------------------------------------------------------------------------
+// DV_BGRID=0 keeps the pattern kernel for block products on grid layouts (A/B comparisons).
+inline bool bgrid_enabled() {
+    const char *v = getenv("DV_BGRID");
+    return !(v && v[0] == '0');
+}
+constexpr int kBgTX = 8, kBgTY = 4;                      // interior nodes of a tile
+constexpr int kBgHX = kBgTX + 2, kBgHY = kBgTY + 2;      // with the halo
+constexpr int kBgRows = kBgHX * kBgHY * 3;               // staged rows of a plane (node dofs)
+constexpr int kBgStages = 3;
+constexpr int kBgSlot = kBgRows * 32 + kBgRows;          // floats of a slot: the rows, then w (Jacobi from zero)
+
+struct BGridGeom {
+    int32_t lx, ly, lz, ntx, nty, zc, ntile, hot, all_hot;
+};
+
+template <class Gather>
+struct BGridSrc;   // the block array a gather stages, and its per-row weight (w .* B)
+template <class T>
+struct BGridSrc<BGatherVec<T, T>> {
+    static constexpr bool WB = false;
+    static const T *block(const BGatherVec<T, T> &g) { return g.x; }
+    __device__ static const T *weights(const BGatherVec<T, T> &) { return nullptr; }
+};
+template <class T>
+struct BGridSrc<BGatherWB<T>> {
+    static constexpr bool WB = true;
+    static const T *block(const BGatherWB<T> &g) { return g.b; }
+    __device__ static const T *weights(const BGatherWB<T> &g) { return g.w; }
+};
+
+template <class Gather>
+__device__ __forceinline__ void bgrid_issue(const Gather &g, const float *__restrict__ X, int ld, float *slot, int x0,
+                                            int y0, int z, const BGridGeom &G, int j0, int kc) {
+    const bool zin = z >= 0 && z < G.lz;
+    for (int c = threadIdx.x; c < kBgRows * 8; c += kThreads) {
+        const int row = c >> 3, sub = c & 7, hn = row / 3, comp = row - 3 * hn;
+        const int gx = x0 - 1 + hn % kBgHX, gy = y0 - 1 + hn / kBgHX;
+        const bool v = zin && gx >= 0 && gx < G.lx && gy >= 0 && gy < G.ly && j0 + 4 * sub < kc;
+        const int64_t grow = 3 * ((int64_t)gx + (int64_t)G.lx * (gy + (int64_t)G.ly * z)) + comp;
+        dvk::cp_async_zfill<16>(slot + row * 32 + 4 * sub, v ? X + grow * ld + j0 + 4 * sub : X, v);
+    }
+    if constexpr (BGridSrc<Gather>::WB) {
+        const float *w = BGridSrc<Gather>::weights(g);
+        for (int row = threadIdx.x; row < kBgRows; row += kThreads) {
+            const int hn = row / 3, comp = row - 3 * hn;
+            const int gx = x0 - 1 + hn % kBgHX, gy = y0 - 1 + hn / kBgHX;
+            const bool v = zin && gx >= 0 && gx < G.lx && gy >= 0 && gy < G.ly;
+            const int64_t grow = 3 * ((int64_t)gx + (int64_t)G.lx * (gy + (int64_t)G.ly * z)) + comp;
+            dvk::cp_async_zfill<4>(slot + kBgRows * 32 + row, v ? w + grow : w, v);
+        }
+    }
+    dvk::cp_async_commit();
+}
+
+template <class Gather, class Epi>
+__global__ void __launch_bounds__(kThreads, 3) k_bprod_grid(BGridGeom G, dvk::GridCoef<float> cf,
+                                                             const uint16_t *__restrict__ pid, const float *__restrict__ X,
+                                                             int ld, int kc, Gather g, Epi ep,
+                                                             const int *__restrict__ done) {
+    static_assert(Epi::NC == 0, "column reductions run on the pattern kernel");
+    if (done && *(volatile const int *)done) return;
+    extern __shared__ uint4 bgrid_smem[];
+    float *ring = reinterpret_cast<float *>(bgrid_smem);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int yw = warp >> 1, xs = (warp & 1) * 4;   // the warp's 4 nodes: tile x xs .. xs+3, tile row yw
+    const int j0 = blockIdx.y * 32;
+    const int64_t lxy = (int64_t)G.lx * G.ly;
+    double nored[1];
+    for (int t = blockIdx.x; t < G.ntile; t += gridDim.x) {
+        const int txi = t % G.ntx, tyi = (t / G.ntx) % G.nty, tzi = t / (G.ntx * G.nty);
+        const int x0 = 1 + txi * kBgTX, y0 = 1 + tyi * kBgTY, z0 = 1 + tzi * G.zc, z1 = min(G.lz - 1, z0 + G.zc);
+        const int gy = y0 + yw;
+        bool inxy[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) inxy[i] = x0 + xs + i <= G.lx - 2 && gy <= G.ly - 2;
+        auto active = [&](int i, int z) {
+            if (!inxy[i] || z < 1 || z > G.lz - 2) return false;
+            return G.all_hot || (int)__ldg(pid + (x0 + xs + i) + (int64_t)G.lx * gy + lxy * z) == G.hot;
+        };
+        bgrid_issue(g, X, ld, ring, x0, y0, z0 - 1, G, j0, kc);
+        if (z0 <= z1) bgrid_issue(g, X, ld, ring + kBgSlot, x0, y0, z0, G, j0, kc);
+        else dvk::cp_async_commit();
+        float a0[4][3], a1[4][3], a2[4][3];
+        bool act0[4], act1[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            act0[i] = act1[i] = false;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) a0[i][d] = a1[i][d] = a2[i][d] = 0.f;
+        }
+        for (int p = z0 - 1, k = 0; p <= z1; ++p, ++k) {
+            dvk::cp_async_wait<kBgStages - 2>();
+            __syncthreads();
+            if (p + 2 <= z1) bgrid_issue(g, X, ld, ring + ((k + 2) % kBgStages) * kBgSlot, x0, y0, p + 2, G, j0, kc);
+            else dvk::cp_async_commit();
+            const float *pl = ring + (k % kBgStages) * kBgSlot;
+            const bool di = p + 1 >= z0 && p + 1 < z1, dm = p >= z0 && p < z1, df = p - 1 >= z0 && p - 1 < z1;
+            bool act2[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                act2[i] = di && active(i, p + 1);
+#pragma unroll
+                for (int d = 0; d < 3; ++d) a2[i][d] = 0.f;
+            }
+#pragma unroll
+            for (int dy = 0; dy < 3; ++dy)
+#pragma unroll
+                for (int hx = 0; hx < 6; ++hx)
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        const int row = ((yw + dy) * kBgHX + xs + hx) * 3 + c;
+                        float v = pl[row * 32 + lane];
+                        if constexpr (BGridSrc<Gather>::WB) v = pl[kBgRows * 32 + row] * v;
+#pragma unroll
+                        for (int i = 0; i < 4; ++i) {
+                            const int dx = hx - i;   // neighbour offset + 1
+                            if (dx < 0 || dx > 2) continue;
+                            const int e = 9 * dy + 3 * dx + c;
+#pragma unroll
+                            for (int d = 0; d < 3; ++d) {
+                                const int ci = dvk::hex_class(3 * e + d), cm = dvk::hex_class(3 * (27 + e) + d),
+                                          cz = dvk::hex_class(3 * (54 + e) + d);
+                                if (ci >= 0 && di) a2[i][d] = fmaf(cf.cls[ci], v, a2[i][d]);
+                                if (cm >= 0 && dm) a1[i][d] = fmaf(cf.cls[cm], v, a1[i][d]);
+                                if (cz >= 0 && df) a0[i][d] = fmaf(cf.cls[cz], v, a0[i][d]);
+                            }
+                        }
+                    }
+            if (df && lane < kc - j0) {
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+                    if (act0[i]) {
+                        const int32_t r = (int32_t)(3 * ((x0 + xs + i) + G.lx * (int64_t)gy + lxy * (p - 1)));
+#pragma unroll
+                        for (int d = 0; d < 3; ++d) ep.apply(r + d, j0 + lane, a0[i][d], nored);
+                    }
+            }
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    a0[i][d] = a1[i][d];
+                    a1[i][d] = a2[i][d];
+                }
+                act0[i] = act1[i];
+                act1[i] = act2[i];
+            }
+        }
+        dvk::cp_async_wait<0>();
+        __syncthreads();
+    }
+}
+
+template <class Gather>
+struct bgrid_gather : std::false_type {};
+template <>
+struct bgrid_gather<BGatherVec<float, float>> : std::true_type {};
+template <>
+struct bgrid_gather<BGatherWB<float>> : std::true_type {};
+
+// The grid-stencil block product and the boundary groups' pattern walk (two launches, disjoint rows).
+template <class Gather, class Epi>
+void launch_bprod_grid(const LaunchEnv &e, const dv_matrix *m, int kc, Gather g, Epi ep) {
+    BGridGeom G;
+    G.lx = m->grid_lx;
+    G.ly = m->grid_ly;
+    G.lz = m->grid_lz;
+    G.ntx = std::max(0, (G.lx - 2 + kBgTX - 1) / kBgTX);   // tiles over the interior nodes 1 .. l-2
+    G.nty = std::max(0, (G.ly - 2 + kBgTY - 1) / kBgTY);
+    G.zc = 8;
+    const int lzi = std::max(1, G.lz - 2);
+    G.ntile = G.lz > 2 ? G.ntx * G.nty * ((lzi + G.zc - 1) / G.zc) : 0;
+    G.hot = m->grid_hot;
+    G.all_hot = m->grid_all_hot;
+    dvk::GridCoef<float> cf;
+    for (int k = 0; k < 81; ++k)
+        for (int d = 0; d < 3; ++d) cf.v[k][d] = (float)m->grid_coef[3 * k + d];
+    for (int c = 0; c < dvk::kHexClasses; ++c) cf.cls[c] = (float)m->grid_cls[c];
+    if (G.ntile > 0) {
+        auto kern = k_bprod_grid<Gather, Epi>;
+        const size_t smem = sizeof(float) * (size_t)kBgStages * kBgSlot;
+        static dvk::SmemLimit limit;   // per instantiation and device
+        limit.raise(kern, smem, e.ctx->device);
+        const dim3 grid((unsigned)G.ntile, (unsigned)((kc + 31) / 32));
+        kern<<<grid, kThreads, smem, e.stream>>>(G, cf, m->pat_id.as<uint16_t>(), BGridSrc<Gather>::block(g), g.ld, kc,
+                                                 g, ep, e.done);
+        DV_CUDA(cudaGetLastError());
+        e.ctx->count();
+    }
+    if (m->grid_nb > 0) {
+        if (kc <= 32) launch_bprod_boundary<1>(e, m, kc, g, ep);
+        else if (kc <= 64) launch_bprod_boundary<2>(e, m, kc, g, ep);
+        else launch_bprod_boundary<4>(e, m, kc, g, ep);
+    }
 }
 
 // Matrix-free trilinear transfer (DV_FORMAT_TRILINEAR): one thread per (node, column j), the
@@ -510,6 +725,15 @@ void launch_bprod(const LaunchEnv &e, const dv_matrix *m, int kc, Gather g, Epi 
     }
     DV_REQUIRE(m->format == DV_FORMAT_CSR || m->format == DV_FORMAT_DUVI, DV_ERR_UNSUPPORTED,
                "block products need an assembled matrix");
+    if constexpr (Epi::NC == 0 && std::is_same<AT, float>::value && bgrid_gather<Gather>::value) {
+        // FP32 hex operators on the grid-stencil layout; 16-byte copies need an aligned block and ld
+        const void *xb = BGridSrc<Gather>::block(g);
+        if (m->format == DV_FORMAT_DUVI && m->duvi_variant == 3 && m->grid_hex && m->precision == DV_F32 &&
+            (reinterpret_cast<uintptr_t>(xb) & 15) == 0 && g.ld % 4 == 0 && bgrid_enabled()) {
+            launch_bprod_grid(e, m, kc, g, ep);
+            return;
+        }
+    }
     if (m->format == DV_FORMAT_DUVI && m->pat_ok && m->lanes_group == 3) {   // node patterns, 3-row groups
         if (!m->pat_based && !m->pat_shift) {
             launch_bprod_pattern<AT, EXACT, false, false>(e, m, kc, g, ep);

@@ -115,3 +115,48 @@ def test_multi_rhs_iteration_limit(ctx, native, problem):
     X, st, conv = s.solve_many(B)
     assert not st.HasConverged and not conv.any()
     assert st.NumIterationsRequired == 3
+
+
+@pytest.mark.parametrize("k", [5, 8, 32, 40, 64, 128])
+def test_block_grid_stencil_equals_pattern_kernel(ctx, native, rng, k, monkeypatch):
+    # FP32 block products of a hex operator on the grid layout: the grid-stencil block kernel
+    # (tiles of 8 x 4 nodes streaming z planes, lanes over 32 right-hand sides; the face groups on
+    # the pattern kernel) sums each row in the pattern kernel's column order with the same fused
+    # multiply-adds, skipping only exact zeros, so both give the same floats.  k = 5 (a block whose
+    # rows are not 16-byte multiples) takes the pattern kernel either way.
+    import torch
+    monkeypatch.setenv("DV_AUTOTUNE", "0")
+    A = native.hex_stiffness((20, 9, 13), scale=2.0)
+    M = native.SparseMatrix(ctx, A, "duvi", "f32")
+    assert M.info()["kernel_variant"] == 303
+    X = rng.standard_normal((A.shape[1], k)).astype(np.float32)
+    dX = torch.from_numpy(X).cuda()
+    out = {}
+    for flag in ("1", "0"):
+        monkeypatch.setenv("DV_BGRID", flag)
+        dY = torch.full((A.shape[0], k), np.nan, dtype=torch.float32, device="cuda")
+        torch.cuda.synchronize()
+        M.multiply_many_device(k, dX.data_ptr(), dY.data_ptr(), "f32")
+        ctx.synchronize()
+        out[flag] = dY.cpu().numpy()
+    np.testing.assert_array_equal(out["1"], out["0"])
+    ref = A @ X.astype(np.float64)
+    scale = np.abs(A) @ np.abs(X.astype(np.float64)) + 1e-300
+    assert np.max(np.abs(out["1"] - ref) / scale) <= 1e-5
+
+
+def test_block_grid_stencil_solver_equals_pattern_solver(ctx, native, problem, monkeypatch):
+    # The multi-right-hand-side V-cycle on the grid-stencil block kernel gives the same iterates
+    # as on the pattern kernel (every block product equal): same iteration count, same solution.
+    ne, A, P = problem
+    B = native.random_face_loads(ne, 16, seed=5)
+    res = {}
+    for flag in ("1", "0"):
+        monkeypatch.setenv("DV_BGRID", flag)
+        s = native.MultigridPcgSolver(ctx, A, P, precision="mixed", fmt="duvi", nu=2, tol=1e-10, max_iterations=200)
+        X, st, conv = s.solve_many(B)
+        assert conv.all()
+        res[flag] = (X, st.NumIterationsRequired)
+        s.release()
+    assert res["1"][1] == res["0"][1]
+    np.testing.assert_array_equal(res["1"][0], res["0"][0])
