@@ -1274,13 +1274,14 @@ __global__ void __launch_bounds__(256, 3)   // 3 blocks an SM: FP64 fits 80 regi
 }
 
 // Planes per z run of a streaming tile: the run that minimises (waves of tiles) x (plane steps
-// per tile), with `conc` tiles resident at once; ties go to the longer run.  Runs of 4, 8, .. 64
+// per tile), with `conc` tiles resident at once; ties go to the longer run.  Runs of 2, 4, .. 64
 // planes: measured at 128^3, the run that fits every tile into one wave (13 planes, 320 tiles) left
-// SMs with fewer resident blocks and was slower (FP32 residual 54 against 46 us) than 512 tiles of 8.
+// SMs with fewer resident blocks and was slower (FP32 residual 54 against 46 us) than 512 tiles of 8;
+// runs of 2 give the coarse levels more tiles (mixed solve 8.45 -> 8.30 ms).
 inline int stream_run_length(int64_t plane_tiles, int lz, int64_t conc) {
-    int best = 4;
+    int best = 2;
     int64_t best_cost = INT64_MAX;
-    for (int zc = 4; zc <= 64; zc *= 2) {
+    for (int zc = 2; zc <= 64; zc *= 2) {
         const int64_t tiles = plane_tiles * ((lz + zc - 1) / zc);
         const int64_t cost = ((tiles + conc - 1) / conc) * (int64_t)(std::min(zc, lz) + 2);
         if (cost <= best_cost) {
