@@ -695,8 +695,8 @@ __global__ void __launch_bounds__(kThreads) k_bprod_tri(dvk::TriGeom G, int kc, 
     if (done && *(volatile const int *)done) return;
     const int64_t work = G.nodes(RESTRICT) * kc;
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < work; t += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t q = t / kc;
-        const int j = (int)(t - q * kc);
+        const uint32_t q = (uint32_t)(t / kc);
+        const int j = (int)(t - (int64_t)q * kc);
         AT s[3] = {AT(0), AT(0), AT(0)};
         dvk::tri_walk<RESTRICT, AT>(G, q, [&](uint32_t col, AT w) {
 #pragma unroll

@@ -1702,10 +1702,12 @@ struct TriGeom {
 // Calls f(first column, weight) for the coarse nodes of fine free node q (prolongation, a row of P)
 // or the fine nodes of coarse free node q (restriction, a row of P^T), in increasing column order.
 template <bool RESTRICT, class AT, class F>
-__device__ __forceinline__ void tri_walk(const TriGeom &G, int64_t q, F &&f) {
+__device__ __forceinline__ void tri_walk(const TriGeom &G, uint32_t q, F &&f) {
+    // 32-bit index arithmetic throughout: rows and columns are below 2^31
+    const uint32_t ny = G.f1 + 1, cx = G.f0 / 2, cy = G.f1 / 2 + 1;
     if constexpr (!RESTRICT) {
-        const int32_t ny = G.f1 + 1, cx = G.f0 / 2, cy = G.f1 / 2 + 1;
-        const int32_t X = (int32_t)(q % G.f0) + 1, Y = (int32_t)((q / G.f0) % ny), Z = (int32_t)(q / ((int64_t)G.f0 * ny));
+        const uint32_t t = q / (uint32_t)G.f0, Zy = t / ny;
+        const int32_t X = (int32_t)(q - t * (uint32_t)G.f0) + 1, Y = (int32_t)(t - Zy * ny), Z = (int32_t)Zy;
         const int nx_ = (X & 1) ? 2 : 1, ny_ = (Y & 1) ? 2 : 1, nz_ = (Z & 1) ? 2 : 1;
         const AT w = (nx_ == 2 ? AT(0.5) : AT(1)) * (ny_ == 2 ? AT(0.5) : AT(1)) * (nz_ == 2 ? AT(0.5) : AT(1));
         for (int c = 0; c < nz_; ++c)
@@ -1713,11 +1715,11 @@ __device__ __forceinline__ void tri_walk(const TriGeom &G, int64_t q, F &&f) {
                 for (int a = 0; a < nx_; ++a) {
                     const int32_t xc = X / 2 + a;
                     if (xc == 0) continue;   // clamped coarse node
-                    f((uint32_t)(3 * ((xc - 1) + cx * ((int64_t)(Y / 2 + b) + cy * (int64_t)(Z / 2 + c)))), w);
+                    f(3u * ((uint32_t)(xc - 1) + cx * ((uint32_t)(Y / 2 + b) + cy * (uint32_t)(Z / 2 + c))), w);
                 }
     } else {
-        const int32_t ny = G.f1 + 1, cx = G.f0 / 2, cy = G.f1 / 2 + 1;
-        const int32_t Xc = (int32_t)(q % cx) + 1, Yc = (int32_t)((q / cx) % cy), Zc = (int32_t)(q / ((int64_t)cx * cy));
+        const uint32_t t = q / cx, Zc_ = t / cy;
+        const int32_t Xc = (int32_t)(q - t * cx) + 1, Yc = (int32_t)(t - Zc_ * cy), Zc = (int32_t)Zc_;
         for (int c = -1; c <= 1; ++c) {
             const int32_t Z = 2 * Zc + c;
             if (Z < 0 || Z > G.f2) continue;
@@ -1728,7 +1730,7 @@ __device__ __forceinline__ void tri_walk(const TriGeom &G, int64_t q, F &&f) {
                     const int32_t X = 2 * Xc + a;
                     if (X > G.f0) continue;   // X >= 1 always (Xc >= 1)
                     const AT w = (a ? AT(0.5) : AT(1)) * (b ? AT(0.5) : AT(1)) * (c ? AT(0.5) : AT(1));
-                    f((uint32_t)(3 * ((X - 1) + G.f0 * ((int64_t)Y + ny * (int64_t)Z))), w);
+                    f(3u * ((uint32_t)(X - 1) + (uint32_t)G.f0 * ((uint32_t)Y + ny * (uint32_t)Z)), w);
                 }
             }
         }
@@ -1744,8 +1746,8 @@ __global__ void __launch_bounds__(256) k_tri(TriGeom G, Gather g, Op op, const i
     double red[Op::NRED > 0 ? Op::NRED : 1];
 #pragma unroll
     for (int i = 0; i < (Op::NRED > 0 ? Op::NRED : 1); ++i) red[i] = 0.0;
-    const int64_t nodes = G.nodes(RESTRICT);
-    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < nodes; q += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t nodes = (uint32_t)G.nodes(RESTRICT);
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < nodes; q += gridDim.x * blockDim.x) {
         const int32_t r0 = (int32_t)(3 * q);
         AT s[3];
 #pragma unroll
