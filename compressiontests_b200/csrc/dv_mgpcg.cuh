@@ -41,6 +41,9 @@ struct VCycle {
     // Flexible-CG reduction fused into the finest level's last sweep (Jacobi only): set
     // by the driver, consumed by level 0.
     const double *fuse_q = nullptr, *fuse_r = nullptr;
+    // w .* b of level 0 when the caller already formed it (the flexible CG's update writes it next to
+    // the FP32 residual): the first sweep then gathers one staged array instead of two
+    const T *wb0 = nullptr;
     SolverScalars *fuse_sc = nullptr;
     bool fused_red() const { return fuse_sc != nullptr && smoother == DV_SMOOTHER_JACOBI; }
 
@@ -65,7 +68,8 @@ struct VCycle {
             ctx->count();
         } else {
             OpJacobiFromZero<T> op{{}, w, b, x};
-            launch_rows<T>(e, L.A.get(), GatherWB<T>{w, b}, op);
+            if (l == 0 && wb0) launch_rows<T>(e, L.A.get(), GatherVec<T, T>{wb0}, op);
+            else launch_rows<T>(e, L.A.get(), GatherWB<T>{w, b}, op);
             for (int k = 2; k < nu; ++k) {
                 OpJacobi<T> oj{{}, x, w, b, t};
                 launch_rows<T>(e, L.A.get(), GatherVec<T, T>{x}, oj);
@@ -131,7 +135,7 @@ struct dv_mgpcg {
     std::unique_ptr<VCycle<double>> v64;
     std::unique_ptr<SolverWs> ws;
     int32_t n = 0;
-    DevMem b, x, r, r32, p, q;
+    DevMem b, x, r, r32, wb32, p, q;
     std::vector<double> omega_eff;
     int64_t launches_last = 0;
     MultiHolder *multi = nullptr;   // block (multi-right-hand-side) work buffers, created on first use

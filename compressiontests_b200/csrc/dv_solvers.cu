@@ -177,11 +177,13 @@ __global__ void k_fcg_red(const ZT *__restrict__ z, const double *__restrict__ q
     }
 }
 
-// x += alpha p; r -= alpha q; r32 = r (mixed); ||r||^2 and the stop decision.
+// x += alpha p; r -= alpha q; r32 = r and wb = w0 .* r32 (mixed: the V-cycle's first sweep gathers
+// wb); ||r||^2 and the stop decision.
 template <class RT>
 __global__ void k_fcg_update(double *__restrict__ x, double *__restrict__ r, RT *__restrict__ rlow,
-                             const double *__restrict__ p, const double *__restrict__ q, int32_t n, SolverScalars *sc,
-                             const int *__restrict__ done, double *partials, unsigned *ticket) {
+                             const RT *__restrict__ w0, RT *__restrict__ wb, const double *__restrict__ p,
+                             const double *__restrict__ q, int32_t n, SolverScalars *sc, const int *__restrict__ done,
+                             double *partials, unsigned *ticket) {
     if (*(volatile const int *)done) return;
     const double a = sc->alpha;
     double red[1] = {0.0};
@@ -189,7 +191,11 @@ __global__ void k_fcg_update(double *__restrict__ x, double *__restrict__ r, RT 
         x[i] = x[i] + a * p[i];
         double ri = r[i] - a * q[i];
         r[i] = ri;
-        if (rlow) rlow[i] = (RT)ri;
+        if (rlow) {
+            const RT rl = (RT)ri;
+            rlow[i] = rl;
+            if (wb) wb[i] = w0[i] * rl;
+        }
         red[0] += ri * ri;
     }
     double t[1];
@@ -601,7 +607,10 @@ extern "C" DV_API int dv_mgpcg_create_hex(dv_context *ctx, const int32_t *ne, do
             s->v64 = build_vcycle<double>(ctx, *s->ws, L, Ash.data(), Psh.data(), *cfg, s->omega_eff, nullptr, &prebuilt, tri);
         const size_t nb = 8 * (size_t)s->n;
         s->b.alloc(nb); s->x.alloc(nb); s->r.alloc(nb); s->p.alloc(nb); s->q.alloc(nb);
-        if (cfg->precision == DV_MIXED) s->r32.alloc(4 * (size_t)s->n);
+        if (cfg->precision == DV_MIXED) {
+            s->r32.alloc(4 * (size_t)s->n);
+            s->wb32.alloc(4 * (size_t)s->n);
+        }
         DV_CUDA(cudaStreamSynchronize(st));
         *out = s.release();
     });
@@ -632,7 +641,10 @@ extern "C" DV_API int dv_mgpcg_create(dv_context *ctx, int32_t L, const dv_csr_h
         else s->v64 = build_vcycle<double>(ctx, *s->ws, L, A, P, *cfg, s->omega_eff, shared);
         const size_t nb = 8 * (size_t)s->n;
         s->b.alloc(nb); s->x.alloc(nb); s->r.alloc(nb); s->p.alloc(nb); s->q.alloc(nb);
-        if (cfg->precision == DV_MIXED) s->r32.alloc(4 * (size_t)s->n);
+        if (cfg->precision == DV_MIXED) {
+            s->r32.alloc(4 * (size_t)s->n);
+            s->wb32.alloc(4 * (size_t)s->n);
+        }
         DV_CUDA(cudaStreamSynchronize(ctx->stream));
         *out = s.release();
     });
@@ -652,12 +664,19 @@ static const T *fcg_step(dv_mgpcg *s, const LaunchEnv &e, VCycle<T> &vc, const T
     }
     OpFcg<T> op{z, s->p.as<double>(), s->q.as<double>(), s->ws->sc(), 0.0};
     launch_rows<double>(e, s->Aout.get(), GatherVec<T, double>{z}, op);
-    T *rl = std::is_same<T, float>::value ? reinterpret_cast<T *>(s->r32.p) : nullptr;
-    k_fcg_update<T><<<g, kThreads, 0, st>>>(s->x.as<double>(), s->r.as<double>(), rl, s->p.as<double>(),
+    const bool mixed = std::is_same<T, float>::value;
+    T *rl = mixed ? reinterpret_cast<T *>(s->r32.p) : nullptr;
+    const bool form_wb = mixed && vc.nu > 1 && vc.smoother == DV_SMOOTHER_JACOBI && !vc.lv.empty();
+    T *wb = form_wb ? reinterpret_cast<T *>(s->wb32.p) : nullptr;
+    const T *w0 = wb ? vc.lv[0].w.template as<T>() : nullptr;
+    k_fcg_update<T><<<g, kThreads, 0, st>>>(s->x.as<double>(), s->r.as<double>(), rl, w0, wb, s->p.as<double>(),
                                             s->q.as<double>(), s->n, s->ws->sc(), e.done, e.partials, e.ticket);
     DV_CUDA(cudaGetLastError());
     s->ctx->count();
-    return vc.run(e, rin);
+    vc.wb0 = wb;
+    const T *zn = vc.run(e, rin);
+    vc.wb0 = nullptr;   // the first cycle and the restarts form w .* b in the sweep
+    return zn;
 }
 
 // Outer iterations to run before the next host read of the stop flag: as many as the
