@@ -234,6 +234,21 @@ struct OpSpmv : NoRed {
     __device__ __forceinline__ void touch(int32_t) const {}
 };
 
+// y = A x (restriction into the next level's right-hand side) and wb = w .* y, the product the
+// next level's first Jacobi sweep gathers
+template <class T>
+struct OpRestrictWB : NoRed {
+    T *__restrict__ y;
+    T *__restrict__ wb;
+    const T *__restrict__ w;
+    __device__ __forceinline__ T init(int32_t) const { return T(0); }
+    __device__ __forceinline__ void row(int32_t r, T s, double *) const {
+        y[r] = s;
+        wb[r] = w[r] * s;
+    }
+    __device__ __forceinline__ void touch(int32_t) const {}
+};
+
 // r = b - A x
 template <class T>
 struct OpResid : NoRed {

@@ -24,6 +24,7 @@ template <class T>
 struct VLevel {
     std::unique_ptr<dv_matrix> A, R, P;
     DevMem w, b, x, t, r;
+    DevMem wb;    // w .* b, written by the restriction from the level above (Jacobi, nu > 1)
     int32_t n = 0;
     GsOrder gs;   // Gauss-Seidel row groups (smoother != Jacobi)
 };
@@ -47,9 +48,10 @@ struct VCycle {
     SolverScalars *fuse_sc = nullptr;
     bool fused_red() const { return fuse_sc != nullptr && smoother == DV_SMOOTHER_JACOBI; }
 
-    T *run(const LaunchEnv &e, const T *b0) { return level(e, 0, b0); }
+    T *run(const LaunchEnv &e, const T *b0) { return level(e, 0, b0, wb0); }
 
-    T *level(const LaunchEnv &e, size_t l, const T *b) {
+    // wb: w .* b of this level when the caller formed it (else the first sweep forms it)
+    T *level(const LaunchEnv &e, size_t l, const T *b, const T *wb = nullptr) {
         cudaStream_t s = e.stream;
         if (l == lv.size()) {
             k_dense_gemv_rows<T><<<std::max(1, std::min(nc, ctx->num_sms * 16)), 128, 0, s>>>(
@@ -68,7 +70,7 @@ struct VCycle {
             ctx->count();
         } else {
             OpJacobiFromZero<T> op{{}, w, b, x};
-            if (l == 0 && wb0) launch_rows<T>(e, L.A.get(), GatherVec<T, T>{wb0}, op);
+            if (wb) launch_rows<T>(e, L.A.get(), GatherVec<T, T>{wb}, op);
             else launch_rows<T>(e, L.A.get(), GatherWB<T>{w, b}, op);
             for (int k = 2; k < nu; ++k) {
                 OpJacobi<T> oj{{}, x, w, b, t};
@@ -79,11 +81,18 @@ struct VCycle {
         OpResid<T> orr{{}, b, L.r.template as<T>()};
         launch_rows<T>(e, L.A.get(), GatherVec<T, T>{x}, orr);
         T *bn = l + 1 < lv.size() ? lv[l + 1].b.template as<T>() : bc.template as<T>();
-        OpSpmv<T, T> orst;
-        orst.y = bn;
-        orst.clear = 1;
-        launch_rows<T>(e, L.R.get(), GatherVec<T, T>{L.r.template as<T>()}, orst);
-        T *xn = level(e, l + 1, bn);
+        T *wbn = nullptr;
+        if (l + 1 < lv.size() && nu > 1) {   // the next level's first sweep gathers w .* b
+            wbn = lv[l + 1].wb.template as<T>();
+            OpRestrictWB<T> orst{{}, bn, wbn, lv[l + 1].w.template as<T>()};
+            launch_rows<T>(e, L.R.get(), GatherVec<T, T>{L.r.template as<T>()}, orst);
+        } else {
+            OpSpmv<T, T> orst;
+            orst.y = bn;
+            orst.clear = 1;
+            launch_rows<T>(e, L.R.get(), GatherVec<T, T>{L.r.template as<T>()}, orst);
+        }
+        T *xn = level(e, l + 1, bn, wbn);
         OpSpmv<T, T> opro;
         opro.y = x;
         opro.clear = 0;

@@ -483,6 +483,7 @@ static std::unique_ptr<VCycle<T>> build_vcycle(dv_context *ctx, SolverWs &ws, in
         omega_eff.push_back(om);
         const size_t vs = sizeof(T) * (size_t)lv.n;
         lv.w.alloc(vs); lv.b.alloc(vs); lv.x.alloc(vs); lv.t.alloc(vs); lv.r.alloc(vs);
+        if (l > 0 && cfg.smoother == DV_SMOOTHER_JACOBI && cfg.nu > 1) lv.wb.alloc(vs);
         if (cfg.smoother != DV_SMOOTHER_JACOBI) gs_build_order(A[l], cfg.smoother == DV_SMOOTHER_GS_LEX, s, lv.gs);
         k_make_weights<T><<<grid_for(ctx, lv.n), kThreads, 0, s>>>(lv.A->diag.template as<double>(), lv.w.template as<T>(), om, lv.n);
         DV_CUDA(cudaGetLastError());
