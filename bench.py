@@ -69,6 +69,8 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--size", type=int, default=128)
     p.add_argument("--tol", type=float, default=1e-8)
+    p.add_argument("--iterations-per-sync", type=int, default=4,
+                   help="most outer iterations between host reads of the stop flag (MG-PCG solvers)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-fp64", action="store_true")
     p.add_argument("--no-spmv", action="store_true")
@@ -424,10 +426,11 @@ def run_ours(args):
         tol = args.tol if tol is None else tol
         if fmt == "duvi" and not args.host_setup:   # hierarchy assembled and encoded on the device
             return cb.MultigridPcgSolver.from_hex(ctx, (n, n, n), coarse_ne=8, precision=precision, nu=2,
-                                                  omega=2 / 3, omega_mode="spectral", tol=tol,
-                                                  max_iterations=500)
+                                                  omega=2 / 3, omega_mode="spectral", tol=tol, max_iterations=500,
+                                                  iterations_per_sync=args.iterations_per_sync)
         return cb.MultigridPcgSolver(ctx, A, P, precision=precision, fmt=fmt, outer_fmt=fmt, nu=2, omega=2 / 3,
-                                     omega_mode="spectral", tol=tol, max_iterations=500)
+                                     omega_mode="spectral", tol=tol, max_iterations=500,
+                                     iterations_per_sync=args.iterations_per_sync)
 
     db = torch.from_numpy(b).to(f"cuda:{local}")
     dx = torch.zeros_like(db)
