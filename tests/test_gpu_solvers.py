@@ -310,6 +310,26 @@ def test_mgpcg_device_built_hierarchy_equals_host_built(ctx, native, precision):
     dev.release()
 
 
+def test_mgpcg_tight_tolerance_mixed_and_fp64(ctx, native):
+    # The multigrid configuration's 1e-10 runs: the device-built mixed solver (FP32 V-cycle in the
+    # FP64 flexible CG, restarts from the FP64 true residual where the recurrence drifts) and the FP64
+    # one both reach a true relative residual of 1e-10, in the same number of iterations within one.
+    ne = (16, 16, 16)
+    A = native.hex_stiffness(ne)
+    b = native.traction_rhs(ne)
+    res = {}
+    for precision in ("mixed", "f64"):
+        s = native.MultigridPcgSolver.from_hex(ctx, ne, coarse_ne=4, precision=precision, tol=1e-10,
+                                               max_iterations=200)
+        x, st = s.Solve(b)
+        assert st.HasConverged and st.RelativeResidual <= 1e-10, st
+        assert np.linalg.norm(b - A @ x) / np.linalg.norm(b) <= 1e-10
+        res[precision] = (x, st.NumIterationsRequired)
+        s.release()
+    assert abs(res["mixed"][1] - res["f64"][1]) <= 1
+    assert rel(res["mixed"][0], res["f64"][0]) < 1e-8
+
+
 def test_slab_operator_on_device_single_rank(ctx, native, oracle):
     # The slab layer's device path on one rank: the owned rows (all of them here) as a DuVi device
     # matrix, the product through the C ABI, and the slab Jacobi-PCG against the oracle's PCG.
